@@ -1,0 +1,227 @@
+// aw_internal.cuh — internal types and device helpers of the sm_100a FLIP-on-MSBG library.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "anitowave.h"
+
+namespace aw {
+
+// ------------------------------------------------------------------------------------------------
+// Errors
+// ------------------------------------------------------------------------------------------------
+aw_status set_error(aw_status s, const char* fmt, ...);
+
+#define AW_CUDA(call)                                                                                  \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return ::aw::set_error(AW_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                                   __FILE__, __LINE__);                                                \
+    } while (0)
+// every kernel launch site is followed by AW_LAUNCH(), which also counts the launch
+extern unsigned long long g_launches;
+#define AW_LAUNCH()                \
+    do {                           \
+        ++::aw::g_launches;        \
+        AW_CUDA(cudaGetLastError()); \
+    } while (0)
+#define AW_TRY(expr)                     \
+    do {                                 \
+        aw_status aw_st_ = (expr);        \
+        if (aw_st_ != AW_OK) return aw_st_; \
+    } while (0)
+#define AW_CHECK_ARG(cond, msg)                                             \
+    do {                                                                    \
+        if (!(cond)) return ::aw::set_error(AW_ERR_INVALID_ARGUMENT, "%s", msg); \
+    } while (0)
+
+// ------------------------------------------------------------------------------------------------
+// Device buffers
+// ------------------------------------------------------------------------------------------------
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    aw_status alloc(size_t count) {
+        free();
+        if (count == 0) return AW_OK;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            return set_error(e == cudaErrorMemoryAllocation ? AW_ERR_OUT_OF_MEMORY : AW_ERR_CUDA,
+                             "cudaMalloc(%zu bytes): %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        n = count;
+        return AW_OK;
+    }
+    aw_status ensure(size_t count) { return count <= n ? AW_OK : alloc(count); }
+    void free() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { free(); }
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) {
+            free();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// Kernel-side views
+// ------------------------------------------------------------------------------------------------
+// Geometry shared by every level.
+struct Geo {
+    int D[3];
+    float bs;
+    float dmin[3];
+    int R0;
+    int L;
+    int nb;
+};
+
+// One block-structured MG level: per-block resolution and offsets (MSBG.cuh:86-89 layout).
+struct LevelView {
+    Geo g;
+    const int* res;          // cells per edge (0 = block owns nothing at this level)
+    const uint32_t* off[4];  // cells, faces x, y, z
+};
+
+struct DenseView {
+    int D[3];
+};
+
+__host__ __device__ inline int bidx(const Geo& g, int x, int y, int z) { return x + g.D[0] * (y + g.D[1] * z); }
+__host__ __device__ inline void bcoord(const Geo& g, int b, int c[3]) {
+    c[0] = b % g.D[0];
+    c[1] = (b / g.D[0]) % g.D[1];
+    c[2] = b / (g.D[0] * g.D[1]);
+}
+__host__ __device__ inline bool inside(const Geo& g, const int c[3]) {
+    return c[0] >= 0 && c[1] >= 0 && c[2] >= 0 && c[0] < g.D[0] && c[1] < g.D[1] && c[2] < g.D[2];
+}
+__host__ __device__ inline uint32_t cidx(int x, int y, int z, int r) { return (uint32_t)(x + r * (y + r * z)); }
+// face index maps (MSBG.cuh:169-179)
+__host__ __device__ inline uint32_t fidx(int a, int x, int y, int z, int r) {
+    return a == 0 ? (uint32_t)(x + (r + 1) * (y + r * z))
+                  : (a == 1 ? (uint32_t)(x + r * (y + (r + 1) * z)) : (uint32_t)(x + r * (y + r * z)));
+}
+__host__ __device__ inline uint32_t didx(const DenseView& d, int i, int j, int k) {
+    return (uint32_t)(i + d.D[0] * (j + d.D[1] * k));
+}
+__host__ __device__ inline uint32_t dfidx(const DenseView& d, int a, int i, int j, int k) {
+    return a == 0 ? (uint32_t)(i + (d.D[0] + 1) * (j + d.D[1] * k))
+                  : (a == 1 ? (uint32_t)(i + d.D[0] * (j + (d.D[1] + 1) * k)) : (uint32_t)(i + d.D[0] * (j + d.D[1] * k)));
+}
+
+// Single-precision block origin and cell size, with the rounding the oracle reproduces.
+__device__ inline float forigin(const Geo& g, int a, int c) { return __fadd_rn(g.dmin[a], __fmul_rn((float)c, g.bs)); }
+__device__ inline float fcell(const Geo& g, int r) { return __fdiv_rn(g.bs, (float)r); }
+
+// Block of a point (worldToBlockCoord, MSBG.cuh:151-159), clamped into the domain.
+__device__ inline void point_block(const Geo& g, const float p[3], int c[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float rel = __fsub_rn(p[a], g.dmin[a]);
+        int v = (int)floorf(__fdiv_rn(rel, g.bs));
+        c[a] = min(max(v, 0), g.D[a] - 1);
+    }
+}
+
+// x of one MG level stored either as float or as FP16 with a per-block float scale.
+struct XStore {
+    float* f = nullptr;        // FP32 storage
+    __half* h = nullptr;       // FP16 storage (mixed precision, MG level >= 1)
+    float* scale = nullptr;    // per-block scale (FP16 storage)
+    __device__ inline float get(uint32_t i, int b) const { return f ? f[i] : __half2float(h[i]) * scale[b]; }
+};
+
+// Warp / block reductions
+__device__ inline float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+__device__ inline double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host-side objects
+// ------------------------------------------------------------------------------------------------
+struct ParticleWork {
+    DBuf<uint32_t> keys, perm, perm2, cell_start, cell_fill, tmp;
+    DBuf<float> soa, soa2;  // 6 SoA arrays: px py pz vx vy vz
+    int64_t n = 0;
+    aw_status ensure(int64_t np, uint32_t ncell);
+};
+
+struct MsbgState {
+    aw_grid_desc desc;
+    Geo geo;
+    int nb = 0;
+    DBuf<uint32_t> level;       // refinement map
+    DBuf<int> res;              // native res per block (0 inactive), after allocate
+    DBuf<uint32_t> off[4];      // level-0 offsets
+    bool allocated = false;
+    uint32_t tot[4] = {0, 0, 0, 0};
+    std::vector<uint32_t> h_level;
+    std::vector<int> h_res;
+    std::vector<uint32_t> h_off[4];
+    DBuf<float> slab;                       // all channels in one allocation
+    float* ch[AW_NUM_CHANNELS_EXT] = {};    // channel pointers into the slab
+    uint32_t ch_count[AW_NUM_CHANNELS_EXT] = {};
+    DBuf<uint32_t> scratch_u32;
+    DBuf<uint8_t> occ;
+    DBuf<int> flag;
+    ParticleWork pw;
+    LevelView view0() const {
+        LevelView v;
+        v.g = geo;
+        v.res = res.p;
+        for (int k = 0; k < 4; ++k) v.off[k] = off[k].p;
+        return v;
+    }
+};
+
+// Exclusive scan of n u32 values into out[0..n] (out[n] = total).  tmp: scan scratch.
+aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<uint32_t>& tmp, cudaStream_t s);
+
+// Particle pipeline (aw_particles.cu)
+aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s);
+aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* cell_start, float* u[3], float* m[3],
+                     float* mom[3], float* cell_count, cudaStream_t s);
+aw_status g2p_launch(MsbgState& G, const float* pos, int pos_stride_soa, float* vel, int vel_soa, int64_t n,
+                     float alpha, const float* un[3], const float* uo[3], cudaStream_t s);
+aw_status sort_core_soa(MsbgState& G, const float* soa_pos, int64_t n, cudaStream_t s);
+aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_soa, const uint32_t* ids_in,
+                     uint32_t* ids_out, cudaStream_t s);
+aw_status advect_launch(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* u[3], cudaStream_t s);
+
+}  // namespace aw
+
+struct aw_msbg {
+    aw::MsbgState st;
+};

@@ -1,0 +1,1469 @@
+// aw_solver.cu — multigrid pressure solver on the MSBG: block red-black smoother, residual,
+// restriction/prolongation, uniform coarse levels, FP64 coarsest solve, FP32 and mixed solves.
+//
+// Reference behaviour followed (paths within the reference project):
+//   Smoother.cuh:23-94    ghost values across blocks (getPressureLevel; T-junction rule D8 fixed)
+//   Smoother.cuh:105-202  smoothActiveBlocks: block parity colouring, <= MAX_BLOCK_ITER block-local
+//                         red-black GS sweeps, early exit at TARGET_RESIDUAL_REDUCTION, activation
+//   Smoother.cuh:249-291  solveLevel: active set per iteration (here device flags, no host sync)
+//   VCycle.cuh:81-131     computeExplicitResidual
+//   MultigridTransfer.cuh:9-102 restriction (8-child sum) / prolongation (injection add)
+//   VCycle.cuh:177-304    init (coarse offsets, Galerkin) and recursive runCycle
+//
+// B200 design: every block-structured kernel is one CTA per block with the block and a one-cell
+// halo staged in shared memory; the smoother runs all its block-local sweeps out of shared
+// memory and touches HBM once per launch.  Uniform coarse levels continue below one cell per
+// block and end in an FP64 dense solve (Cholesky inverse built on the device each setup).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+#include "aw_internal.cuh"
+
+namespace aw {
+
+static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 1) / t); }
+aw_status level_offsets(MsbgState& G, int m, int vanish, uint32_t* d_off4, int* d_res, uint32_t tot[4], cudaStream_t s);
+__global__ void k_galerkin_ref(Geo g, const uint32_t* __restrict__ level, int axis, int dest,
+                               const float* __restrict__ fine, float* __restrict__ coarse,
+                               const uint32_t* __restrict__ foff, const uint32_t* __restrict__ coff);
+
+constexpr int EXACT_CAP = 512;       // largest coarsest system factorised densely
+constexpr int EXACT_POS_CAP = 32768; // largest coarsest grid scanned by the factor kernel
+
+struct MGLevel {
+    bool dense = false;
+    int D[3] = {0, 0, 0};
+    float H = 0.f;
+    bool half = false;  // x stored as FP16 + per-block scale
+    DBuf<int> res;
+    std::vector<int> h_res;
+    DBuf<uint32_t> off[4];
+    uint32_t tot[4] = {0, 0, 0, 0};
+    DBuf<int> list[2];
+    int nlist[2] = {0, 0};
+    int maxres = 0;
+    DBuf<float> W[3], bbar[3];
+    DBuf<uint8_t> fluid;
+    DBuf<float> x, b, r;
+    DBuf<__half> xh;
+    DBuf<float> xscale;
+    DBuf<uint8_t> status[2];
+    size_t ncell() const { return dense ? (size_t)D[0] * D[1] * D[2] : tot[0]; }
+    size_t nface(int a) const {
+        return dense ? (size_t)(D[0] + (a == 0)) * (D[1] + (a == 1)) * (D[2] + (a == 2)) : tot[1 + a];
+    }
+};
+
+}  // namespace aw
+
+struct aw_solver {
+    aw_msbg* g = nullptr;
+    aw_solver_desc d{};
+    std::vector<aw::MGLevel> lv;
+    int nmsbg = 0;
+    // coarsest exact solve
+    bool exact = false;
+    aw::DBuf<double> M, Minv;
+    aw::DBuf<int> ex_idx, ex_n, ex_pos;
+    // level-0 bindings for the current solve
+    float* x0 = nullptr;
+    const float* b0 = nullptr;
+    // mixed precision
+    aw::DBuf<double> p64tmp;
+    aw::DBuf<double> partials, norm;
+    size_t smem_max = 0;
+};
+
+namespace aw {
+
+struct SmoothParams {
+    float omega, target, theta;
+    int iters;
+    int check_fluid;
+};
+
+__host__ __device__ inline int xi3(int x, int y, int z, int R2) { return (x + 1) + R2 * ((y + 1) + R2 * (z + 1)); }
+
+// Ghost value across face (a, s) of cell c in block b: same level -> mirror cell, coarser
+// neighbour -> parent cell, finer neighbour -> mean of the 4 touching cells, outside the domain
+// or absent -> 0 (Dirichlet / air).
+__device__ inline float ghost_val(const LevelView& L, const XStore& x, int b, const int cb[3], const int c[3], int a, int s) {
+    int nc[3] = {cb[0], cb[1], cb[2]};
+    nc[a] += s;
+    if (!inside(L.g, nc)) return 0.f;
+    const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+    const int rn = L.res[n], r = L.res[b];
+    if (!rn) return 0.f;
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    const int na = s > 0 ? 0 : rn - 1;
+    int q[3];
+    q[a] = na;
+    if (rn == r) {
+        q[t1] = c[t1];
+        q[t2] = c[t2];
+        return x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
+    }
+    if (rn < r) {  // coarser neighbour (2:1 grading: rn == r / 2)
+        q[t1] = min(c[t1] >> 1, rn - 1);
+        q[t2] = min(c[t2] >> 1, rn - 1);
+        return x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
+    }
+    float sum = 0.f;  // finer neighbour (rn == 2 r)
+#pragma unroll
+    for (int d1 = 0; d1 < 2; ++d1)
+#pragma unroll
+        for (int d2 = 0; d2 < 2; ++d2) {
+            q[t1] = min(2 * c[t1] + d1, rn - 1);
+            q[t2] = min(2 * c[t2] + d2, rn - 1);
+            sum += x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
+        }
+    return 0.25f * sum;
+}
+
+// Stage x (block + 6 halo faces) into xs[(r+2)^3].
+__device__ inline void stage_x(const LevelView& L, const XStore& x, int b, const int cb[3], int r, float* xs) {
+    const int R2 = r + 2, n3 = r * r * r;
+    const uint32_t oc = L.off[0][b];
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        xs[xi3(cx, cy, cz, R2)] = x.get(oc + i, b);
+    }
+    const int rr = r * r;
+    for (int i = threadIdx.x; i < 6 * rr; i += blockDim.x) {
+        int face = i / rr, rem = i - face * rr;
+        int a = face >> 1, s = (face & 1) ? 1 : -1;
+        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        int c[3];
+        c[a] = s > 0 ? r - 1 : 0;
+        c[t1] = rem % r;
+        c[t2] = rem / r;
+        float v = ghost_val(L, x, b, cb, c, a, s);
+        int q[3] = {c[0], c[1], c[2]};
+        q[a] += s;
+        xs[xi3(q[0], q[1], q[2], R2)] = v;
+    }
+}
+
+__device__ inline float block_max(float v, float* red) {
+    v = warp_max(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        float t = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.f;
+        t = warp_max(t);
+        if (lane == 0) red[32] = t;
+    }
+    __syncthreads();
+    float out = red[32];
+    __syncthreads();
+    return out;
+}
+
+__device__ inline double block_sum(double v, double* red) {
+    v = warp_sum(v);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    double out = 0.0;
+    if (w == 0) {
+        double t = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+        out = warp_sum(t);
+    }
+    __syncthreads();
+    return out;  // valid in thread 0
+}
+
+struct Coef3 {
+    const float* w[3];
+};
+
+// Write a block of x back (FP32, or FP16 with a fresh per-block scale).
+__device__ inline void store_x(const LevelView& L, const XStore& x, int b, int r, const float* xs, float* red) {
+    const int R2 = r + 2, n3 = r * r * r;
+    const uint32_t oc = L.off[0][b];
+    if (x.f) {
+        for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+            int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+            x.f[oc + i] = xs[xi3(cx, cy, cz, R2)];
+        }
+        return;
+    }
+    float m = 0.f;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        m = fmaxf(m, fabsf(xs[xi3(cx, cy, cz, R2)]));
+    }
+    m = block_max(m, red);
+    const float scale = m > 0.f ? m * (1.f / 32768.f) : 0.f;
+    const float inv = m > 0.f ? 32768.f / m : 0.f;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        x.h[oc + i] = __float2half_rn(xs[xi3(cx, cy, cz, R2)] * inv);
+    }
+    if (threadIdx.x == 0) x.scale[b] = scale;
+}
+
+// smoothActiveBlocks (Smoother.cuh:105-202) for one block colour.
+__global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
+                                                const uint8_t* __restrict__ fluid, const int* __restrict__ list,
+                                                const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
+                                                SmoothParams P) {
+    extern __shared__ float sm[];
+    __shared__ float red[33];
+    const int b = list[blockIdx.x];
+    if (!status[b]) return;
+    const int r = L.res[b];
+    const int R2 = r + 2, n3 = r * r * r, nf = (r + 1) * r * r;
+    float* xs = sm;
+    float* bs = xs + R2 * R2 * R2;
+    float* Ws = bs + n3;
+    uint8_t* fs = (uint8_t*)(Ws + 3 * nf);
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const uint32_t oc = L.off[0][b];
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        bs[i] = bvec[oc + i];
+        fs[i] = fluid[oc + i];
+    }
+    for (int i = threadIdx.x; i < 3 * nf; i += blockDim.x) {
+        int a = i / nf;
+        Ws[i] = W.w[a][L.off[1 + a][b] + (i - a * nf)];
+    }
+    stage_x(L, x, b, cb, r, xs);
+    __syncthreads();
+    float init = -1.f, mr = 0.f;
+    const int sy = R2, sz = R2 * R2;
+    for (int bi = 0; bi < P.iters; ++bi) {
+        float lmax = 0.f;
+        for (int col = 0; col < 2; ++col) {
+            for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+                int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+                if (((cx + cy + cz) & 1) != col) continue;
+                if (P.check_fluid && !fs[i]) continue;
+                float wW = Ws[fidx(0, cx, cy, cz, r)];
+                float wE = Ws[fidx(0, cx + 1, cy, cz, r)];
+                float wS = Ws[nf + fidx(1, cx, cy, cz, r)];
+                float wN = Ws[nf + fidx(1, cx, cy + 1, cz, r)];
+                float wB = Ws[2 * nf + fidx(2, cx, cy, cz, r)];
+                float wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, r)];
+                float diag = -(wW + wE + wS + wN + wB + wT);
+                if (fabsf(diag) < 1e-9f) continue;
+                int q = xi3(cx, cy, cz, R2);
+                float xc = xs[q];
+                float Ax = wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] + wB * xs[q - sz] +
+                           wT * xs[q + sz] + diag * xc;
+                float res = bs[i] - Ax;
+                xs[q] = xc + P.omega * (res / diag);
+                lmax = fmaxf(lmax, fabsf(res));
+            }
+            __syncthreads();
+        }
+        mr = block_max(lmax, red);
+        if (bi == 0) init = mr;
+        if (init > 1e-9f && mr < init * P.target) break;
+    }
+    store_x(L, x, b, r, xs, red);
+    if (threadIdx.x == 0 && mr > P.theta) {
+        status_next[b] = 1;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int s = -1; s <= 1; s += 2) {
+                int nc[3] = {cb[0], cb[1], cb[2]};
+                nc[a] += s;
+                if (inside(L.g, nc)) status_next[bidx(L.g, nc[0], nc[1], nc[2])] = 1;
+            }
+    }
+}
+
+// computeExplicitResidual (VCycle.cuh:81-131): r = b - A x on every cell of every listed block
+// (air cells get 0 in FV mode); optional per-block partial sums of r^2.
+__global__ void __launch_bounds__(256) k_residual(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
+                                                  const uint8_t* __restrict__ fluid, const int* __restrict__ list,
+                                                  int check_fluid, float* __restrict__ rout, double* __restrict__ part) {
+    extern __shared__ float sm[];
+    __shared__ double dred[32];
+    const int b = list[blockIdx.x];
+    const int r = L.res[b];
+    const int R2 = r + 2, n3 = r * r * r;
+    float* xs = sm;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    stage_x(L, x, b, cb, r, xs);
+    __syncthreads();
+    const uint32_t oc = L.off[0][b];
+    const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+    const int sy = R2, sz = R2 * R2;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        float rv = 0.f;
+        if (!check_fluid || fluid[oc + i]) {
+            float wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
+            float wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
+            float wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
+            float wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
+            float wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
+            float wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
+            float diag = -(wW + wE + wS + wN + wB + wT);
+            int q = xi3(cx, cy, cz, R2);
+            float Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                       wB * xs[q - sz] + wT * xs[q + sz];
+            rv = bvec[oc + i] - Ax;
+        }
+        rout[oc + i] = rv;
+        acc += (double)rv * (double)rv;
+    }
+    if (part) {
+        double t = block_sum(acc, dred);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+
+// FP64 residual of the outer defect correction: r = b - A p (p in FP64), stored as FP32 into the
+// V-cycle right-hand side, with per-block partial sums of r^2.
+__global__ void __launch_bounds__(256) k_residual64(LevelView L, const double* __restrict__ p,
+                                                    const float* __restrict__ bvec, Coef3 W,
+                                                    const uint8_t* __restrict__ fluid, const int* __restrict__ list,
+                                                    int check_fluid, float* __restrict__ rout, double* __restrict__ part) {
+    extern __shared__ double smd[];
+    __shared__ double dred[32];
+    const int b = list[blockIdx.x];
+    const int r = L.res[b];
+    const int R2 = r + 2, n3 = r * r * r, rr = r * r;
+    double* xs = smd;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const uint32_t oc = L.off[0][b];
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        xs[xi3(cx, cy, cz, R2)] = p[oc + i];
+    }
+    for (int i = threadIdx.x; i < 6 * rr; i += blockDim.x) {
+        int face = i / rr, rem = i - face * rr;
+        int a = face >> 1, s = (face & 1) ? 1 : -1;
+        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        int c[3];
+        c[a] = s > 0 ? r - 1 : 0;
+        c[t1] = rem % r;
+        c[t2] = rem / r;
+        int nc[3] = {cb[0], cb[1], cb[2]};
+        nc[a] += s;
+        double v = 0.0;
+        if (inside(L.g, nc)) {
+            int n = bidx(L.g, nc[0], nc[1], nc[2]);
+            int rn = L.res[n];
+            if (rn) {
+                int q[3];
+                q[a] = s > 0 ? 0 : rn - 1;
+                if (rn == r) {
+                    q[t1] = c[t1];
+                    q[t2] = c[t2];
+                    v = p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
+                } else if (rn < r) {
+                    q[t1] = min(c[t1] >> 1, rn - 1);
+                    q[t2] = min(c[t2] >> 1, rn - 1);
+                    v = p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
+                } else {
+                    for (int d1 = 0; d1 < 2; ++d1)
+                        for (int d2 = 0; d2 < 2; ++d2) {
+                            q[t1] = min(2 * c[t1] + d1, rn - 1);
+                            q[t2] = min(2 * c[t2] + d2, rn - 1);
+                            v += p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
+                        }
+                    v *= 0.25;
+                }
+            }
+        }
+        int q[3] = {c[0], c[1], c[2]};
+        q[a] += s;
+        xs[xi3(q[0], q[1], q[2], R2)] = v;
+    }
+    __syncthreads();
+    const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+    const int sy = R2, sz = R2 * R2;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        double rv = 0.0;
+        if (!check_fluid || fluid[oc + i]) {
+            double wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
+            double wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
+            double wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
+            double wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
+            double wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
+            double wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
+            double diag = -(wW + wE + wS + wN + wB + wT);
+            int q = xi3(cx, cy, cz, R2);
+            double Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                        wB * xs[q - sz] + wT * xs[q + sz];
+            rv = (double)bvec[oc + i] - Ax;
+        }
+        rout[oc + i] = (float)rv;
+        acc += rv * rv;
+    }
+    double t = block_sum(acc, dred);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+__global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] += (double)e[i];
+}
+
+__global__ void k_reduce_sum(const double* __restrict__ part, int n, double* out) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+    double t = block_sum(acc, red);
+    if (threadIdx.x == 0) *out = t;
+}
+
+// sum of b^2 over fluid cells (or all cells)
+__global__ void k_sumsq(const float* __restrict__ v, const uint8_t* __restrict__ fluid, size_t n, int check_fluid,
+                        double* part) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (!check_fluid || fluid[i]) acc += (double)v[i] * (double)v[i];
+    double t = block_sum(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// restrictResidualsKernel (MultigridTransfer.cuh:9-59): 8-child sum, or copy for a block whose
+// resolution stays one cell.  Coarse air cells get 0.
+__global__ void k_restrict(LevelView F, LevelView K, const float* __restrict__ r, float* __restrict__ bc,
+                           const uint8_t* __restrict__ fluid_c, int check_fluid) {
+    const int b = blockIdx.x;
+    const int rc = K.res[b], rf = F.res[b];
+    if (!rc) return;
+    const bool halved = rf == 2 * rc;
+    const uint32_t of = F.off[0][b], oc = K.off[0][b];
+    const int n3 = rc * rc * rc;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int x = i % rc, y = (i / rc) % rc, z = i / (rc * rc);
+        float s;
+        if (halved) {
+            int fx = 2 * x, fy = 2 * y, fz = 2 * z;
+            s = r[of + cidx(fx, fy, fz, rf)];
+            s += r[of + cidx(fx + 1, fy, fz, rf)];
+            s += r[of + cidx(fx, fy + 1, fz, rf)];
+            s += r[of + cidx(fx + 1, fy + 1, fz, rf)];
+            s += r[of + cidx(fx, fy, fz + 1, rf)];
+            s += r[of + cidx(fx + 1, fy, fz + 1, rf)];
+            s += r[of + cidx(fx, fy + 1, fz + 1, rf)];
+            s += r[of + cidx(fx + 1, fy + 1, fz + 1, rf)];
+        } else {
+            s = r[of + i];
+        }
+        bc[oc + i] = (!check_fluid || fluid_c[oc + i]) ? s : 0.f;
+    }
+}
+
+// prolongateCorrection (MultigridTransfer.cuh:63-102): x_f += x_c[parent] on fluid cells.
+__global__ void __launch_bounds__(256) k_prolong(LevelView F, LevelView K, XStore xf, XStore xc,
+                                                 const uint8_t* __restrict__ fluid_f, int check_fluid) {
+    extern __shared__ float sm[];
+    __shared__ float red[33];
+    const int b = blockIdx.x;
+    const int rc = K.res[b], rf = F.res[b];
+    if (!rc || !rf) return;
+    const bool halved = rf == 2 * rc;
+    const uint32_t of = F.off[0][b], oc = K.off[0][b];
+    const int n3 = rf * rf * rf;
+    if (xf.f) {
+        for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+            if (check_fluid && !fluid_f[of + i]) continue;
+            int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
+            uint32_t ci = halved ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
+            xf.f[of + i] += xc.get(oc + ci, b);
+        }
+        return;
+    }
+    // FP16 fine storage: decode, add, re-encode with a new block scale
+    const int R2 = rf + 2;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
+        float v = xf.get(of + i, b);
+        if (!check_fluid || fluid_f[of + i]) {
+            uint32_t ci = halved ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
+            v += xc.get(oc + ci, b);
+        }
+        sm[xi3(x, y, z, R2)] = v;
+    }
+    __syncthreads();
+    store_x(F, xf, b, rf, sm, red);
+}
+
+__global__ void k_zero_scale(float* s, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) s[i] = 0.f;
+}
+
+// ---------------------------------- uniform (dense) levels ------------------------------------
+struct DenseArgs {
+    DenseView d;
+    const float* W[3];
+    const uint8_t* fluid;
+};
+
+__device__ inline float dense_nb(const DenseView& d, const float* x, int i, int j, int k, int a, int s) {
+    int q[3] = {i, j, k};
+    q[a] += s;
+    if (q[a] < 0 || q[a] >= d.D[a]) return 0.f;
+    return x[didx(d, q[0], q[1], q[2])];
+}
+
+__device__ inline float dense_Ax(const DenseArgs& A, const float* x, int i, int j, int k, float* diag_out) {
+    const DenseView& d = A.d;
+    float wW = A.W[0][dfidx(d, 0, i, j, k)], wE = A.W[0][dfidx(d, 0, i + 1, j, k)];
+    float wS = A.W[1][dfidx(d, 1, i, j, k)], wN = A.W[1][dfidx(d, 1, i, j + 1, k)];
+    float wB = A.W[2][dfidx(d, 2, i, j, k)], wT = A.W[2][dfidx(d, 2, i, j, k + 1)];
+    float diag = -(wW + wE + wS + wN + wB + wT);
+    *diag_out = diag;
+    return wW * dense_nb(d, x, i, j, k, 0, -1) + wE * dense_nb(d, x, i, j, k, 0, 1) + wS * dense_nb(d, x, i, j, k, 1, -1) +
+           wN * dense_nb(d, x, i, j, k, 1, 1) + wB * dense_nb(d, x, i, j, k, 2, -1) + wT * dense_nb(d, x, i, j, k, 2, 1) +
+           diag * x[didx(d, i, j, k)];
+}
+
+__global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ b, int col, float omega) {
+    const DenseView& d = A.d;
+    int n = d.D[0] * d.D[1] * d.D[2];
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
+    if (((i + j + k) & 1) != col || !A.fluid[t]) return;
+    float diag;
+    float ax = dense_Ax(A, x, i, j, k, &diag);
+    if (fabsf(diag) < 1e-30f) return;
+    x[t] += omega * (b[t] - ax) / diag;
+}
+
+__global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const float* __restrict__ b, float* r) {
+    const DenseView& d = A.d;
+    int n = d.D[0] * d.D[1] * d.D[2];
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
+    float diag;
+    r[t] = A.fluid[t] ? b[t] - dense_Ax(A, x, i, j, k, &diag) : 0.f;
+}
+
+// restriction into a dense level from the one-cell-per-block MSBG level (first) or a dense level
+__global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_c, float* __restrict__ bc, int from_msbg,
+                                 LevelView F, DenseView Fd, const float* __restrict__ rf) {
+    int n = K.D[0] * K.D[1] * K.D[2];
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int i = t % K.D[0], j = (t / K.D[0]) % K.D[1], k = t / (K.D[0] * K.D[1]);
+    float s = 0.f;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                int ci = 2 * i + dx, cj = 2 * j + dy, ck = 2 * k + dz;
+                if (from_msbg) {
+                    int b = bidx(F.g, ci, cj, ck);
+                    if (F.res[b]) s += rf[F.off[0][b]];
+                } else {
+                    s += rf[didx(Fd, ci, cj, ck)];
+                }
+            }
+    bc[t] = fluid_c[t] ? s : 0.f;
+}
+
+__global__ void k_dense_prolong(DenseView K, const float* __restrict__ xc, int to_msbg, LevelView F, XStore xf_msbg,
+                                DenseView Fd, float* __restrict__ xf, const uint8_t* __restrict__ fluid_f) {
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (to_msbg) {
+        if (t >= F.g.nb) return;
+        if (!F.res[t]) return;
+        uint32_t ci = F.off[0][t];
+        if (!fluid_f[ci]) return;
+        int c[3];
+        bcoord(F.g, t, c);
+        xf_msbg.f[ci] += xc[didx(K, c[0] >> 1, c[1] >> 1, c[2] >> 1)];
+    } else {
+        int n = Fd.D[0] * Fd.D[1] * Fd.D[2];
+        if (t >= n) return;
+        if (!fluid_f[t]) return;
+        int i = t % Fd.D[0], j = (t / Fd.D[0]) % Fd.D[1], k = t / (Fd.D[0] * Fd.D[1]);
+        xf[t] += xc[didx(K, i >> 1, j >> 1, k >> 1)];
+    }
+}
+
+// ------------------------------- hierarchy setup kernels --------------------------------------
+// coarse fluid flags: a coarse cell is fluid iff all of its children are fluid (copy when the
+// block keeps one cell)
+__global__ void k_coarse_fluid(LevelView F, LevelView K, const uint8_t* __restrict__ ff, uint8_t* __restrict__ fc) {
+    const int b = blockIdx.x;
+    const int rc = K.res[b], rf = F.res[b];
+    if (!rc) return;
+    const bool halved = rf == 2 * rc;
+    const uint32_t of = F.off[0][b], oc = K.off[0][b];
+    const int n3 = rc * rc * rc;
+    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
+        int x = i % rc, y = (i / rc) % rc, z = i / (rc * rc);
+        uint8_t f = 1;
+        if (halved) {
+            for (int dz = 0; dz < 2; ++dz)
+                for (int dy = 0; dy < 2; ++dy)
+                    for (int dx = 0; dx < 2; ++dx) f &= ff[of + cidx(2 * x + dx, 2 * y + dy, 2 * z + dz, rf)];
+        } else {
+            f = ff[of + i];
+        }
+        fc[oc + i] = f;
+    }
+}
+
+// coarse 1/rho per face: mean of the 4 fine faces (copy when the block keeps one cell)
+__global__ void k_coarse_bbar(LevelView F, LevelView K, int a, const float* __restrict__ bf, float* __restrict__ bcv) {
+    const int b = blockIdx.x;
+    const int rc = K.res[b], rf = F.res[b];
+    if (!rc) return;
+    const bool halved = rf == 2 * rc;
+    const int nf = (rc + 1) * rc * rc;
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+        int f[3];
+        if (a == 0) { f[0] = i % (rc + 1); int rem = i / (rc + 1); f[1] = rem % rc; f[2] = rem / rc; }
+        else if (a == 1) { f[0] = i % rc; int rem = i / rc; f[1] = rem % (rc + 1); f[2] = rem / (rc + 1); }
+        else { f[0] = i % rc; int rem = i / rc; f[1] = rem % rc; f[2] = rem / rc; }
+        float v;
+        if (halved) {
+            float s = 0.f;
+            for (int d1 = 0; d1 < 2; ++d1)
+                for (int d2 = 0; d2 < 2; ++d2) {
+                    int q[3];
+                    q[a] = 2 * f[a];
+                    q[t1] = 2 * f[t1] + d1;
+                    q[t2] = 2 * f[t2] + d2;
+                    s += bf[F.off[1 + a][b] + fidx(a, q[0], q[1], q[2], rf)];
+                }
+            v = 0.25f * s;
+        } else {
+            v = bf[F.off[1 + a][b] + i];
+        }
+        bcv[K.off[1 + a][b] + i] = v;
+    }
+}
+
+// finite-volume conductance W = geo * bbar: interior h, wall 0, absent neighbour h (Dirichlet),
+// same level h, coarser neighbour (2/3) h, finer neighbour (4/3) h  (h = the block's cell size)
+__global__ void k_conductance(LevelView L, int a, const float* __restrict__ bbar, float* __restrict__ W) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const float H = L.g.bs / (float)r;
+    const int nf = (r + 1) * r * r;
+    float gl = H, gh = H;
+    for (int s = -1; s <= 1; s += 2) {
+        int nc[3] = {cb[0], cb[1], cb[2]};
+        nc[a] += s;
+        float gv;
+        if (!inside(L.g, nc)) gv = 0.f;
+        else {
+            int rn = L.res[bidx(L.g, nc[0], nc[1], nc[2])];
+            if (rn == 0 || rn == r) gv = H;
+            else if (2 * rn == r) gv = (2.f / 3.f) * H;
+            else gv = (4.f / 3.f) * H;
+        }
+        if (s < 0) gl = gv;
+        else gh = gv;
+    }
+    for (int i = threadIdx.x; i < nf; i += blockDim.x) {
+        int fa;
+        if (a == 0) fa = i % (r + 1);
+        else if (a == 1) fa = (i / r) % (r + 1);
+        else fa = i / (r * r);
+        float geo = fa == 0 ? gl : (fa == r ? gh : H);
+        W[L.off[1 + a][b] + i] = geo * bbar[L.off[1 + a][b] + i];
+    }
+}
+
+__global__ void k_dense_fluid(DenseView K, int from_msbg, LevelView F, const uint8_t* __restrict__ ff, DenseView Fd,
+                              uint8_t* __restrict__ fc) {
+    int n = K.D[0] * K.D[1] * K.D[2];
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int i = t % K.D[0], j = (t / K.D[0]) % K.D[1], k = t / (K.D[0] * K.D[1]);
+    uint8_t f = 1;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                int ci = 2 * i + dx, cj = 2 * j + dy, ck = 2 * k + dz;
+                uint8_t c;
+                if (from_msbg) {
+                    int b = bidx(F.g, ci, cj, ck);
+                    c = F.res[b] ? ff[F.off[0][b]] : 0;
+                } else {
+                    c = ff[didx(Fd, ci, cj, ck)];
+                }
+                f &= c;
+            }
+    fc[t] = f;
+}
+
+__global__ void k_dense_conductance(DenseView K, int a, float H, float* W) {
+    int n = (K.D[0] + (a == 0)) * (K.D[1] + (a == 1)) * (K.D[2] + (a == 2));
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int dx = K.D[0] + (a == 0), dy = K.D[1] + (a == 1);
+    int f[3] = {t % dx, (t / dx) % dy, t / (dx * dy)};
+    W[t] = (f[a] == 0 || f[a] == K.D[a]) ? 0.f : H;
+}
+
+// ------------------------------- coarsest FP64 dense solve ------------------------------------
+// The coarsest level is a uniform grid (dense level, or the one-cell-per-block MSBG level).
+struct Uniform {
+    int D[3];
+    int msbg;
+    LevelView L;       // msbg == 1
+    DenseArgs A;       // msbg == 0
+    const uint8_t* fluid;
+};
+
+__device__ inline int uni_cell(const Uniform& U, int p) {  // cell index of grid position p, or -1
+    if (!U.msbg) return p;
+    return U.L.res[p] ? (int)U.L.off[0][p] : -1;
+}
+__device__ inline float uni_W(const Uniform& U, int p, int a, int hi) {
+    if (!U.msbg) {
+        int c[3] = {p % U.D[0], (p / U.D[0]) % U.D[1], p / (U.D[0] * U.D[1])};
+        c[a] += hi;
+        return U.A.W[a][dfidx(U.A.d, a, c[0], c[1], c[2])];
+    }
+    return U.A.W[a][U.L.off[1 + a][p] + hi];
+}
+
+// One CTA: enumerate fluid cells, assemble -A, regularise Neumann components, Cholesky, and
+// write Minv = -( -A + reg )^-1 so that x = Minv b.  ex_n[0] = n (or -1 when n > EXACT_CAP).
+__global__ void __launch_bounds__(512) k_coarse_factor(Uniform U, int* pos_of, int* idx, int* ex_n, double* M,
+                                                       double* Minv) {
+    __shared__ int cnt;
+    __shared__ int lab[EXACT_CAP];
+    __shared__ int dir[EXACT_CAP];
+    __shared__ double dsum[EXACT_CAP];
+    __shared__ int csz[EXACT_CAP];
+    __shared__ int changed;
+    __shared__ double piv;
+    const int np = U.D[0] * U.D[1] * U.D[2];
+    if (threadIdx.x == 0) cnt = 0;
+    __syncthreads();
+    // deterministic compaction: serial order by position (np <= EXACT_POS_CAP)
+    if (threadIdx.x == 0) {
+        int c = 0;
+        for (int p = 0; p < np; ++p) {
+            int ci = uni_cell(U, p);
+            if (ci >= 0 && U.fluid[ci]) {
+                if (c < EXACT_CAP) idx[c] = p;
+                pos_of[p] = c;
+                ++c;
+            } else {
+                pos_of[p] = -1;
+            }
+        }
+        cnt = c;
+    }
+    __syncthreads();
+    const int n = cnt;
+    if (n > EXACT_CAP) {
+        if (threadIdx.x == 0) ex_n[0] = -1;
+        return;
+    }
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) M[t] = 0.0;
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        int p = idx[i];
+        int c[3] = {p % U.D[0], (p / U.D[0]) % U.D[1], p / (U.D[0] * U.D[1])};
+        double diag = 0.0, off = 0.0;
+        for (int a = 0; a < 3; ++a)
+            for (int s = 0; s < 2; ++s) {
+                double w = uni_W(U, p, a, s);
+                diag += w;
+                int q[3] = {c[0], c[1], c[2]};
+                q[a] += s ? 1 : -1;
+                if (q[a] < 0 || q[a] >= U.D[a]) continue;
+                int qp = q[0] + U.D[0] * (q[1] + U.D[1] * q[2]);
+                int j = pos_of[qp];
+                if (j >= 0) {
+                    M[(size_t)i * n + j] -= w;
+                    off += w;
+                }
+            }
+        M[(size_t)i * n + i] += diag;
+        dir[i] = (diag - off) > 1e-12 * diag ? 1 : 0;
+        lab[i] = i;
+    }
+    __syncthreads();
+    // connected components by min-label propagation
+    for (int it = 0; it < n + 1; ++it) {
+        if (threadIdx.x == 0) changed = 0;
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            int l = lab[i];
+            for (int j = 0; j < n; ++j)
+                if (M[(size_t)i * n + j] != 0.0 && j != i && lab[j] < l) l = lab[j];
+            if (l < lab[i]) {
+                lab[i] = l;
+                changed = 1;
+            }
+        }
+        __syncthreads();
+        if (!changed) break;
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        dsum[i] = 0.0;
+        csz[i] = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < n; ++i) {
+            int l = lab[i];
+            dsum[l] += M[(size_t)i * n + i];
+            csz[l] += 1;
+            if (dir[i]) dir[l] = 1;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n * n; t += blockDim.x) {
+        int i = t / n, j = t % n;
+        int l = lab[i];
+        if (lab[j] == l && !dir[l]) M[t] += dsum[l] / ((double)csz[l] * csz[l]);
+    }
+    __syncthreads();
+    // Cholesky (lower, in place)
+    for (int j = 0; j < n; ++j) {
+        if (threadIdx.x == 0) {
+            double s = M[(size_t)j * n + j];
+            for (int k = 0; k < j; ++k) s -= M[(size_t)j * n + k] * M[(size_t)j * n + k];
+            piv = sqrt(fmax(s, 1e-300));
+            M[(size_t)j * n + j] = piv;
+        }
+        __syncthreads();
+        for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+            double t = M[(size_t)i * n + j];
+            for (int k = 0; k < j; ++k) t -= M[(size_t)i * n + k] * M[(size_t)j * n + k];
+            M[(size_t)i * n + j] = t / piv;
+        }
+        __syncthreads();
+    }
+    // inverse, one column per thread
+    for (int col = threadIdx.x; col < n; col += blockDim.x) {
+        for (int i = 0; i < n; ++i) {
+            double t = (i == col) ? 1.0 : 0.0;
+            for (int k = 0; k < i; ++k) t -= M[(size_t)i * n + k] * Minv[(size_t)k * n + col];
+            Minv[(size_t)i * n + col] = t / M[(size_t)i * n + i];
+        }
+        for (int i = n - 1; i >= 0; --i) {
+            double t = Minv[(size_t)i * n + col];
+            for (int k = i + 1; k < n; ++k) t -= M[(size_t)k * n + i] * Minv[(size_t)k * n + col];
+            Minv[(size_t)i * n + col] = t / M[(size_t)i * n + i];
+        }
+        for (int i = 0; i < n; ++i) Minv[(size_t)i * n + col] = -Minv[(size_t)i * n + col];
+    }
+    if (threadIdx.x == 0) ex_n[0] = n;
+}
+
+// x = Minv b on the fluid cells of the coarsest level (FP64 accumulation)
+__global__ void k_coarse_apply(Uniform U, const int* __restrict__ idx, const int* __restrict__ ex_n,
+                               const double* __restrict__ Minv, const float* __restrict__ b, float* __restrict__ x) {
+    const int n = ex_n[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int j = 0; j < n; ++j) s += Minv[(size_t)i * n + j] * (double)b[uni_cell(U, idx[j])];
+        x[uni_cell(U, idx[i])] = (float)s;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host orchestration
+// ------------------------------------------------------------------------------------------------
+static LevelView lview(const aw_solver* S, int m) {
+    const MsbgState& G = S->g->st;
+    const MGLevel& L = S->lv[m];
+    LevelView v;
+    v.g = G.geo;
+    v.res = L.res.p;
+    for (int k = 0; k < 4; ++k) v.off[k] = L.off[k].p;
+    return v;
+}
+static DenseView dview(const MGLevel& L) {
+    DenseView d;
+    d.D[0] = L.D[0];
+    d.D[1] = L.D[1];
+    d.D[2] = L.D[2];
+    return d;
+}
+static XStore xstore(aw_solver* S, int m) {
+    MGLevel& L = S->lv[m];
+    XStore x;
+    if (m == 0 && S->x0) {
+        x.f = S->x0;
+        return x;
+    }
+    if (L.half) {
+        x.h = L.xh.p;
+        x.scale = L.xscale.p;
+    } else {
+        x.f = L.x.p;
+    }
+    return x;
+}
+static const float* bptr(aw_solver* S, int m) { return (m == 0 && S->b0) ? S->b0 : S->lv[m].b.p; }
+static Coef3 coef(const MGLevel& L) { return Coef3{{L.W[0].p, L.W[1].p, L.W[2].p}}; }
+static size_t smooth_smem(int r) {
+    return (size_t)((r + 2) * (r + 2) * (r + 2) + r * r * r + 3 * (r + 1) * r * r) * sizeof(float) + (size_t)r * r * r + 16;
+}
+static bool fv(const aw_solver* S) { return S->d.operator_mode == AW_OPERATOR_FV; }
+
+static Uniform uniform_of(aw_solver* S, int m) {
+    MGLevel& L = S->lv[m];
+    Uniform U{};
+    if (L.dense) {
+        for (int a = 0; a < 3; ++a) U.D[a] = L.D[a];
+        U.msbg = 0;
+    } else {
+        for (int a = 0; a < 3; ++a) U.D[a] = S->g->st.geo.D[a];
+        U.msbg = 1;
+        U.L = lview(S, m);
+    }
+    U.A.d = dview(L);
+    for (int a = 0; a < 3; ++a) U.A.W[a] = L.W[a].p;
+    U.A.fluid = L.fluid.p;
+    U.fluid = L.fluid.p;
+    return U;
+}
+
+static aw_status zero_x(aw_solver* S, int m, cudaStream_t s) {
+    MGLevel& L = S->lv[m];
+    if (L.half) {
+        AW_CUDA(cudaMemsetAsync(L.xh.p, 0, L.ncell() * sizeof(__half), s));
+        AW_CUDA(cudaMemsetAsync(L.xscale.p, 0, S->g->st.nb * sizeof(float), s));
+    } else if (m == 0 && S->x0) {
+        AW_CUDA(cudaMemsetAsync(S->x0, 0, L.ncell() * sizeof(float), s));
+    } else {
+        AW_CUDA(cudaMemsetAsync(L.x.p, 0, L.ncell() * sizeof(float), s));
+    }
+    return AW_OK;
+}
+
+static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t s) {
+    MGLevel& L = S->lv[m];
+    const int cf = fv(S) ? 1 : 0;
+    if (L.dense) {
+        DenseArgs A{dview(L), {L.W[0].p, L.W[1].p, L.W[2].p}, L.fluid.p};
+        size_t n = L.ncell();
+        for (int it = 0; it < iterations; ++it)
+            for (int col = 0; col < 2; ++col) {
+                k_dense_smooth<<<nblk(n), 256, 0, s>>>(A, L.x.p, L.b.p, col, S->d.omega);
+                AW_LAUNCH();
+            }
+        return AW_OK;
+    }
+    const int nb = S->g->st.nb;
+    AW_CUDA(cudaMemsetAsync(L.status[0].p, 1, nb, s));
+    SmoothParams P{S->d.omega, S->d.target_reduction, S->d.theta, S->d.block_iterations, cf};
+    LevelView V = lview(S, m);
+    XStore x = xstore(S, m);
+    size_t smem = smooth_smem(L.maxres);
+    int cur = 0;
+    for (int it = 0; it < iterations; ++it) {
+        AW_CUDA(cudaMemsetAsync(L.status[cur ^ 1].p, 0, nb, s));
+        for (int rb = 0; rb < 2; ++rb) {
+            if (!L.nlist[rb]) continue;
+            k_smooth<<<L.nlist[rb], 256, smem, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, L.list[rb].p, L.status[cur].p,
+                                                    L.status[cur ^ 1].p, P);
+            AW_LAUNCH();
+        }
+        cur ^= 1;
+    }
+    return AW_OK;
+}
+
+static aw_status residual_level(aw_solver* S, int m, double* part, cudaStream_t s) {
+    MGLevel& L = S->lv[m];
+    const int cf = fv(S) ? 1 : 0;
+    if (L.dense) {
+        DenseArgs A{dview(L), {L.W[0].p, L.W[1].p, L.W[2].p}, L.fluid.p};
+        k_dense_residual<<<nblk(L.ncell()), 256, 0, s>>>(A, L.x.p, L.b.p, L.r.p);
+        AW_LAUNCH();
+        return AW_OK;
+    }
+    LevelView V = lview(S, m);
+    XStore x = xstore(S, m);
+    size_t smem = (size_t)(L.maxres + 2) * (L.maxres + 2) * (L.maxres + 2) * sizeof(float);
+    int off = 0;
+    for (int rb = 0; rb < 2; ++rb) {
+        if (!L.nlist[rb]) continue;
+        k_residual<<<L.nlist[rb], 256, smem, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, L.list[rb].p, cf, L.r.p,
+                                                  part ? part + off : nullptr);
+        AW_LAUNCH();
+        off += L.nlist[rb];
+    }
+    return AW_OK;
+}
+
+static aw_status restrict_level(aw_solver* S, int m, cudaStream_t s) {
+    MGLevel& F = S->lv[m];
+    MGLevel& K = S->lv[m + 1];
+    const int cf = fv(S) ? 1 : 0;
+    if (K.dense) {
+        LevelView Fv = F.dense ? LevelView{} : lview(S, m);
+        if (F.dense) Fv.g = S->g->st.geo;
+        k_dense_restrict<<<nblk(K.ncell()), 256, 0, s>>>(dview(K), K.fluid.p, K.b.p, F.dense ? 0 : 1, Fv, dview(F), F.r.p);
+        AW_LAUNCH();
+        return AW_OK;
+    }
+    k_restrict<<<S->g->st.nb, 128, 0, s>>>(lview(S, m), lview(S, m + 1), F.r.p, K.b.p, K.fluid.p, cf);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+static aw_status prolong_level(aw_solver* S, int m, cudaStream_t s) {
+    MGLevel& F = S->lv[m];
+    MGLevel& K = S->lv[m + 1];
+    const int cf = fv(S) ? 1 : 0;
+    if (K.dense) {
+        LevelView Fv = F.dense ? LevelView{} : lview(S, m);
+        if (F.dense) Fv.g = S->g->st.geo;
+        size_t n = F.dense ? F.ncell() : (size_t)S->g->st.nb;
+        XStore xf = F.dense ? XStore{} : xstore(S, m);
+        AW_CHECK_ARG(F.dense || xf.f, "FP16 storage on the one-cell MSBG level is not supported");
+        k_dense_prolong<<<nblk(n), 256, 0, s>>>(dview(K), K.x.p, F.dense ? 0 : 1, Fv, xf, dview(F), F.x.p, F.fluid.p);
+        AW_LAUNCH();
+        return AW_OK;
+    }
+    size_t smem = F.half ? (size_t)(F.maxres + 2) * (F.maxres + 2) * (F.maxres + 2) * sizeof(float) : 0;
+    k_prolong<<<S->g->st.nb, 256, smem, s>>>(lview(S, m), lview(S, m + 1), xstore(S, m), xstore(S, m + 1), F.fluid.p, cf);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+static aw_status coarsest(aw_solver* S, int m, cudaStream_t s) {
+    MGLevel& L = S->lv[m];
+    if (fv(S) && S->exact) {
+        Uniform U = uniform_of(S, m);
+        float* x = L.dense ? L.x.p : (m == 0 && S->x0 ? S->x0 : L.x.p);
+        k_coarse_apply<<<4, 128, 0, s>>>(U, S->ex_idx.p, S->ex_n.p, S->Minv.p, bptr(S, m), x);
+        AW_LAUNCH();
+        return AW_OK;
+    }
+    return smooth_level(S, m, S->d.coarsest_iterations, s);
+}
+
+static aw_status vcycle(aw_solver* S, int m, cudaStream_t s) {
+    const int last = (int)S->lv.size() - 1;
+    if (m == last) return coarsest(S, m, s);
+    MGLevel& L = S->lv[m];
+    AW_TRY(smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.pre_smooth, s));
+    AW_TRY(residual_level(S, m, nullptr, s));
+    AW_TRY(restrict_level(S, m, s));
+    AW_TRY(zero_x(S, m + 1, s));
+    AW_TRY(vcycle(S, m + 1, s));
+    AW_TRY(prolong_level(S, m, s));
+    AW_TRY(smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.post_smooth, s));
+    return AW_OK;
+}
+
+}  // namespace aw
+
+using namespace aw;
+
+// ================================================================================================
+// C ABI
+// ================================================================================================
+extern "C" aw_status aw_solver_default_desc(int32_t mode, aw_solver_desc* d) {
+    AW_CHECK_ARG(d && (mode == AW_OPERATOR_FV || mode == AW_OPERATOR_REFERENCE), "bad argument");
+    memset(d, 0, sizeof *d);
+    d->operator_mode = mode;
+    d->precision = AW_PRECISION_FP32;
+    d->mg_levels = 0;
+    d->pre_smooth = 2;
+    d->post_smooth = 2;
+    d->coarsest_iterations = 50;
+    d->dense_sweeps = 2;
+    d->max_cycles = 100;
+    d->tolerance = 1e-6;
+    if (mode == AW_OPERATOR_REFERENCE) {
+        d->block_iterations = 10;     // MAX_BLOCK_ITER
+        d->omega = 0.85714f;          // OMEGA
+        d->target_reduction = 0.33f;  // TARGET_RESIDUAL_REDUCTION
+        d->theta = 1e-4f;             // Smoother.cuh:286
+    } else {
+        d->block_iterations = 2;
+        d->omega = 1.0f;
+        d->target_reduction = 0.33f;
+        d->theta = 0.0f;
+    }
+    return AW_OK;
+}
+
+static int ilog2(int v) {
+    int l = 0;
+    while ((1 << l) < v) ++l;
+    return l;
+}
+
+extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_solver** out) {
+    AW_CHECK_ARG(g && d && out, "null argument");
+    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
+    AW_CHECK_ARG(d->operator_mode == AW_OPERATOR_FV || d->operator_mode == AW_OPERATOR_REFERENCE, "bad operator mode");
+    AW_CHECK_ARG(d->precision == AW_PRECISION_FP32 || d->precision == AW_PRECISION_MIXED, "bad precision");
+    AW_CHECK_ARG(d->block_iterations >= 1 && d->pre_smooth >= 0 && d->post_smooth >= 0, "bad smoother settings");
+    *out = nullptr;
+    MsbgState& G = g->st;
+    {  // the stencils assume 2:1 grading between face neighbours
+        const Geo& geo = G.geo;
+        for (int b = 0; b < G.nb; ++b) {
+            if ((int)G.h_level[b] >= geo.L) continue;
+            int c[3];
+            bcoord(geo, b, c);
+            for (int a = 0; a < 3; ++a) {
+                int nc[3] = {c[0], c[1], c[2]};
+                nc[a] += 1;
+                if (!inside(geo, nc)) continue;
+                uint32_t nl = G.h_level[bidx(geo, nc[0], nc[1], nc[2])];
+                if ((int)nl < geo.L && std::abs((int)nl - (int)G.h_level[b]) > 1)
+                    return set_error(AW_ERR_INVALID_ARGUMENT,
+                                     "level map is not 2:1 graded (block %d); run aw_msbg_enforce_grading first", b);
+            }
+        }
+    }
+    std::unique_ptr<aw_solver> S(new aw_solver());
+    S->g = g;
+    S->d = *d;
+    const bool ref = d->operator_mode == AW_OPERATOR_REFERENCE;
+    const int nb = G.nb;
+    int M = d->mg_levels > 0 ? d->mg_levels : (ref ? G.geo.L : ilog2(G.geo.R0) + 1);
+    if (!ref) M = std::min(M, ilog2(G.geo.R0) + 1);
+    cudaStream_t s = 0;
+    S->lv.resize(M);
+    for (int m = 0; m < M; ++m) {
+        MGLevel& L = S->lv[m];
+        AW_TRY(L.res.alloc(nb));
+        DBuf<uint32_t> off4;
+        AW_TRY(off4.alloc(4 * (size_t)nb));
+        AW_TRY(level_offsets(G, m, ref ? 1 : 0, off4.p, L.res.p, L.tot, s));
+        for (int k = 0; k < 4; ++k) {
+            AW_TRY(L.off[k].alloc(nb));
+            AW_CUDA(cudaMemcpy(L.off[k].p, off4.p + (size_t)k * nb, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice));
+        }
+        L.h_res.resize(nb);
+        AW_CUDA(cudaMemcpy(L.h_res.data(), L.res.p, nb * sizeof(int), cudaMemcpyDeviceToHost));
+        std::vector<int> lists[2];
+        for (int b = 0; b < nb; ++b) {
+            if (!L.h_res[b]) continue;
+            int c[3];
+            bcoord(G.geo, b, c);
+            lists[(c[0] + c[1] + c[2]) & 1].push_back(b);
+            L.maxres = std::max(L.maxres, L.h_res[b]);
+        }
+        if (L.maxres == 0) {
+            S->lv.resize(m);
+            break;
+        }
+        for (int rb = 0; rb < 2; ++rb) {
+            L.nlist[rb] = (int)lists[rb].size();
+            if (L.nlist[rb]) {
+                AW_TRY(L.list[rb].alloc(L.nlist[rb]));
+                AW_CUDA(cudaMemcpy(L.list[rb].p, lists[rb].data(), L.nlist[rb] * sizeof(int), cudaMemcpyHostToDevice));
+            }
+        }
+        AW_TRY(L.status[0].alloc(nb));
+        AW_TRY(L.status[1].alloc(nb));
+        L.half = (d->precision == AW_PRECISION_MIXED) && m >= 1 && m < M - 1 + (ref ? 0 : 1) && L.maxres > 1;
+        size_t nc = L.ncell();
+        AW_TRY(L.x.alloc(nc));
+        AW_TRY(L.b.alloc(nc));
+        AW_TRY(L.r.alloc(nc));
+        AW_TRY(L.fluid.alloc(nc));
+        AW_CUDA(cudaMemset(L.x.p, 0, nc * sizeof(float)));
+        AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
+        AW_CUDA(cudaMemset(L.fluid.p, 1, nc));
+        if (L.half) {
+            AW_TRY(L.xh.alloc(nc));
+            AW_TRY(L.xscale.alloc(nb));
+            AW_CUDA(cudaMemset(L.xh.p, 0, nc * sizeof(__half)));
+            AW_CUDA(cudaMemset(L.xscale.p, 0, nb * sizeof(float)));
+        }
+        for (int a = 0; a < 3; ++a) {
+            AW_TRY(L.W[a].alloc(L.nface(a)));
+            AW_TRY(L.bbar[a].alloc(L.nface(a)));
+        }
+        S->smem_max = std::max(S->smem_max, smooth_smem(L.maxres));
+    }
+    S->nmsbg = (int)S->lv.size();
+    // coefficients of the block-structured levels
+    for (int m = 0; m < S->nmsbg; ++m) {
+        MGLevel& L = S->lv[m];
+        LevelView V = lview(S.get(), m);
+        for (int a = 0; a < 3; ++a) {
+            if (m == 0) {
+                AW_CUDA(cudaMemcpy(L.bbar[a].p, G.ch[AW_BETA_COEFF_X + a], L.nface(a) * sizeof(float),
+                                   cudaMemcpyDeviceToDevice));
+            } else {
+                k_coarse_bbar<<<nb, 128>>>(lview(S.get(), m - 1), V, a, S->lv[m - 1].bbar[a].p, L.bbar[a].p);
+                AW_LAUNCH();
+            }
+            if (ref) {
+                if (m == 0) {
+                    AW_CUDA(cudaMemcpy(L.W[a].p, L.bbar[a].p, L.nface(a) * sizeof(float), cudaMemcpyDeviceToDevice));
+                } else {
+                    AW_CUDA(cudaMemset(L.W[a].p, 0, L.nface(a) * sizeof(float)));
+                    k_galerkin_ref<<<nb, 256>>>(G.geo, G.level.p, a, m, S->lv[m - 1].W[a].p, L.W[a].p,
+                                                S->lv[m - 1].off[1 + a].p, L.off[1 + a].p);
+                    AW_LAUNCH();
+                }
+            } else {
+                k_conductance<<<nb, 128>>>(V, a, L.bbar[a].p, L.W[a].p);
+                AW_LAUNCH();
+            }
+        }
+    }
+    // uniform continuation below one cell per block (FV mode)
+    if (!ref && S->nmsbg > 0 && S->lv.back().maxres == 1) {
+        int Dd[3] = {G.geo.D[0], G.geo.D[1], G.geo.D[2]};
+        float H = G.geo.bs;
+        while (Dd[0] % 2 == 0 && Dd[1] % 2 == 0 && Dd[2] % 2 == 0 && (long)Dd[0] * Dd[1] * Dd[2] > 64) {
+            S->lv.emplace_back();
+            MGLevel& L = S->lv.back();
+            L.dense = true;
+            for (int a = 0; a < 3; ++a) L.D[a] = Dd[a] / 2;
+            H *= 2.f;
+            L.H = H;
+            size_t nc = L.ncell();
+            AW_TRY(L.x.alloc(nc));
+            AW_TRY(L.b.alloc(nc));
+            AW_TRY(L.r.alloc(nc));
+            AW_TRY(L.fluid.alloc(nc));
+            AW_CUDA(cudaMemset(L.x.p, 0, nc * sizeof(float)));
+            AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
+            for (int a = 0; a < 3; ++a) {
+                AW_TRY(L.W[a].alloc(L.nface(a)));
+                k_dense_conductance<<<nblk(L.nface(a)), 256>>>(dview(L), a, H, L.W[a].p);
+                AW_LAUNCH();
+            }
+            for (int a = 0; a < 3; ++a) Dd[a] /= 2;
+        }
+        // the coarsest level is uniform: factorise it densely when small enough
+        MGLevel& C = S->lv.back();
+        size_t npos = C.dense ? C.ncell() : (size_t)nb;
+        if (npos <= (size_t)EXACT_POS_CAP) {
+            AW_TRY(S->M.alloc((size_t)EXACT_CAP * EXACT_CAP));
+            AW_TRY(S->Minv.alloc((size_t)EXACT_CAP * EXACT_CAP));
+            AW_TRY(S->ex_idx.alloc(EXACT_CAP));
+            AW_TRY(S->ex_pos.alloc(npos));
+            AW_TRY(S->ex_n.alloc(1));
+            AW_CUDA(cudaMemset(S->ex_n.p, 0, sizeof(int)));
+            S->exact = true;
+        }
+    }
+    if (S->smem_max > 48 * 1024) {
+        AW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
+        AW_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
+        AW_CUDA(cudaFuncSetAttribute(k_prolong, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
+        AW_CUDA(cudaFuncSetAttribute(k_residual64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S->smem_max)));
+    }
+    size_t nparts = (size_t)nb + 1024;
+    AW_TRY(S->partials.alloc(nparts));
+    AW_TRY(S->norm.alloc(2));
+    AW_CUDA(cudaDeviceSynchronize());
+    *out = S.release();
+    // default setup: every cell fluid
+    return aw_solver_setup(*out, nullptr, 0);
+}
+
+extern "C" aw_status aw_solver_destroy(aw_solver* sv) {
+    delete sv;
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solver_setup(aw_solver* S, const uint8_t* d_fluid, aw_stream s_) {
+    AW_CHECK_ARG(S, "null solver");
+    cudaStream_t s = (cudaStream_t)s_;
+    MsbgState& G = S->g->st;
+    MGLevel& L0 = S->lv[0];
+    if (d_fluid) AW_CUDA(cudaMemcpyAsync(L0.fluid.p, d_fluid, L0.ncell(), cudaMemcpyDeviceToDevice, s));
+    else AW_CUDA(cudaMemsetAsync(L0.fluid.p, 1, L0.ncell(), s));
+    for (int m = 1; m < (int)S->lv.size(); ++m) {
+        MGLevel& L = S->lv[m];
+        MGLevel& F = S->lv[m - 1];
+        if (!L.dense) {
+            k_coarse_fluid<<<G.nb, 128, 0, s>>>(lview(S, m - 1), lview(S, m), F.fluid.p, L.fluid.p);
+        } else {
+            LevelView Fv = F.dense ? LevelView{} : lview(S, m - 1);
+            if (F.dense) Fv.g = G.geo;
+            k_dense_fluid<<<nblk(L.ncell()), 256, 0, s>>>(dview(L), F.dense ? 0 : 1, Fv, F.fluid.p, dview(F), L.fluid.p);
+        }
+        AW_LAUNCH();
+    }
+    if (S->exact) {
+        Uniform U = uniform_of(S, (int)S->lv.size() - 1);
+        k_coarse_factor<<<1, 512, 0, s>>>(U, S->ex_pos.p, S->ex_idx.p, S->ex_n.p, S->M.p, S->Minv.p);
+        AW_LAUNCH();
+    }
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solver_num_levels(const aw_solver* S, int32_t* n) {
+    AW_CHECK_ARG(S && n, "null argument");
+    *n = (int32_t)S->lv.size();
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solver_level_array(aw_solver* S, int32_t m, int32_t which, void** p, uint32_t* count) {
+    AW_CHECK_ARG(S && p && m >= 0 && m < (int)S->lv.size(), "bad argument");
+    MGLevel& L = S->lv[m];
+    uint32_t c = 0;
+    void* q = nullptr;
+    switch (which) {
+        case 0: q = L.half ? (void*)L.xh.p : (void*)L.x.p; c = (uint32_t)L.ncell(); break;
+        case 1: q = L.b.p; c = (uint32_t)L.ncell(); break;
+        case 2: q = L.r.p; c = (uint32_t)L.ncell(); break;
+        case 3: case 4: case 5: q = L.W[which - 3].p; c = (uint32_t)L.nface(which - 3); break;
+        case 6: q = L.fluid.p; c = (uint32_t)L.ncell(); break;
+        case 7: case 8: case 9: case 10:
+            AW_CHECK_ARG(!L.dense, "offsets exist on block-structured levels only");
+            q = L.off[which - 7].p;
+            c = (uint32_t)S->g->st.nb;
+            break;
+        case 11:
+            AW_CHECK_ARG(!L.dense, "res exists on block-structured levels only");
+            q = L.res.p;
+            c = (uint32_t)S->g->st.nb;
+            break;
+        default: return set_error(AW_ERR_INVALID_ARGUMENT, "unknown level array %d", which);
+    }
+    *p = q;
+    if (count) *count = c;
+    return AW_OK;
+}
+
+extern "C" aw_status aw_smoother_solve_level(aw_solver* S, int32_t m, int32_t iterations, aw_stream s) {
+    AW_CHECK_ARG(S && m >= 0 && m < (int)S->lv.size() && iterations >= 0, "bad argument");
+    return smooth_level(S, m, iterations, (cudaStream_t)s);
+}
+extern "C" aw_status aw_mg_residual(aw_solver* S, int32_t m, aw_stream s) {
+    AW_CHECK_ARG(S && m >= 0 && m < (int)S->lv.size(), "bad argument");
+    return residual_level(S, m, nullptr, (cudaStream_t)s);
+}
+extern "C" aw_status aw_mg_restrict(aw_solver* S, int32_t m, aw_stream s) {
+    AW_CHECK_ARG(S && m >= 0 && m + 1 < (int)S->lv.size(), "bad argument");
+    return restrict_level(S, m, (cudaStream_t)s);
+}
+extern "C" aw_status aw_mg_prolongate(aw_solver* S, int32_t m, aw_stream s) {
+    AW_CHECK_ARG(S && m >= 0 && m + 1 < (int)S->lv.size(), "bad argument");
+    return prolong_level(S, m, (cudaStream_t)s);
+}
+extern "C" aw_status aw_vcycle_run(aw_solver* S, aw_stream s) {
+    AW_CHECK_ARG(S, "null solver");
+    return vcycle(S, 0, (cudaStream_t)s);
+}
+
+static aw_status read_norm(aw_solver* S, int nparts, cudaStream_t s, double* out) {
+    k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, nparts, S->norm.p);
+    AW_LAUNCH();
+    double h = 0;
+    AW_CUDA(cudaMemcpyAsync(&h, S->norm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    AW_CUDA(cudaStreamSynchronize(s));
+    *out = std::sqrt(h);
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t* cycles, double* final_rel,
+                              aw_stream s_) {
+    AW_CHECK_ARG(S && d_b && d_p, "null argument");
+    cudaStream_t s = (cudaStream_t)s_;
+    MGLevel& L0 = S->lv[0];
+    const int cf = fv(S) ? 1 : 0;
+    const size_t nc = L0.ncell();
+    // ||b||
+    int nparts = 256;
+    k_sumsq<<<nparts, 256, 0, s>>>(d_b, L0.fluid.p, nc, cf, S->partials.p);
+    AW_LAUNCH();
+    double bn;
+    AW_TRY(read_norm(S, nparts, s, &bn));
+    if (!(bn == bn) || std::isinf(bn)) return set_error(AW_ERR_NAN, "right-hand side contains NaN/Inf");
+    if (bn == 0.0) bn = 1.0;
+    const int nlist = L0.nlist[0] + L0.nlist[1];
+    int it = 0;
+    double rel = 0;
+    aw_status st = AW_OK;
+    if (S->d.precision == AW_PRECISION_FP32) {
+        S->x0 = (float*)d_p;
+        S->b0 = d_b;
+        for (;; ++it) {
+            st = residual_level(S, 0, S->partials.p, s);
+            if (st != AW_OK) break;
+            double rn;
+            st = read_norm(S, nlist, s, &rn);
+            if (st != AW_OK) break;
+            rel = rn / bn;
+            if (!(rel == rel)) {
+                st = set_error(AW_ERR_NAN, "residual became NaN after %d cycles", it);
+                break;
+            }
+            if (rel < S->d.tolerance) break;
+            if (it >= S->d.max_cycles) {
+                st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d cycles", rel, it);
+                break;
+            }
+            st = vcycle(S, 0, s);
+            if (st != AW_OK) break;
+        }
+        S->x0 = nullptr;
+        S->b0 = nullptr;
+    } else {
+        double* p = (double*)d_p;
+        size_t smem = (size_t)(L0.maxres + 2) * (L0.maxres + 2) * (L0.maxres + 2) * sizeof(double);
+        LevelView V = lview(S, 0);
+        for (;; ++it) {
+            int off = 0;
+            for (int rb = 0; rb < 2; ++rb) {
+                if (!L0.nlist[rb]) continue;
+                k_residual64<<<L0.nlist[rb], 256, smem, s>>>(V, p, d_b, coef(L0), L0.fluid.p, L0.list[rb].p, cf, L0.b.p,
+                                                             S->partials.p + off);
+                off += L0.nlist[rb];
+                ++g_launches;
+            }
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                st = set_error(AW_ERR_CUDA, "k_residual64: %s", cudaGetErrorString(e));
+                break;
+            }
+            double rn;
+            st = read_norm(S, nlist, s, &rn);
+            if (st != AW_OK) break;
+            rel = rn / bn;
+            if (!(rel == rel)) {
+                st = set_error(AW_ERR_NAN, "residual became NaN after %d cycles", it);
+                break;
+            }
+            if (rel < S->d.tolerance) break;
+            if (it >= S->d.max_cycles) {
+                st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d cycles", rel, it);
+                break;
+            }
+            st = zero_x(S, 0, s);
+            if (st != AW_OK) break;
+            st = vcycle(S, 0, s);
+            if (st != AW_OK) break;
+            k_accum64<<<nblk(nc), 256, 0, s>>>(p, L0.x.p, nc);
+            ++g_launches;
+            e = cudaGetLastError();
+            if (e != cudaSuccess) {
+                st = set_error(AW_ERR_CUDA, "k_accum64: %s", cudaGetErrorString(e));
+                break;
+            }
+        }
+    }
+    if (cycles) *cycles = it;
+    if (final_rel) *final_rel = rel;
+    return st;
+}

@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the FLIP step on the MSBG (metric: P2G+G2P Mparticles/s; Poisson time to a
+relative residual, mixed vs FP32 V-cycle).
+
+Workload (one process per GPU; the path does not shard, so N GPUs run N replicas):
+  step     = one FLIP step of dam_drop_128 (128^3 effective, 3 levels, 4.14M particles) on
+             library-owned particles already resident in HBM.
+  value    = particles * steps / sum over steps of (P2G kernel + G2P kernel) device time.
+  e2e      = the same metric through the drop-in C-ABI calls with host buffers: per step a pinned
+             host->device copy of positions and velocities, aw_p2g (sort + P2G), backup, aw_g2p,
+             and a device->host copy of the velocities.
+  poisson  = poisson_256 (256^3 effective, 4 levels) projection to 1e-6 and 1e-9 relative residual,
+             FP32 V-cycle vs mixed precision.
+  --impl reference: the FP64 OpenMP CPU restatement (oracle) of the same P2G+G2P workload, timed on
+             the host cores.
+
+Inputs are larger than L2 (cfg particles 4.14M x 24 B = 99 MB SoA + grid); the timed steps also
+re-sort and re-scatter the particle arrays, so consecutive steps do not reuse a warm L2 copy.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Poisson ms to 1e-6 rel. resid (mixed vs FP32 V-cycle); P2G+G2P Mparticles/s"
+UNIT = "Mparticles/s"
+WORKLOAD = "dam_drop_128"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().strip().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(ws, v):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------------------------
+# CPU baseline: FP64 OpenMP oracle on the host cores
+# --------------------------------------------------------------------------------------------
+def cpu_p2g_g2p(S, budget_s=12.0, max_reps=6):
+    from oracle import pyoracle as po
+    lv = po.levels_from_particles(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, S.pos, S.thresholds)
+    lv, _ = po.enforce_grading(S.dims, S.num_levels, lv)
+    O = po.Oracle(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, lv)
+    _, perm = O.particle_keys(S.pos)
+    pos, vel = S.pos[perm], S.vel[perm]
+    times = []
+    t0 = time.perf_counter()
+    while len(times) < max_reps and (time.perf_counter() - t0 < budget_s or not times):
+        t = time.perf_counter()
+        u, m, _ = O.p2g(pos, vel)
+        O.g2p(pos, u, u, S.alpha, vel)
+        times.append(time.perf_counter() - t)
+    return S.n / np.mean(times) / 1e6, po.num_threads(), len(times), times
+
+
+# --------------------------------------------------------------------------------------------
+def run_reference(args, ws, rank):
+    from anitowave_adaptive_b200 import scenes
+    if rank != 0:
+        return
+    S = scenes.config(WORKLOAD)
+    from oracle import pyoracle as po
+    po.set_threads(os.cpu_count() or 1)
+    lv = po.levels_from_particles(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, S.pos, S.thresholds)
+    lv, _ = po.enforce_grading(S.dims, S.num_levels, lv)
+    O = po.Oracle(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, lv)
+    _, perm = O.particle_keys(S.pos)
+    pos, vel = S.pos[perm], S.vel[perm]
+    for _ in range(args.warmup):
+        u, m, _ = O.p2g(pos, vel)
+        O.g2p(pos, u, u, S.alpha, vel)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        u, m, _ = O.p2g(pos, vel)
+        O.g2p(pos, u, u, S.alpha, vel)
+    dt = time.perf_counter() - t0
+    value = S.n * args.steps / dt / 1e6
+    cores = po.num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "particles": S.n, "grid": "128^3 effective, 8^3-cell blocks, 3 levels",
+                   "l2": "inputs > L2 (99 MB particles + grid)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"full {WORKLOAD} P2G+G2P per step ({S.n} particles), FP64 OpenMP restatement; "
+                                   "the reference has no CPU implementation"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, ws, rank, local):
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import scenes
+
+    torch.cuda.set_device(local)
+    S = scenes.config(WORKLOAD)
+    g = aw.build_grid(S)
+    F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_FP32, tolerance=1e-6,
+                max_cycles=100)
+    for _ in range(args.warmup):
+        F.step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = Clocks(local) if rank == 0 else None
+    l0 = aw.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record()
+    ms_p2g = ms_g2p = 0.0
+    stats = []
+    for _ in range(args.steps):
+        F.step()
+        st = F.stats()
+        stats.append(st)
+        ms_p2g += st["ms_p2g"]
+        ms_g2p += st["ms_g2p"]
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = aw.launch_count() - l0
+    clocks = clk.stop() if clk else None
+    barrier(ws)
+    ms_total = max_over_ranks(ws, ev0.elapsed_time(ev1))
+    kern_ms = max_over_ranks(ws, ms_p2g + ms_g2p)
+    value = ws * S.n * args.steps / (kern_ms / 1e3) / 1e6
+
+    # roofline of the P2G kernel (algorithmic bytes: particles 24 B, faces u + m 8 B)
+    tot = g.totals()
+    faces = sum(tot[1:])
+    p2g_bytes = S.n * 24 + faces * 8
+    g2p_bytes = S.n * 36 + faces * 8
+    hbm, peak_kind = peaks()
+    p2g_ms = ms_p2g / args.steps
+    g2p_ms = ms_g2p / args.steps
+    p2g_gbs = p2g_bytes / (p2g_ms / 1e3) / 1e9
+    g2p_gbs = g2p_bytes / (g2p_ms / 1e3) / 1e9
+
+    # e2e through the drop-in C ABI with host buffers
+    pos_h = torch.from_numpy(S.pos).pin_memory()
+    vel_h = torch.from_numpy(S.vel).pin_memory()
+    vel_out = torch.empty_like(vel_h).pin_memory()
+    pos_d = torch.empty_like(pos_h, device="cuda")
+    vel_d = torch.empty_like(vel_h, device="cuda")
+    e2e_steps = max(3, args.steps)
+    for it in range(args.warmup + e2e_steps):
+        if it == args.warmup:
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+        pos_d.copy_(pos_h, non_blocking=True)
+        vel_d.copy_(vel_h, non_blocking=True)
+        g.p2g(pos_d, vel_d)
+        g.backup_grid_velocity()
+        g.g2p(vel_d, pos_d, S.alpha)
+        vel_out.copy_(vel_d, non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    e2e_value = ws * S.n * e2e_steps / (e2e_ms / 1e3) / 1e6
+
+    poisson = None
+    if not args.skip_poisson:
+        poisson = poisson_bench(args)
+
+    if rank != 0:
+        return
+    cpu = None
+    if ws == 1 and not args.skip_cpu:
+        v, cores, reps, times = cpu_p2g_g2p(S)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"P2G+G2P of the full {WORKLOAD} particle set ({S.n}), FP64 OpenMP restatement, "
+                         f"{reps} repetitions ({sum(times):.1f} s)"}
+    last = stats[-1]
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded dam break + falling sphere)",
+        "config": {"workload": WORKLOAD, "particles": S.n, "grid": "128^3 effective, 8^3-cell blocks, 3 levels",
+                   "cells": tot[0], "faces": faces, "parallelism": f"replicas x{ws}",
+                   "l2": "inputs larger than L2 (particles 99 MB + grid); particles re-sorted every step"},
+        "roofline": {"kernel": "k_p2g_gather", "bound": "hbm", "achieved": p2g_gbs, "peak": hbm, "unit": "GB/s",
+                     "frac": p2g_gbs / hbm, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_launch": p2g_bytes, "ms_per_launch": p2g_ms},
+        "roofline_g2p": {"kernel": "k_g2p", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": g2p_gbs / hbm, "bytes_per_launch": g2p_bytes, "ms_per_launch": g2p_ms},
+        "step_breakdown_ms": {k: last[k] for k in ("ms_sort", "ms_p2g", "ms_solve", "ms_g2p", "ms_advect", "ms_other")},
+        "solver": {"cycles": last["cycles"], "residual": last["residual"], "div_before": last["div_before"],
+                   "div_after": last["div_after"]},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": S.n * 24, "d2h_bytes_per_step": S.n * 12},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    if poisson is not None:
+        line["poisson"] = poisson
+    print(json.dumps(line), flush=True)
+
+
+def poisson_bench(args):
+    """poisson_256: closed box, level map from 32 spheres, blob divergence; FP32 vs mixed."""
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import poisson as pz
+    prob = pz.build_problem(256)
+    out = {"workload": "poisson_256", "cells": int(prob.b.numel())}
+    for name, prec in (("fp32", aw.PRECISION_FP32), ("mixed", aw.PRECISION_MIXED)):
+        for tol in (1e-6, 1e-9):
+            sv = aw.Solver(prob.grid, precision=prec, tolerance=tol, max_cycles=60)
+            sv.setup(None)
+            p = torch.zeros(prob.b.numel(), dtype=torch.float32 if prec == aw.PRECISION_FP32 else torch.float64,
+                            device="cuda")
+            sv.solve(prob.b, p, raise_on_error=False)  # warm
+            times = []
+            for _ in range(3):
+                p.zero_()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                cyc, rel, st = sv.solve(prob.b, p, raise_on_error=False)
+                torch.cuda.synchronize()
+                times.append(1e3 * (time.perf_counter() - t0))
+            div = prob.divergence_after(sv, p)
+            out[f"{name}_{tol:.0e}"] = {"ms": min(times), "cycles": cyc, "rel_residual": rel,
+                                        "converged": st == 0, "div_after": div}
+            sv.close()
+    a, b = out.get("fp32_1e-06"), out.get("mixed_1e-06")
+    if a and b and a["converged"] and b["converged"]:
+        out["speedup_mixed_vs_fp32_1e-6"] = a["ms"] / b["ms"]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-poisson", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+    ws, rank, local = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()
