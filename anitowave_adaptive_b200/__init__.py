@@ -114,6 +114,7 @@ SIGNATURES = {
     "aw_mg_residual": (C.c_int, [_VP, _I32, _VP]),
     "aw_mg_restrict": (C.c_int, [_VP, _I32, _VP]),
     "aw_mg_prolongate": (C.c_int, [_VP, _I32, _VP]),
+    "aw_solver_coarsest_solve": (C.c_int, [_VP, _VP]),
     "aw_vcycle_run": (C.c_int, [_VP, _VP]),
     "aw_solve": (C.c_int, [_VP, _VP, _VP, C.POINTER(_I32), C.POINTER(_D), _VP]),
     "aw_flip_create": (C.c_int, [_VP, C.POINTER(FlipDesc), _VP, _VP, _I64, _PP]),
@@ -227,6 +228,7 @@ class MSBG:
         t = torch.as_tensor(np.ascontiguousarray(levels, np.uint32).view(np.int32), device="cuda")
         torch.cuda.synchronize()
         _cudart_copy(self.refinement_map_ptr(), t.data_ptr(), 4 * self.nb)
+        self.allocated = False
 
     def refinement_map(self):
         import torch
@@ -411,6 +413,9 @@ class Solver:
 
     def prolongate(self, level, stream=None):
         check(lib().aw_mg_prolongate(self.h, level, _stream(stream)))
+
+    def coarsest_solve(self, stream=None):
+        check(lib().aw_solver_coarsest_solve(self.h, _stream(stream)))
 
     def vcycle(self, stream=None):
         check(lib().aw_vcycle_run(self.h, _stream(stream)))

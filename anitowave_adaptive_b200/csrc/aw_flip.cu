@@ -398,12 +398,13 @@ extern "C" aw_status aw_flip_step(aw_flip* F, aw_stream s_) {
     // 7. G2P (FLIP blend) on the sorted SoA particles
     const float* un[3] = {U[0], U[1], U[2]};
     const float* uo[3] = {UO[0], UO[1], UO[2]};
-    AW_TRY(g2p_launch(G, soa, 1, soa + 3 * n, 1, n, F->d.alpha, un, uo, s));
+    AW_TRY(g2p_sorted(G, soa, n, G.pw.cell_start.p, F->d.alpha, un, uo, s));
     AW_CUDA(cudaEventRecord(F->ev[6], s));
-    // 8. RK3 advection
-    AW_TRY(advect_launch(G, soa, 1, n, F->d.dt, un, s));
+    // 8. RK3 advection through the u_new tiles built for G2P
+    AW_TRY(advect_tiles(G, soa, 1, n, F->d.dt, G.tiles_new.p, s));
     AW_CUDA(cudaEventRecord(F->ev[7], s));
     AW_CUDA(cudaEventSynchronize(F->ev[7]));
+    AW_TRY(check_device_errors(G, s));
     float dm[2];
     AW_CUDA(cudaMemcpy(dm, F->divmax.p, sizeof dm, cudaMemcpyDeviceToHost));
     F->stats.div_before = dm[0];

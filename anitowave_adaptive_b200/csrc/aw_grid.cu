@@ -419,7 +419,6 @@ extern "C" aw_status aw_msbg_init_refinement_map(aw_msbg* g, uint32_t value, aw_
 extern "C" aw_status aw_msbg_refinement_map(aw_msbg* g, uint32_t** d_levels) {
     AW_CHECK_ARG(g && d_levels, "null argument");
     *d_levels = g->st.level.p;
-    g->st.allocated = false;  // the caller may write it
     return AW_OK;
 }
 
@@ -532,6 +531,7 @@ extern "C" aw_status aw_msbg_allocate(aw_msbg* g, aw_stream s_) {
         AW_LAUNCH();
     }
     AW_CUDA(cudaStreamSynchronize(s));
+    G.h_tile_off.clear();  // tiles follow the new resolutions
     G.allocated = true;
     return AW_OK;
 }

@@ -172,7 +172,8 @@ __device__ inline double warp_sum(double v) {
 // Host-side objects
 // ------------------------------------------------------------------------------------------------
 struct ParticleWork {
-    DBuf<uint32_t> keys, perm, perm2, cell_start, cell_fill, tmp;
+    DBuf<uint32_t> keys, keys2, keys3, perm, perm2, cell_start, cell_fill, tmp, hist, hscan;
+    uint32_t* sorted = nullptr;  // sorted slot -> input index (perm or perm2)
     DBuf<float> soa, soa2;  // 6 SoA arrays: px py pz vx vy vz
     int64_t n = 0;
     aw_status ensure(int64_t np, uint32_t ncell);
@@ -194,6 +195,12 @@ struct MsbgState {
     float* ch[AW_NUM_CHANNELS_EXT] = {};    // channel pointers into the slab
     uint32_t ch_count[AW_NUM_CHANNELS_EXT] = {};
     DBuf<uint32_t> scratch_u32;
+    // ghosted face tiles (per block: 3 axes x (r+1)(r+2)^2, padded to 16 bytes)
+    DBuf<uint32_t> tile_off;
+    std::vector<uint32_t> h_tile_off;
+    uint32_t tile_tot = 0;
+    DBuf<float> tiles_new, tiles_old;
+    DBuf<int> err;  // device error flags: [0] P2G row overflow, [1] TMA wait timeout
     DBuf<uint8_t> occ;
     DBuf<int> flag;
     ParticleWork pw;
@@ -215,6 +222,12 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
                      float* mom[3], float* cell_count, cudaStream_t s);
 aw_status g2p_launch(MsbgState& G, const float* pos, int pos_stride_soa, float* vel, int vel_soa, int64_t n,
                      float alpha, const float* un[3], const float* uo[3], cudaStream_t s);
+aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float alpha, const float* un[3],
+                     const float* uo[3], cudaStream_t s);
+aw_status build_tiles(MsbgState& G, const float* u[3], float* tiles, cudaStream_t s);
+aw_status ensure_tiles(MsbgState& G);
+aw_status advect_tiles(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* tiles, cudaStream_t s);
+aw_status check_device_errors(MsbgState& G, cudaStream_t s);
 aw_status sort_core_soa(MsbgState& G, const float* soa_pos, int64_t n, cudaStream_t s);
 aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_soa, const uint32_t* ids_in,
                      uint32_t* ids_out, cudaStream_t s);

@@ -8,6 +8,8 @@
 //   G2P.cuh:87-128  FLIP blend v = a (v + du) + (1 - a) u_new
 //   G2P.cuh:131-173 Ralston RK3 advection
 // New (no reference code): stable particle sort by (block, cell) key.
+#include <algorithm>
+
 #include "aw_internal.cuh"
 
 namespace aw {
@@ -54,27 +56,86 @@ __global__ void k_keys(LevelView L, PArr pos, int64_t n, uint32_t invalid, uint3
     atomicAdd(&count[k], 1u);
 }
 
-__global__ void k_scatter(const uint32_t* __restrict__ keys, int64_t n, uint32_t* fill, uint32_t* slot_of) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t s = atomicAdd(&fill[keys[i]], 1u);
-    slot_of[s] = (uint32_t)i;
+// ------------------------------------------------------------------------------------------------
+// Stable LSD radix sort of (key, index) pairs, 10-bit digits.  Each pass: per-tile digit
+// histograms -> one exclusive scan over (digit, tile) -> scatter in which one warp walks its tile
+// in order and ranks equal digits with __match_any_sync, so equal keys keep their input order.
+// ------------------------------------------------------------------------------------------------
+constexpr int RADIX_BITS = 10, RADIX_BINS = 1 << RADIX_BITS, RADIX_TILE = 2048;
+
+__global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift,
+                                                    uint32_t* __restrict__ hist, uint32_t ntiles) {
+    __shared__ uint32_t h[RADIX_BINS];
+    for (int i = threadIdx.x; i < RADIX_BINS; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * RADIX_TILE;
+    for (int i = threadIdx.x; i < RADIX_TILE; i += blockDim.x) {
+        int64_t j = base + i;
+        if (j < n) atomicAdd(&h[(keys[j] >> shift) & (RADIX_BINS - 1)], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < RADIX_BINS; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
 }
 
-// Within each bucket, order the particle indices ascending: this makes the sort stable.
-__global__ void k_bucket_order(const uint32_t* __restrict__ start, uint32_t nbucket, uint32_t* idx) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= nbucket) return;
-    uint32_t s = start[c], e = start[c + 1];
-    for (uint32_t i = s + 1; i < e; ++i) {
-        uint32_t v = idx[i];
-        uint32_t j = i;
-        while (j > s && idx[j - 1] > v) {
-            idx[j] = idx[j - 1];
-            --j;
+__global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
+                                                       uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
+                                                       int shift, const uint32_t* __restrict__ offs, uint32_t ntiles) {
+    extern __shared__ uint32_t cnt[];  // RADIX_BINS per warp
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t tile = blockIdx.x * (blockDim.x >> 5) + w;
+    uint32_t* c = cnt + w * RADIX_BINS;
+    if (tile >= ntiles) return;
+    for (int d = lane; d < RADIX_BINS; d += 32) c[d] = offs[(size_t)d * ntiles + tile];
+    __syncwarp();
+    const int64_t base = (int64_t)tile * RADIX_TILE;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int ch = 0; ch < RADIX_TILE; ch += 32) {
+        const int64_t j = base + ch + lane;
+        const bool valid = j < n;
+        uint32_t key = 0, val = 0, dig = 0;
+        if (valid) {
+            key = kin[j];
+            val = vin ? vin[j] : (uint32_t)j;
+            dig = (key >> shift) & (RADIX_BINS - 1);
         }
-        idx[j] = v;
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? dig : (uint32_t)(RADIX_BINS + lane));
+        const uint32_t pos = valid ? c[dig] + __popc(peers & lt) : 0u;
+        __syncwarp();
+        if (valid && (__ffs(peers) - 1) == lane) c[dig] += __popc(peers);
+        __syncwarp();
+        if (valid) {
+            kout[pos] = key;
+            vout[pos] = val;
+        }
     }
+}
+
+static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* vals, uint32_t* vals2, int64_t n,
+                                  uint32_t maxkey, DBuf<uint32_t>& hist, DBuf<uint32_t>& scan_out, DBuf<uint32_t>& tmp,
+                                  uint32_t** sorted_vals, cudaStream_t s) {
+    int bits = 1;
+    while (bits < 32 && (maxkey >> bits)) ++bits;
+    const int passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
+    const uint32_t ntiles = (uint32_t)((n + RADIX_TILE - 1) / RADIX_TILE);
+    const size_t nh = (size_t)RADIX_BINS * ntiles;
+    AW_TRY(hist.ensure(nh));
+    AW_TRY(scan_out.ensure(nh + 1));
+    uint32_t *kin = keys, *kout = keys2, *vin = nullptr, *vout = vals;
+    const int wpb = 8;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * RADIX_BITS;
+        k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, hist.p, ntiles);
+        AW_LAUNCH();
+        AW_TRY(exclusive_scan_u32(hist.p, scan_out.p, nh, tmp, s));
+        k_radix_scatter<<<(ntiles + wpb - 1) / wpb, 32 * wpb, wpb * RADIX_BINS * sizeof(uint32_t), s>>>(
+            kin, vin, kout, vout, n, shift, scan_out.p, ntiles);
+        AW_LAUNCH();
+        std::swap(kin, kout);
+        vin = vout;
+        vout = (vout == vals) ? vals2 : vals;
+    }
+    *sorted_vals = vin;
+    return AW_OK;
 }
 
 // gather pos/vel into SoA sorted order, carry the original ids
@@ -121,13 +182,13 @@ aw_status sort_core(MsbgState& G, PArr pos, int64_t n, cudaStream_t s) {
         AW_LAUNCH();
     }
     AW_TRY(exclusive_scan_u32(W.cell_fill.p, W.cell_start.p, (size_t)nc + 1, W.tmp, s));
-    AW_CUDA(cudaMemcpyAsync(W.cell_fill.p, W.cell_start.p, ((size_t)nc + 1) * sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                            s));
+    W.sorted = W.perm.p;
     if (n > 0) {
-        k_scatter<<<nblk(n), 256, 0, s>>>(W.keys.p, n, W.cell_fill.p, W.perm.p);
-        AW_LAUNCH();
-        k_bucket_order<<<nblk((size_t)nc + 1), 256, 0, s>>>(W.cell_start.p, nc + 1, W.perm.p);
-        AW_LAUNCH();
+        // keys are consumed by the sort: keep a copy for aw_sort_particles' key output
+        AW_TRY(W.keys2.ensure((size_t)n));
+        AW_TRY(W.keys3.ensure((size_t)n));
+        AW_CUDA(cudaMemcpyAsync(W.keys3.p, W.keys.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        AW_TRY(radix_sort_pairs(W.keys3.p, W.keys2.p, W.perm.p, W.perm2.p, n, nc, W.hist, W.hscan, W.tmp, &W.sorted, s));
     }
     return AW_OK;
 }
@@ -136,7 +197,7 @@ aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* ve
     PArr pos{pos_aos, 3, 1}, vel{vel_aos, 3, 1};
     AW_TRY(sort_core(G, pos, n, s));
     if (n > 0) {
-        k_gather<<<nblk(n), 256, 0, s>>>(G.pw.perm.p, n, pos, vel, G.pw.soa.p, nullptr, nullptr, nullptr, nullptr);
+        k_gather<<<nblk(n), 256, 0, s>>>(G.pw.sorted, n, pos, vel, G.pw.soa.p, nullptr, nullptr, nullptr, nullptr);
         AW_LAUNCH();
     }
     return AW_OK;
@@ -150,7 +211,7 @@ aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_so
                      uint32_t* ids_out, cudaStream_t s) {
     if (n <= 0) return AW_OK;
     PArr pos{in_soa, 1, n}, vel{in_soa + 3 * n, 1, n};
-    k_gather<<<nblk(n), 256, 0, s>>>(G.pw.perm.p, n, pos, vel, out_soa, ids_in, ids_out, nullptr, nullptr);
+    k_gather<<<nblk(n), 256, 0, s>>>(G.pw.sorted, n, pos, vel, out_soa, ids_in, ids_out, nullptr, nullptr);
     AW_LAUNCH();
     return AW_OK;
 }
@@ -186,77 +247,190 @@ struct FaceOut {
     float* mom[3];
 };
 
-__global__ void __launch_bounds__(256) k_p2g_gather(LevelView L, const float* __restrict__ soa, int64_t n,
-                                                    const uint32_t* __restrict__ cstart, FaceOut out) {
+// P2G as a block-local scatter.  One CTA per block b accumulates, in shared memory, the weights
+// w = (1 - d^2/h_b^2)^3 of every particle that can reach one of b's faces: b's own particles and
+// the boundary cell layers of its 26 neighbours (rows of cells that are contiguous in the sorted
+// particle array).  Contributions that land outside b are dropped here and accumulated by the
+// owning block's CTA instead, so every face copy is written exactly once (mass and
+// velocity = momentum / mass fused), with no global atomics.  Lanes of a warp walk particles a
+// 32nd of the range apart, so that one warp's shared-memory atomics hit different faces.
+constexpr int P2G_MAXROWS = 2048;
+
+__device__ inline void p2g_nbr_box(const LevelView& L, const int cb[3], int r, int d, int* nblk, int lo[3], int hi[3]) {
+    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+    int nc[3] = {cb[0] + dd[0], cb[1] + dd[1], cb[2] + dd[2]};
+    *nblk = -1;
+    if (!inside(L.g, nc)) return;
+    const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+    const int rn = L.res[n];
+    if (!rn) return;
+    const int k = rn > r ? rn / r : 1;  // neighbour cell layers within one of b's cells
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        if (dd[q] == 0) { lo[q] = 0; hi[q] = rn - 1; }
+        else if (dd[q] > 0) { lo[q] = 0; hi[q] = k - 1; }
+        else { lo[q] = rn - k; hi[q] = rn - 1; }
+    }
+    *nblk = n;
+}
+
+__global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* __restrict__ soa, int64_t n,
+                                                     const uint32_t* __restrict__ cs, FaceOut out, int* err) {
+    extern __shared__ float sm[];
+    __shared__ int dcnt[27];
+    __shared__ int doff[28];
+    __shared__ uint32_t wsum[8];
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
     const Geo& g = L.g;
+    const int nf = (r + 1) * r * r;
+    float* am = sm;
+    float* ap = am + 3 * nf;
+    uint32_t* rstart = (uint32_t*)(ap + 3 * nf);
+    uint32_t* rpre = rstart + P2G_MAXROWS;  // P2G_MAXROWS + 1 entries
     int cb[3];
     bcoord(g, b, cb);
+    for (int i = threadIdx.x; i < 6 * nf; i += blockDim.x) sm[i] = 0.f;
+    if (threadIdx.x < 27) {
+        int nb_, lo[3], hi[3];
+        p2g_nbr_box(L, cb, r, threadIdx.x, &nb_, lo, hi);
+        dcnt[threadIdx.x] = nb_ < 0 ? 0 : (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int d = 0; d < 27; ++d) {
+            doff[d] = acc;
+            acc += dcnt[d];
+        }
+        doff[27] = acc;
+        if (acc > P2G_MAXROWS) *err = 1;
+    }
+    __syncthreads();
+    const int nrows = min(doff[27], P2G_MAXROWS);
+    for (int k = threadIdx.x; k < nrows; k += blockDim.x) {
+        int d = 0;
+        while (doff[d + 1] <= k) ++d;
+        int nb_, lo[3], hi[3];
+        p2g_nbr_box(L, cb, r, d, &nb_, lo, hi);
+        const int rn = L.res[nb_];
+        const int local = k - doff[d];
+        const int ny = hi[1] - lo[1] + 1;
+        const int y = lo[1] + local % ny, z = lo[2] + local / ny;
+        const uint32_t base = L.off[0][nb_];
+        const uint32_t s0 = cs[base + cidx(lo[0], y, z, rn)];
+        rstart[k] = s0;
+        rpre[k] = cs[base + cidx(hi[0], y, z, rn) + 1] - s0;  // length for now
+    }
+    __syncthreads();
+    // exclusive scan of the row lengths (<= 2048 rows, 8 per thread)
+    {
+        const int per = (P2G_MAXROWS + blockDim.x - 1) / blockDim.x;
+        const int r0 = threadIdx.x * per;
+        uint32_t loc = 0;
+        for (int k = r0; k < min(r0 + per, nrows); ++k) loc += rpre[k];
+        // block exclusive scan of loc
+        uint32_t x = loc;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        uint32_t wpre = 0;
+        for (int i = 0; i < w; ++i) wpre += wsum[i];
+        uint32_t pre = wpre + x - loc;
+        __syncthreads();
+        for (int k = r0; k < min(r0 + per, nrows); ++k) {
+            uint32_t len = rpre[k];
+            rpre[k] = pre;
+            pre += len;
+        }
+        if (threadIdx.x == blockDim.x - 1) rpre[nrows] = pre;
+    }
+    __syncthreads();
+    const uint32_t T = rpre[nrows];
     const float h = fcell(g, r);
-    const float R2 = h * h, invR2 = 1.f / R2;
+    const float invh = 1.f / h;
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
-    const float* px = soa;
-    const float* py = soa + n;
-    const float* pz = soa + 2 * n;
-    const int nf = (r + 1) * r * r;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t Ls = (T + 31) / 32;
+    const float rf = (float)r;
+    int row = 0;  // per-lane cursor: v only grows along a lane's walk
+    for (uint32_t i = w; i < Ls; i += nw) {
+        const uint32_t v = lane * Ls + i;
+        if (v >= T) break;
+        while (row + 1 < nrows && rpre[row + 1] <= v) ++row;
+        const uint32_t sidx = rstart[row] + (v - rpre[row]);
+        float q[3], vel[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
+            vel[k] = soa[(int64_t)(3 + k) * n + sidx];
+        }
+        if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f)
+            continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            const int ia = (int)floorf(q[a]);
+            const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
+            // squared distances per candidate index, +inf where the index is outside the block
+            float dA2[2], dB2[2], dC2[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const float dA = q[a] - (float)(ia + k);
+                const float dB = q[t1] - ((float)(j1 + k) + 0.5f);
+                const float dC = q[t2] - ((float)(j2 + k) + 0.5f);
+                dA2[k] = (ia + k >= 0 && ia + k <= r) ? dA * dA : 4.f;
+                dB2[k] = (j1 + k >= 0 && j1 + k < r) ? dB * dB : 4.f;
+                dC2[k] = (j2 + k >= 0 && j2 + k < r) ? dC * dC : 4.f;
+            }
+            float* Am = am + a * nf;
+            float* Ap = ap + a * nf;
+            const float va = vel[a];
+#pragma unroll
+            for (int da = 0; da < 2; ++da)
+#pragma unroll
+                for (int d1 = 0; d1 < 2; ++d1) {
+                    const float dAB = dA2[da] + dB2[d1];
+                    if (dAB >= 1.f) continue;
+#pragma unroll
+                    for (int d2 = 0; d2 < 2; ++d2) {
+                        const float d2s = dAB + dC2[d2];
+                        if (d2s < 1.f) {
+                            const float tt = 1.f - d2s;
+                            const float wgt = tt * tt * tt;
+                            int f[3];
+                            f[a] = ia + da;
+                            f[t1] = j1 + d1;
+                            f[t2] = j2 + d2;
+                            const uint32_t fi = fidx(a, f[0], f[1], f[2], r);
+                            atomicAdd(&Am[fi], wgt);
+                            atomicAdd(&Ap[fi], wgt * va);
+                        }
+                    }
+                }
+        }
+    }
+    __syncthreads();
     for (int t = threadIdx.x; t < 3 * nf; t += blockDim.x) {
         const int a = t / nf, fi = t - a * nf;
-        int f[3];
-        face_coords(a, fi, r, f);
-        float xf[3];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) xf[q] = o[q] + h * ((float)f[q] + (q == a ? 0.f : 0.5f));
-        const float* pv = soa + (3 + a) * n;
-        int blo[3], bhi[3];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-            blo[q] = max(0, (int)floorf((xf[q] - h - g.dmin[q]) / g.bs));
-            bhi[q] = min(g.D[q] - 1, (int)floorf((xf[q] + h - g.dmin[q]) / g.bs));
-        }
-        float msum = 0.f, psum = 0.f;
-        for (int nz = blo[2]; nz <= bhi[2]; ++nz)
-            for (int ny = blo[1]; ny <= bhi[1]; ++ny)
-                for (int nx = blo[0]; nx <= bhi[0]; ++nx) {
-                    const int nbk = bidx(g, nx, ny, nz);
-                    const int rn = L.res[nbk];
-                    if (!rn) continue;
-                    const int nc[3] = {nx, ny, nz};
-                    const float hn = fcell(g, rn);
-                    int clo[3], chi[3];
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        float on = forigin(g, q, nc[q]);
-                        clo[q] = max(0, (int)floorf((xf[q] - h - on) / hn));
-                        chi[q] = min(rn - 1, (int)floorf((xf[q] + h - on) / hn));
-                    }
-                    const uint32_t base = L.off[0][nbk];
-                    for (int cz = clo[2]; cz <= chi[2]; ++cz)
-                        for (int cy = clo[1]; cy <= chi[1]; ++cy) {
-                            // cells cx = clo..chi are contiguous in the sorted particle array
-                            uint32_t k0 = base + cidx(clo[0], cy, cz, rn);
-                            uint32_t k1 = base + cidx(chi[0], cy, cz, rn) + 1;
-                            uint32_t s0 = cstart[k0], s1 = cstart[k1];
-                            for (uint32_t s = s0; s < s1; ++s) {
-                                float dx = px[s] - xf[0], dy = py[s] - xf[1], dz = pz[s] - xf[2];
-                                float d2 = dx * dx + dy * dy + dz * dz;
-                                if (d2 < R2) {
-                                    float tt = 1.f - d2 * invR2;
-                                    float w = tt * tt * tt;
-                                    msum += w;
-                                    psum += w * pv[s];
-                                }
-                            }
-                        }
-                }
+        const float m = am[t], P = ap[t];
         const uint32_t oi = L.off[1 + a][b] + (uint32_t)fi;
-        out.m[a][oi] = msum;
-        if (out.mom[a]) out.mom[a][oi] = psum;
-        out.u[a][oi] = msum > 1e-6f ? psum / msum : 0.f;
+        out.m[a][oi] = m;
+        if (out.mom[a]) out.mom[a][oi] = P;
+        out.u[a][oi] = m > 1e-6f ? P / m : 0.f;
     }
+}
+
+static size_t p2g_smem(int r) {
+    return (size_t)6 * (r + 1) * r * r * sizeof(float) + (size_t)(2 * P2G_MAXROWS + 1) * sizeof(uint32_t);
 }
 
 __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, float* out) {
@@ -272,7 +446,12 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
         o.m[a] = m[a];
         o.mom[a] = mom[a];
     }
-    k_p2g_gather<<<G.nb, 256, 0, s>>>(G.view0(), soa, n, cstart, o);
+    int maxres = 0;
+    for (int r : G.h_res) maxres = std::max(maxres, r);
+    const size_t smem = p2g_smem(maxres);
+    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    AW_TRY(G.flag.ensure(1));
+    k_p2g_scatter<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, o, G.flag.p);
     AW_LAUNCH();
     if (cell_count) {
         k_cell_count<<<nblk(G.tot[0]), 256, 0, s>>>(cstart, G.tot[0], cell_count);
@@ -405,6 +584,276 @@ __global__ void k_advect(LevelView L, PArrW pos, int64_t n, float dt, Field3 u) 
     }
 }
 
+// ------------------------------------------------------------------------------------------------
+// Ghosted face tiles.  For every block and axis a the tile holds the faces [0,r] along a and
+// [-1,r] along both tangential axes (ghost layer filled by face_value's neighbour rule), so a
+// trilinear MAC sample anywhere in the block reads 8 tile entries and nothing else.  Layout per
+// block: axis-major, entry (iA, i1, i2) at iA + (r+1) ((i1+1) + (r+2) (i2+1)); each block's
+// tiles start on a 16-byte boundary so they can be staged with one TMA bulk copy.
+// ------------------------------------------------------------------------------------------------
+__host__ __device__ inline uint32_t tile_axis(int r) { return (uint32_t)((r + 1) * (r + 2) * (r + 2)); }
+__host__ __device__ inline uint32_t tile_block(int r) { return r ? ((3 * tile_axis(r) + 3u) & ~3u) : 0u; }
+
+__global__ void k_build_tiles(LevelView L, Field3 u, const uint32_t* __restrict__ toff, float* __restrict__ tiles) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const int R1 = r + 1, R2 = r + 2;
+    const int TA = (int)tile_axis(r);
+    float* out = tiles + toff[b];
+    for (int t = threadIdx.x; t < 3 * TA; t += blockDim.x) {
+        const int a = t / TA, rem = t - a * TA;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        int fi[3];
+        fi[a] = rem % R1;
+        fi[t1] = (rem / R1) % R2 - 1;
+        fi[t2] = rem / (R1 * R2) - 1;
+        out[t] = face_value(L, u.c[a], a, b, cb, r, fi);
+    }
+}
+
+// Trilinear sample of component a at X from the ghosted tiles (same stencil as sample_comp).
+__device__ inline float tile_interp(const float* __restrict__ t, int a, int r, const float o[3], float h, const float X[3]) {
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    float sA = (X[a] - o[a]) / h;
+    float s1 = (X[t1] - o[t1]) / h - 0.5f;
+    float s2 = (X[t2] - o[t2]) / h - 0.5f;
+    sA = fminf(fmaxf(sA, 0.f), (float)r);
+    s1 = fminf(fmaxf(s1, -1.f), (float)r);
+    s2 = fminf(fmaxf(s2, -1.f), (float)r);
+    const int iA = min(max((int)floorf(sA), 0), r - 1);
+    const int i1 = min(max((int)floorf(s1), -1), r - 1);
+    const int i2 = min(max((int)floorf(s2), -1), r - 1);
+    const float fA = sA - (float)iA, f1 = s1 - (float)i1, f2 = s2 - (float)i2;
+    const int R1 = r + 1, R2 = r + 2;
+    const float* p = t + a * (int)tile_axis(r) + iA + R1 * ((i1 + 1) + R2 * (i2 + 1));
+    const int s_1 = R1, s_2 = R1 * R2;
+    const float c00 = p[0] + fA * (p[1] - p[0]);
+    const float c10 = p[s_1] + fA * (p[s_1 + 1] - p[s_1]);
+    const float c01 = p[s_2] + fA * (p[s_2 + 1] - p[s_2]);
+    const float c11 = p[s_1 + s_2] + fA * (p[s_1 + s_2 + 1] - p[s_1 + s_2]);
+    const float c0 = c00 + f1 * (c10 - c00);
+    const float c1 = c01 + f1 * (c11 - c01);
+    return c0 + f2 * (c1 - c0);
+}
+
+__device__ inline float sample_tiles(const LevelView& L, const uint32_t* __restrict__ toff, const float* __restrict__ tiles,
+                                     int a, const float X[3]) {
+    int cb[3];
+    point_block(L.g, X, cb);
+    const int b = bidx(L.g, cb[0], cb[1], cb[2]);
+    const int r = L.res[b];
+    if (!r) return 0.f;
+    const float h = fcell(L.g, r);
+    float o[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[k] = forigin(L.g, k, cb[k]);
+    return tile_interp(tiles + toff[b], a, r, o, h, X);
+}
+
+// ---- TMA bulk copies (cp.async.bulk, no multicast) and a bounded mbarrier wait ----------------
+__device__ inline uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ inline void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ inline void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ inline void tma_bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// true when phase `parity` completed; false (and the error flag set) after ~1 s of polling
+__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
+    for (int it = 0; it < (1 << 20); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicExch(err, 1);
+    return false;
+}
+
+// G2P on sorted particles.  One CTA per block: thread 0 issues two TMA bulk copies (u_new and
+// u_old ghosted tiles, 16-byte aligned), every thread waits on the mbarrier, then each particle
+// of the block interpolates both fields from shared memory and applies the FLIP blend.
+__global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict__ soa, int64_t n,
+                                                  const uint32_t* __restrict__ cs, float alpha,
+                                                  const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
+                                                  const float* __restrict__ to_g, int* err) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    const uint32_t p0 = cs[L.off[0][b]], p1 = cs[L.off[0][b] + (uint32_t)(r * r * r)];
+    if (p0 == p1) return;
+    const uint32_t tb = tile_block(r);
+    float* tn = sm;
+    float* to = sm + tb;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, 2 * tb * sizeof(float));
+        tma_bulk_load(tn, tn_g + toff[b], tb * sizeof(float), &bar);
+        tma_bulk_load(to, to_g + toff[b], tb * sizeof(float), &bar);
+    }
+    const bool ok = mbar_wait_bounded(&bar, 0, err);
+    if (!__syncthreads_and(ok)) return;
+    const Geo& g = L.g;
+    int cb[3];
+    bcoord(g, b, cb);
+    const float h = fcell(g, r);
+    float o[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        float X[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) X[k] = soa[(int64_t)k * n + i];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float vn = tile_interp(tn, a, r, o, h, X);
+            const float vo = tile_interp(to, a, r, o, h, X);
+            float* vp = soa + (int64_t)(3 + a) * n + i;
+            *vp = alpha * (*vp + (vn - vo)) + (1.f - alpha) * vn;
+        }
+    }
+}
+
+// particles of inactive blocks (the last bucket of the sort) sample zero velocity: v = alpha v
+__global__ void k_g2p_inactive(float* soa, int64_t n, const uint32_t* __restrict__ bucket, float alpha) {
+    const uint32_t p0 = bucket[0], p1 = bucket[1];
+    for (uint32_t i = p0 + blockIdx.x * blockDim.x + threadIdx.x; i < p1; i += gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) soa[(int64_t)(3 + a) * n + i] *= alpha;
+}
+
+aw_status ensure_tiles(MsbgState& G) {
+    if (G.tile_off.p && G.h_tile_off.size() == (size_t)G.nb) return AW_OK;
+    G.h_tile_off.resize(G.nb);
+    uint32_t acc = 0;
+    for (int b = 0; b < G.nb; ++b) {
+        G.h_tile_off[b] = acc;
+        acc += tile_block(G.h_res[b]);
+    }
+    G.tile_tot = acc;
+    AW_TRY(G.tile_off.alloc(G.nb));
+    AW_CUDA(cudaMemcpy(G.tile_off.p, G.h_tile_off.data(), G.nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    AW_TRY(G.tiles_new.alloc(std::max<uint32_t>(acc, 4)));
+    AW_TRY(G.tiles_old.alloc(std::max<uint32_t>(acc, 4)));
+    AW_TRY(G.err.ensure(4));
+    AW_CUDA(cudaMemset(G.err.p, 0, 4 * sizeof(int)));
+    return AW_OK;
+}
+
+aw_status build_tiles(MsbgState& G, const float* u[3], float* tiles, cudaStream_t s) {
+    AW_CHECK_ARG(G.tile_off.p && tiles, "tiles not allocated");
+    Field3 f{{u[0], u[1], u[2]}};
+    k_build_tiles<<<G.nb, 128, 0, s>>>(G.view0(), f, G.tile_off.p, tiles);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
+    if (!G.err.p) return AW_OK;
+    int h[4];
+    AW_CUDA(cudaMemcpyAsync(h, G.err.p, sizeof h, cudaMemcpyDeviceToHost, s));
+    AW_CUDA(cudaStreamSynchronize(s));
+    if (h[0]) return set_error(AW_ERR_STATE, "P2G halo row table overflow");
+    if (h[1]) return set_error(AW_ERR_STATE, "TMA bulk-copy wait timed out in G2P");
+    return AW_OK;
+}
+
+static size_t g2p_smem(int r) { return (size_t)2 * tile_block(r) * sizeof(float); }
+
+aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float alpha, const float* un[3],
+                     const float* uo[3], cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, un, G.tiles_new.p, s));
+    AW_TRY(build_tiles(G, uo, G.tiles_old.p, s));
+    int maxres = 0;
+    for (int r : G.h_res) maxres = std::max(maxres, r);
+    const size_t smem = g2p_smem(maxres);
+    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_g2p_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_g2p_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, alpha, G.tile_off.p, G.tiles_new.p, G.tiles_old.p,
+                                       G.err.p + 1);
+    AW_LAUNCH();
+    k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+__global__ void k_advect_tiles(LevelView L, PArrW pos, int64_t n, float dt, const uint32_t* __restrict__ toff,
+                               const float* __restrict__ tiles) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Geo& g = L.g;
+    const float h0 = g.bs / (float)g.R0;
+    float x[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
+    float k1[3], k2[3], k3[3], y[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) k1[a] = sample_tiles(L, toff, tiles, a, x);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.5f * dt * k1[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) k2[a] = sample_tiles(L, toff, tiles, a, y);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.75f * dt * k2[a];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) k3[a] = sample_tiles(L, toff, tiles, a, y);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float v = (2.f / 9.f) * k1[a] + (3.f / 9.f) * k2[a] + (4.f / 9.f) * k3[a];
+        float lo = g.dmin[a] + 0.01f * h0;
+        float hi = g.dmin[a] + (float)g.D[a] * g.bs - 0.01f * h0;
+        pos(i, a) = fminf(fmaxf(x[a] + dt * v, lo), hi);
+    }
+}
+
+// G2P / sampling on arbitrary (unsorted, AoS) particles through the ghosted tiles
+__global__ void k_g2p_tiles(LevelView L, PArr pos, PArrW vel, int64_t n, float alpha, const uint32_t* __restrict__ toff,
+                            const float* __restrict__ tn, const float* __restrict__ to) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float X[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float vn = sample_tiles(L, toff, tn, a, X);
+        const float vo = sample_tiles(L, toff, to, a, X);
+        const float vp = vel(i, a);
+        vel(i, a) = alpha * (vp + (vn - vo)) + (1.f - alpha) * vn;
+    }
+}
+
+__global__ void k_sample_tiles(LevelView L, PArr pts, int64_t n, const uint32_t* __restrict__ toff,
+                               const float* __restrict__ tiles, float* out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float X[3] = {pts(i, 0), pts(i, 1), pts(i, 2)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[3 * i + a] = sample_tiles(L, toff, tiles, a, X);
+}
+
+aw_status advect_tiles(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* tiles, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    PArrW P = pos_soa ? PArrW{pos, 1, n} : PArrW{pos, 3, 1};
+    k_advect_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), P, n, dt, G.tile_off.p, tiles);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 aw_status g2p_launch(MsbgState& G, const float* pos, int pos_soa, float* vel, int vel_soa, int64_t n, float alpha,
                      const float* un[3], const float* uo[3], cudaStream_t s) {
     if (n <= 0) return AW_OK;
@@ -442,9 +891,9 @@ extern "C" aw_status aw_sort_particles(aw_msbg* g, const float* d_pos, int64_t n
     AW_TRY(sort_core(G, pos, n, s));
     if (n > 0 && (d_keys || d_perm)) {
         if (d_perm)
-            AW_CUDA(cudaMemcpyAsync(d_perm, G.pw.perm.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+            AW_CUDA(cudaMemcpyAsync(d_perm, G.pw.sorted, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         if (d_keys) {
-            k_gather<<<nblk(n), 256, 0, s>>>(G.pw.perm.p, n, pos, PArr{nullptr, 3, 1}, G.pw.soa.p, nullptr, nullptr,
+            k_gather<<<nblk(n), 256, 0, s>>>(G.pw.sorted, n, pos, PArr{nullptr, 3, 1}, G.pw.soa.p, nullptr, nullptr,
                                              G.pw.keys.p, d_keys);
             AW_LAUNCH();
         }
@@ -479,7 +928,15 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
     MsbgState& G = g->st;
     const float* un[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     const float* uo[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
-    return g2p_launch(G, d_pos, 0, d_vel, 0, n, alpha, un, uo, (cudaStream_t)s_);
+    if (n == 0) return AW_OK;
+    cudaStream_t s = (cudaStream_t)s_;
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, un, G.tiles_new.p, s));
+    AW_TRY(build_tiles(G, uo, G.tiles_old.p, s));
+    k_g2p_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), PArr{d_pos, 3, 1}, PArrW{d_vel, 3, 1}, n, alpha, G.tile_off.p,
+                                        G.tiles_new.p, G.tiles_old.p);
+    AW_LAUNCH();
+    return AW_OK;
 }
 
 extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw_stream s_) {
@@ -487,7 +944,10 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     MsbgState& G = g->st;
     const float* u[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
-    return advect_launch(G, d_pos, 0, n, dt, u, (cudaStream_t)s_);
+    if (n == 0) return AW_OK;
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, u, G.tiles_new.p, (cudaStream_t)s_));
+    return advect_tiles(G, d_pos, 0, n, dt, G.tiles_new.p, (cudaStream_t)s_);
 }
 
 extern "C" aw_status aw_sample_velocity(aw_msbg* g, const float* d_points, int64_t n, int32_t old, float* d_out,
@@ -497,8 +957,11 @@ extern "C" aw_status aw_sample_velocity(aw_msbg* g, const float* d_points, int64
     if (n == 0) return AW_OK;
     MsbgState& G = g->st;
     int base = old ? AW_VELOCITY_OLD_X : AW_VELOCITY_X;
-    Field3 f{{G.ch[base], G.ch[base + 1], G.ch[base + 2]}};
-    k_sample<<<nblk(n), 256, 0, (cudaStream_t)s_>>>(G.view0(), PArr{d_points, 3, 1}, n, f, d_out);
+    const float* u[3] = {G.ch[base], G.ch[base + 1], G.ch[base + 2]};
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, u, G.tiles_old.p, (cudaStream_t)s_));
+    k_sample_tiles<<<nblk(n), 256, 0, (cudaStream_t)s_>>>(G.view0(), PArr{d_points, 3, 1}, n, G.tile_off.p,
+                                                          G.tiles_old.p, d_out);
     AW_LAUNCH();
     return AW_OK;
 }

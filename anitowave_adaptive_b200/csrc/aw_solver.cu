@@ -16,6 +16,7 @@
 // block and end in an FP64 dense solve (Cholesky inverse built on the device each setup).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 
@@ -41,8 +42,11 @@ struct MGLevel {
     std::vector<int> h_res;
     DBuf<uint32_t> off[4];
     uint32_t tot[4] = {0, 0, 0, 0};
-    DBuf<int> list[2];
-    int nlist[2] = {0, 0};
+    // CTA batches: [0]/[1] blocks of one colour, [2] all blocks; each entry {first, count, res, 0}
+    DBuf<int4> desc[3];
+    DBuf<int> blocks[3];
+    int ndesc[3] = {0, 0, 0};
+    size_t smem_smooth = 0, smem_x = 0, smem_x64 = 0;
     int maxres = 0;
     DBuf<float> W[3], bbar[3];
     DBuf<uint8_t> fluid;
@@ -74,6 +78,17 @@ struct aw_solver {
     aw::DBuf<double> p64tmp;
     aw::DBuf<double> partials, norm;
     size_t smem_max = 0;
+    // the whole V-cycle as a CUDA graph, captured once per (x0, b0) binding
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t cycle = nullptr;
+    const void* cycle_x0 = nullptr;
+    const void* cycle_b0 = nullptr;
+    unsigned long long cycle_kernels = 0;
+    bool use_graph = true;
+    ~aw_solver() {
+        if (cycle) cudaGraphExecDestroy(cycle);
+        if (cap) cudaStreamDestroy(cap);
+    }
 };
 
 namespace aw {
@@ -180,185 +195,278 @@ struct Coef3 {
     const float* w[3];
 };
 
-// Write a block of x back (FP32, or FP16 with a fresh per-block scale).
-__device__ inline void store_x(const LevelView& L, const XStore& x, int b, int r, const float* xs, float* red) {
+// ------------------------------------------------------------------------------------------------
+// Batched block kernels.  A CTA serves `count` blocks ("slots") of one resolution r, listed
+// contiguously: 1 block of 8^3 or 16^3 cells, 4 of 4^3, 32 of 2^3, 256 of 1^3.  Every slot keeps
+// its block and a one-cell halo in shared memory; slots never interact (same colour = no shared
+// faces), so each slot's arithmetic, early exit and activation are exactly those of a CTA that
+// owns one block.
+// ------------------------------------------------------------------------------------------------
+struct Batch {
+    const int4* desc;  // {first index into blocks, count, res, 0}
+    const int* blocks;
+};
+
+__device__ inline float slot_get(const XStore& x, const LevelView& L, int b, uint32_t i) { return x.get(L.off[0][b] + i, b); }
+
+// Stage x of every slot (block interior + halo faces) into xs[slot * X3 + ...].
+__device__ inline void stage_slots(const LevelView& L, const XStore& x, const int* sb, int G, int r, float* xs, int stride) {
+    const int R2 = r + 2, n3 = r * r * r, rr = r * r;
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        if (b < 0) continue;
+        const int cx = i % r, cy = (i / r) % r, cz = i / rr;
+        xs[sl * stride + xi3(cx, cy, cz, R2)] = slot_get(x, L, b, (uint32_t)i);
+    }
+    for (int t = threadIdx.x; t < G * 6 * rr; t += blockDim.x) {
+        const int sl = t / (6 * rr), rem0 = t - sl * 6 * rr;
+        const int b = sb[sl];
+        if (b < 0) continue;
+        const int face = rem0 / rr, rem = rem0 - face * rr;
+        const int a = face >> 1, sd = (face & 1) ? 1 : -1;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        int c[3], cb[3];
+        c[a] = sd > 0 ? r - 1 : 0;
+        c[t1] = rem % r;
+        c[t2] = rem / r;
+        bcoord(L.g, b, cb);
+        const float v = ghost_val(L, x, b, cb, c, a, sd);
+        int q[3] = {c[0], c[1], c[2]};
+        q[a] += sd;
+        xs[sl * stride + xi3(q[0], q[1], q[2], R2)] = v;
+    }
+}
+
+// Write every slot's x back: FP32, or FP16 with a fresh per-block scale.
+__device__ inline void store_slots(const LevelView& L, const XStore& x, const int* sb, int G, int r, const float* xs,
+                                   int stride, int* smax) {
     const int R2 = r + 2, n3 = r * r * r;
-    const uint32_t oc = L.off[0][b];
     if (x.f) {
-        for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-            int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-            x.f[oc + i] = xs[xi3(cx, cy, cz, R2)];
+        for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+            const int sl = t / n3, i = t - sl * n3;
+            const int b = sb[sl];
+            if (b < 0) continue;
+            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+            x.f[L.off[0][b] + i] = xs[sl * stride + xi3(cx, cy, cz, R2)];
         }
         return;
     }
-    float m = 0.f;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        m = fmaxf(m, fabsf(xs[xi3(cx, cy, cz, R2)]));
+    for (int t = threadIdx.x; t < G; t += blockDim.x) smax[t] = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        if (sb[sl] < 0) continue;
+        const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        atomicMax(&smax[sl], __float_as_int(fabsf(xs[sl * stride + xi3(cx, cy, cz, R2)])));
     }
-    m = block_max(m, red);
-    const float scale = m > 0.f ? m * (1.f / 32768.f) : 0.f;
-    const float inv = m > 0.f ? 32768.f / m : 0.f;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        x.h[oc + i] = __float2half_rn(xs[xi3(cx, cy, cz, R2)] * inv);
+    __syncthreads();
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        if (b < 0) continue;
+        const float m = __int_as_float(smax[sl]);
+        const float inv = m > 0.f ? 32768.f / m : 0.f;
+        const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+        x.h[L.off[0][b] + i] = __float2half_rn(xs[sl * stride + xi3(cx, cy, cz, R2)] * inv);
     }
-    if (threadIdx.x == 0) x.scale[b] = scale;
+    for (int t = threadIdx.x; t < G; t += blockDim.x)
+        if (sb[t] >= 0) {
+            const float m = __int_as_float(smax[t]);
+            x.scale[sb[t]] = m > 0.f ? m * (1.f / 32768.f) : 0.f;
+        }
 }
 
-// smoothActiveBlocks (Smoother.cuh:105-202) for one block colour.
+__host__ __device__ inline int smooth_slot_floats(int r) {
+    return (r + 2) * (r + 2) * (r + 2) + r * r * r + 3 * (r + 1) * r * r;
+}
+
+// smoothActiveBlocks (Smoother.cuh:105-202) for one block colour, batched.
 __global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
-                                                const uint8_t* __restrict__ fluid, const int* __restrict__ list,
+                                                const uint8_t* __restrict__ fluid, Batch B,
                                                 const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
                                                 SmoothParams P) {
     extern __shared__ float sm[];
-    __shared__ float red[33];
-    const int b = list[blockIdx.x];
-    if (!status[b]) return;
-    const int r = L.res[b];
-    const int R2 = r + 2, n3 = r * r * r, nf = (r + 1) * r * r;
-    float* xs = sm;
-    float* bs = xs + R2 * R2 * R2;
-    float* Ws = bs + n3;
-    uint8_t* fs = (uint8_t*)(Ws + 3 * nf);
-    int cb[3];
-    bcoord(L.g, b, cb);
-    const uint32_t oc = L.off[0][b];
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        bs[i] = bvec[oc + i];
-        fs[i] = fluid[oc + i];
+    __shared__ int sb[256], smr[256], sdone[256];
+    __shared__ float sinit[256];
+    const int4 d = B.desc[blockIdx.x];
+    const int G = d.y, r = d.z;
+    const int R2 = r + 2, n3 = r * r * r, nf = (r + 1) * r * r, X3 = R2 * R2 * R2;
+    const int per = smooth_slot_floats(r);
+    uint8_t* fsb = (uint8_t*)(sm + G * per);
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        const int b = B.blocks[d.x + t];
+        sb[t] = status[b] ? b : -1;
+        smr[t] = 0;
+        sdone[t] = 0;
+        sinit[t] = -1.f;
     }
-    for (int i = threadIdx.x; i < 3 * nf; i += blockDim.x) {
-        int a = i / nf;
-        Ws[i] = W.w[a][L.off[1 + a][b] + (i - a * nf)];
-    }
-    stage_x(L, x, b, cb, r, xs);
     __syncthreads();
-    float init = -1.f, mr = 0.f;
+    if (!__syncthreads_or(threadIdx.x < G && sb[threadIdx.x] >= 0)) return;
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        if (b < 0) continue;
+        const uint32_t oc = L.off[0][b];
+        sm[sl * per + X3 + i] = bvec[oc + i];
+        fsb[sl * n3 + i] = fluid[oc + i];
+    }
+    for (int t = threadIdx.x; t < G * 3 * nf; t += blockDim.x) {
+        const int sl = t / (3 * nf), j = t - sl * 3 * nf;
+        const int b = sb[sl];
+        if (b < 0) continue;
+        const int a = j / nf;
+        sm[sl * per + X3 + n3 + j] = W.w[a][L.off[1 + a][b] + (j - a * nf)];
+    }
+    stage_slots(L, x, sb, G, r, sm, per);
+    __syncthreads();
     const int sy = R2, sz = R2 * R2;
     for (int bi = 0; bi < P.iters; ++bi) {
-        float lmax = 0.f;
         for (int col = 0; col < 2; ++col) {
-            for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-                int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+            for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+                const int sl = t / n3, i = t - sl * n3;
+                if (sb[sl] < 0 || sdone[sl]) continue;
+                const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
                 if (((cx + cy + cz) & 1) != col) continue;
-                if (P.check_fluid && !fs[i]) continue;
-                float wW = Ws[fidx(0, cx, cy, cz, r)];
-                float wE = Ws[fidx(0, cx + 1, cy, cz, r)];
-                float wS = Ws[nf + fidx(1, cx, cy, cz, r)];
-                float wN = Ws[nf + fidx(1, cx, cy + 1, cz, r)];
-                float wB = Ws[2 * nf + fidx(2, cx, cy, cz, r)];
-                float wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, r)];
-                float diag = -(wW + wE + wS + wN + wB + wT);
+                if (P.check_fluid && !fsb[sl * n3 + i]) continue;
+                float* xs = sm + sl * per;
+                const float* Ws = xs + X3 + n3;
+                const float wW = Ws[fidx(0, cx, cy, cz, r)];
+                const float wE = Ws[fidx(0, cx + 1, cy, cz, r)];
+                const float wS = Ws[nf + fidx(1, cx, cy, cz, r)];
+                const float wN = Ws[nf + fidx(1, cx, cy + 1, cz, r)];
+                const float wB = Ws[2 * nf + fidx(2, cx, cy, cz, r)];
+                const float wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, r)];
+                const float diag = -(wW + wE + wS + wN + wB + wT);
                 if (fabsf(diag) < 1e-9f) continue;
-                int q = xi3(cx, cy, cz, R2);
-                float xc = xs[q];
-                float Ax = wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] + wB * xs[q - sz] +
-                           wT * xs[q + sz] + diag * xc;
-                float res = bs[i] - Ax;
+                const int q = xi3(cx, cy, cz, R2);
+                const float xc = xs[q];
+                const float Ax = wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] + wB * xs[q - sz] +
+                                 wT * xs[q + sz] + diag * xc;
+                const float res = xs[X3 + i] - Ax;
                 xs[q] = xc + P.omega * (res / diag);
-                lmax = fmaxf(lmax, fabsf(res));
+                atomicMax(&smr[sl], __float_as_int(fabsf(res)));
             }
             __syncthreads();
         }
-        mr = block_max(lmax, red);
-        if (bi == 0) init = mr;
-        if (init > 1e-9f && mr < init * P.target) break;
+        // per-slot early exit (block-uniform); smr keeps the last executed sweep's max
+        int more = 0;
+        for (int t = threadIdx.x; t < G; t += blockDim.x) {
+            if (sb[t] < 0 || sdone[t]) continue;
+            const float mr = __int_as_float(smr[t]);
+            if (bi == 0) sinit[t] = mr;
+            if (sinit[t] > 1e-9f && mr < sinit[t] * P.target) sdone[t] = 1;
+            else if (bi + 1 < P.iters) {
+                smr[t] = 0;
+                more = 1;
+            }
+        }
+        if (!__syncthreads_or(more)) break;
     }
-    store_x(L, x, b, r, xs, red);
-    if (threadIdx.x == 0 && mr > P.theta) {
+    __syncthreads();
+    int* smax = sdone;  // reused as per-slot |x| max for FP16 storage
+    store_slots(L, x, sb, G, r, sm, per, smax);
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        const int b = sb[t];
+        if (b < 0 || !(__int_as_float(smr[t]) > P.theta)) continue;
         status_next[b] = 1;
-#pragma unroll
+        int cb[3];
+        bcoord(L.g, b, cb);
         for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int s = -1; s <= 1; s += 2) {
+            for (int sd = -1; sd <= 1; sd += 2) {
                 int nc[3] = {cb[0], cb[1], cb[2]};
-                nc[a] += s;
+                nc[a] += sd;
                 if (inside(L.g, nc)) status_next[bidx(L.g, nc[0], nc[1], nc[2])] = 1;
             }
     }
 }
 
-// computeExplicitResidual (VCycle.cuh:81-131): r = b - A x on every cell of every listed block
-// (air cells get 0 in FV mode); optional per-block partial sums of r^2.
+// computeExplicitResidual (VCycle.cuh:81-131), batched: r = b - A x on every cell (0 on air cells
+// in FV mode); optional per-CTA partial sums of r^2.
 __global__ void __launch_bounds__(256) k_residual(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
-                                                  const uint8_t* __restrict__ fluid, const int* __restrict__ list,
-                                                  int check_fluid, float* __restrict__ rout, double* __restrict__ part) {
+                                                  const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
+                                                  float* __restrict__ rout, double* __restrict__ part) {
     extern __shared__ float sm[];
+    __shared__ int sb[256];
     __shared__ double dred[32];
-    const int b = list[blockIdx.x];
-    const int r = L.res[b];
-    const int R2 = r + 2, n3 = r * r * r;
-    float* xs = sm;
-    int cb[3];
-    bcoord(L.g, b, cb);
-    stage_x(L, x, b, cb, r, xs);
+    const int4 d = B.desc[blockIdx.x];
+    const int G = d.y, r = d.z;
+    const int R2 = r + 2, n3 = r * r * r, X3 = R2 * R2 * R2;
+    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
     __syncthreads();
-    const uint32_t oc = L.off[0][b];
-    const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+    stage_slots(L, x, sb, G, r, sm, X3);
+    __syncthreads();
     const int sy = R2, sz = R2 * R2;
     double acc = 0.0;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        const uint32_t oc = L.off[0][b];
         float rv = 0.f;
         if (!check_fluid || fluid[oc + i]) {
-            float wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
-            float wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
-            float wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
-            float wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
-            float wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
-            float wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
-            float diag = -(wW + wE + wS + wN + wB + wT);
-            int q = xi3(cx, cy, cz, R2);
-            float Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
-                       wB * xs[q - sz] + wT * xs[q + sz];
+            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+            const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+            const float wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
+            const float wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
+            const float wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
+            const float wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
+            const float wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
+            const float wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
+            const float diag = -(wW + wE + wS + wN + wB + wT);
+            const float* xs = sm + sl * X3;
+            const int q = xi3(cx, cy, cz, R2);
+            const float Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                             wB * xs[q - sz] + wT * xs[q + sz];
             rv = bvec[oc + i] - Ax;
         }
         rout[oc + i] = rv;
         acc += (double)rv * (double)rv;
     }
     if (part) {
-        double t = block_sum(acc, dred);
-        if (threadIdx.x == 0) part[blockIdx.x] = t;
+        double tsum = block_sum(acc, dred);
+        if (threadIdx.x == 0) part[blockIdx.x] = tsum;
     }
 }
 
-// FP64 residual of the outer defect correction: r = b - A p (p in FP64), stored as FP32 into the
-// V-cycle right-hand side, with per-block partial sums of r^2.
+// FP64 residual of the outer defect correction, batched: r = b - A p with p in FP64, stored as
+// FP32 into the V-cycle right-hand side, with per-CTA partial sums of r^2.
 __global__ void __launch_bounds__(256) k_residual64(LevelView L, const double* __restrict__ p,
                                                     const float* __restrict__ bvec, Coef3 W,
-                                                    const uint8_t* __restrict__ fluid, const int* __restrict__ list,
-                                                    int check_fluid, float* __restrict__ rout, double* __restrict__ part) {
+                                                    const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
+                                                    float* __restrict__ rout, double* __restrict__ part) {
     extern __shared__ double smd[];
+    __shared__ int sb[256];
     __shared__ double dred[32];
-    const int b = list[blockIdx.x];
-    const int r = L.res[b];
-    const int R2 = r + 2, n3 = r * r * r, rr = r * r;
-    double* xs = smd;
-    int cb[3];
-    bcoord(L.g, b, cb);
-    const uint32_t oc = L.off[0][b];
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        xs[xi3(cx, cy, cz, R2)] = p[oc + i];
+    const int4 d = B.desc[blockIdx.x];
+    const int G = d.y, r = d.z;
+    const int R2 = r + 2, n3 = r * r * r, rr = r * r, X3 = R2 * R2 * R2;
+    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
+    __syncthreads();
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int cx = i % r, cy = (i / r) % r, cz = i / rr;
+        smd[sl * X3 + xi3(cx, cy, cz, R2)] = p[L.off[0][sb[sl]] + i];
     }
-    for (int i = threadIdx.x; i < 6 * rr; i += blockDim.x) {
-        int face = i / rr, rem = i - face * rr;
-        int a = face >> 1, s = (face & 1) ? 1 : -1;
-        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        int c[3];
-        c[a] = s > 0 ? r - 1 : 0;
+    for (int t = threadIdx.x; t < G * 6 * rr; t += blockDim.x) {
+        const int sl = t / (6 * rr), rem0 = t - sl * 6 * rr;
+        const int b = sb[sl];
+        const int face = rem0 / rr, rem = rem0 - face * rr;
+        const int a = face >> 1, sd = (face & 1) ? 1 : -1;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        int c[3], cb[3];
+        c[a] = sd > 0 ? r - 1 : 0;
         c[t1] = rem % r;
         c[t2] = rem / r;
+        bcoord(L.g, b, cb);
         int nc[3] = {cb[0], cb[1], cb[2]};
-        nc[a] += s;
+        nc[a] += sd;
         double v = 0.0;
         if (inside(L.g, nc)) {
-            int n = bidx(L.g, nc[0], nc[1], nc[2]);
-            int rn = L.res[n];
+            const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+            const int rn = L.res[n];
             if (rn) {
                 int q[3];
-                q[a] = s > 0 ? 0 : rn - 1;
+                q[a] = sd > 0 ? 0 : rn - 1;
                 if (rn == r) {
                     q[t1] = c[t1];
                     q[t2] = c[t2];
@@ -379,34 +487,38 @@ __global__ void __launch_bounds__(256) k_residual64(LevelView L, const double* _
             }
         }
         int q[3] = {c[0], c[1], c[2]};
-        q[a] += s;
-        xs[xi3(q[0], q[1], q[2], R2)] = v;
+        q[a] += sd;
+        smd[sl * X3 + xi3(q[0], q[1], q[2], R2)] = v;
     }
     __syncthreads();
-    const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
     const int sy = R2, sz = R2 * R2;
     double acc = 0.0;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        const uint32_t oc = L.off[0][b];
         double rv = 0.0;
         if (!check_fluid || fluid[oc + i]) {
-            double wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
-            double wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
-            double wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
-            double wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
-            double wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
-            double wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
-            double diag = -(wW + wE + wS + wN + wB + wT);
-            int q = xi3(cx, cy, cz, R2);
-            double Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
-                        wB * xs[q - sz] + wT * xs[q + sz];
+            const int cx = i % r, cy = (i / r) % r, cz = i / rr;
+            const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+            const double wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
+            const double wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
+            const double wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
+            const double wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
+            const double wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
+            const double wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
+            const double diag = -(wW + wE + wS + wN + wB + wT);
+            const double* xs = smd + sl * X3;
+            const int q = xi3(cx, cy, cz, R2);
+            const double Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                              wB * xs[q - sz] + wT * xs[q + sz];
             rv = (double)bvec[oc + i] - Ax;
         }
         rout[oc + i] = (float)rv;
         acc += rv * rv;
     }
-    double t = block_sum(acc, dred);
-    if (threadIdx.x == 0) part[blockIdx.x] = t;
+    double tsum = block_sum(acc, dred);
+    if (threadIdx.x == 0) part[blockIdx.x] = tsum;
 }
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
@@ -433,21 +545,22 @@ __global__ void k_sumsq(const float* __restrict__ v, const uint8_t* __restrict__
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 
-// restrictResidualsKernel (MultigridTransfer.cuh:9-59): 8-child sum, or copy for a block whose
-// resolution stays one cell.  Coarse air cells get 0.
-__global__ void k_restrict(LevelView F, LevelView K, const float* __restrict__ r, float* __restrict__ bc,
-                           const uint8_t* __restrict__ fluid_c, int check_fluid) {
-    const int b = blockIdx.x;
-    const int rc = K.res[b], rf = F.res[b];
-    if (!rc) return;
-    const bool halved = rf == 2 * rc;
-    const uint32_t of = F.off[0][b], oc = K.off[0][b];
-    const int n3 = rc * rc * rc;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int x = i % rc, y = (i / rc) % rc, z = i / (rc * rc);
+// restrictResidualsKernel (MultigridTransfer.cuh:9-59), batched over the coarse level's blocks:
+// 8-child sum, or a copy for a block that keeps one cell.  Coarse air cells get 0.
+__global__ void __launch_bounds__(256) k_restrict(LevelView F, LevelView K, const float* __restrict__ r,
+                                                  float* __restrict__ bc, const uint8_t* __restrict__ fluid_c,
+                                                  int check_fluid, Batch B) {
+    const int4 d = B.desc[blockIdx.x];
+    const int G = d.y, rc = d.z, n3 = rc * rc * rc;
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = B.blocks[d.x + sl];
+        const int rf = F.res[b];
+        const uint32_t of = F.off[0][b], oc = K.off[0][b];
         float s;
-        if (halved) {
-            int fx = 2 * x, fy = 2 * y, fz = 2 * z;
+        if (rf == 2 * rc) {
+            const int x = i % rc, y = (i / rc) % rc, z = i / (rc * rc);
+            const int fx = 2 * x, fy = 2 * y, fz = 2 * z;
             s = r[of + cidx(fx, fy, fz, rf)];
             s += r[of + cidx(fx + 1, fy, fz, rf)];
             s += r[of + cidx(fx, fy + 1, fz, rf)];
@@ -463,39 +576,34 @@ __global__ void k_restrict(LevelView F, LevelView K, const float* __restrict__ r
     }
 }
 
-// prolongateCorrection (MultigridTransfer.cuh:63-102): x_f += x_c[parent] on fluid cells.
+// prolongateCorrection (MultigridTransfer.cuh:63-102), batched over the fine level's blocks:
+// x_f += x_c[parent] on fluid cells (FP16 fine storage is decoded, updated and re-encoded).
 __global__ void __launch_bounds__(256) k_prolong(LevelView F, LevelView K, XStore xf, XStore xc,
-                                                 const uint8_t* __restrict__ fluid_f, int check_fluid) {
+                                                 const uint8_t* __restrict__ fluid_f, int check_fluid, Batch B) {
     extern __shared__ float sm[];
-    __shared__ float red[33];
-    const int b = blockIdx.x;
-    const int rc = K.res[b], rf = F.res[b];
-    if (!rc || !rf) return;
-    const bool halved = rf == 2 * rc;
-    const uint32_t of = F.off[0][b], oc = K.off[0][b];
-    const int n3 = rf * rf * rf;
-    if (xf.f) {
-        for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-            if (check_fluid && !fluid_f[of + i]) continue;
-            int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
-            uint32_t ci = halved ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
-            xf.f[of + i] += xc.get(oc + ci, b);
-        }
-        return;
-    }
-    // FP16 fine storage: decode, add, re-encode with a new block scale
-    const int R2 = rf + 2;
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
-        float v = xf.get(of + i, b);
-        if (!check_fluid || fluid_f[of + i]) {
-            uint32_t ci = halved ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
-            v += xc.get(oc + ci, b);
-        }
-        sm[xi3(x, y, z, R2)] = v;
-    }
+    __shared__ int sb[256], smax[256];
+    const int4 d = B.desc[blockIdx.x];
+    const int G = d.y, rf = d.z, n3 = rf * rf * rf;
+    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
     __syncthreads();
-    store_x(F, xf, b, rf, sm, red);
+    const int R2 = rf + 2, X3 = R2 * R2 * R2;
+    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+        const int sl = t / n3, i = t - sl * n3;
+        const int b = sb[sl];
+        const int rc = K.res[b];
+        const uint32_t of = F.off[0][b], oc = K.off[0][b];
+        const int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
+        float add = 0.f;
+        if (rc && (!check_fluid || fluid_f[of + i])) {
+            const uint32_t ci = (rf == 2 * rc) ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
+            add = xc.get(oc + ci, b);
+        }
+        if (xf.f) xf.f[of + i] += add;
+        else sm[sl * X3 + xi3(x, y, z, R2)] = xf.get(of + i, b) + add;
+    }
+    if (xf.f) return;
+    __syncthreads();
+    store_slots(F, xf, sb, G, rf, sm, X3, smax);
 }
 
 __global__ void k_zero_scale(float* s, int n) {
@@ -917,9 +1025,50 @@ static XStore xstore(aw_solver* S, int m) {
 }
 static const float* bptr(aw_solver* S, int m) { return (m == 0 && S->b0) ? S->b0 : S->lv[m].b.p; }
 static Coef3 coef(const MGLevel& L) { return Coef3{{L.W[0].p, L.W[1].p, L.W[2].p}}; }
-static size_t smooth_smem(int r) {
-    return (size_t)((r + 2) * (r + 2) * (r + 2) + r * r * r + 3 * (r + 1) * r * r) * sizeof(float) + (size_t)r * r * r + 16;
+static int slots_per_cta(int r) { return std::max(1, std::min(256, 256 / (r * r * r))); }
+
+// Build the CTA batches of one block-structured level from its per-block resolutions.
+static aw_status build_batches(MGLevel& L, const Geo& geo) {
+    const int nb = (int)L.h_res.size();
+    for (int k = 0; k < 3; ++k) {
+        std::vector<int> by_res[17];
+        for (int b = 0; b < nb; ++b) {
+            const int r = L.h_res[b];
+            if (!r) continue;
+            if (k < 2) {
+                int c[3];
+                bcoord(geo, b, c);
+                if (((c[0] + c[1] + c[2]) & 1) != k) continue;
+            }
+            by_res[r].push_back(b);
+        }
+        std::vector<int> blocks;
+        std::vector<int4> desc;
+        for (int r = 16; r >= 1; --r) {
+            const int G = slots_per_cta(r);
+            for (size_t i = 0; i < by_res[r].size(); i += G) {
+                const int cnt = (int)std::min<size_t>(G, by_res[r].size() - i);
+                desc.push_back(make_int4((int)blocks.size(), cnt, r, 0));
+                for (int j = 0; j < cnt; ++j) blocks.push_back(by_res[r][i + j]);
+            }
+            if (!by_res[r].empty()) {
+                const size_t Gm = (size_t)std::min<int>(G, (int)by_res[r].size());
+                L.smem_smooth = std::max(L.smem_smooth, Gm * (smooth_slot_floats(r) * sizeof(float) + (size_t)r * r * r) + 16);
+                L.smem_x = std::max(L.smem_x, Gm * (size_t)(r + 2) * (r + 2) * (r + 2) * sizeof(float));
+                L.smem_x64 = std::max(L.smem_x64, Gm * (size_t)(r + 2) * (r + 2) * (r + 2) * sizeof(double));
+            }
+        }
+        L.ndesc[k] = (int)desc.size();
+        if (L.ndesc[k]) {
+            AW_TRY(L.desc[k].alloc(desc.size()));
+            AW_TRY(L.blocks[k].alloc(blocks.size()));
+            AW_CUDA(cudaMemcpy(L.desc[k].p, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice));
+            AW_CUDA(cudaMemcpy(L.blocks[k].p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
+        }
+    }
+    return AW_OK;
 }
+static Batch batch(const MGLevel& L, int k) { return Batch{L.desc[k].p, L.blocks[k].p}; }
 static bool fv(const aw_solver* S) { return S->d.operator_mode == AW_OPERATOR_FV; }
 
 static Uniform uniform_of(aw_solver* S, int m) {
@@ -971,14 +1120,13 @@ static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t 
     SmoothParams P{S->d.omega, S->d.target_reduction, S->d.theta, S->d.block_iterations, cf};
     LevelView V = lview(S, m);
     XStore x = xstore(S, m);
-    size_t smem = smooth_smem(L.maxres);
     int cur = 0;
     for (int it = 0; it < iterations; ++it) {
         AW_CUDA(cudaMemsetAsync(L.status[cur ^ 1].p, 0, nb, s));
         for (int rb = 0; rb < 2; ++rb) {
-            if (!L.nlist[rb]) continue;
-            k_smooth<<<L.nlist[rb], 256, smem, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, L.list[rb].p, L.status[cur].p,
-                                                    L.status[cur ^ 1].p, P);
+            if (!L.ndesc[rb]) continue;
+            k_smooth<<<L.ndesc[rb], 256, L.smem_smooth, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, rb),
+                                                              L.status[cur].p, L.status[cur ^ 1].p, P);
             AW_LAUNCH();
         }
         cur ^= 1;
@@ -997,14 +1145,9 @@ static aw_status residual_level(aw_solver* S, int m, double* part, cudaStream_t 
     }
     LevelView V = lview(S, m);
     XStore x = xstore(S, m);
-    size_t smem = (size_t)(L.maxres + 2) * (L.maxres + 2) * (L.maxres + 2) * sizeof(float);
-    int off = 0;
-    for (int rb = 0; rb < 2; ++rb) {
-        if (!L.nlist[rb]) continue;
-        k_residual<<<L.nlist[rb], 256, smem, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, L.list[rb].p, cf, L.r.p,
-                                                  part ? part + off : nullptr);
+    if (L.ndesc[2]) {
+        k_residual<<<L.ndesc[2], 256, L.smem_x, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, 2), cf, L.r.p, part);
         AW_LAUNCH();
-        off += L.nlist[rb];
     }
     return AW_OK;
 }
@@ -1020,8 +1163,10 @@ static aw_status restrict_level(aw_solver* S, int m, cudaStream_t s) {
         AW_LAUNCH();
         return AW_OK;
     }
-    k_restrict<<<S->g->st.nb, 128, 0, s>>>(lview(S, m), lview(S, m + 1), F.r.p, K.b.p, K.fluid.p, cf);
-    AW_LAUNCH();
+    if (K.ndesc[2]) {
+        k_restrict<<<K.ndesc[2], 256, 0, s>>>(lview(S, m), lview(S, m + 1), F.r.p, K.b.p, K.fluid.p, cf, batch(K, 2));
+        AW_LAUNCH();
+    }
     return AW_OK;
 }
 
@@ -1039,9 +1184,11 @@ static aw_status prolong_level(aw_solver* S, int m, cudaStream_t s) {
         AW_LAUNCH();
         return AW_OK;
     }
-    size_t smem = F.half ? (size_t)(F.maxres + 2) * (F.maxres + 2) * (F.maxres + 2) * sizeof(float) : 0;
-    k_prolong<<<S->g->st.nb, 256, smem, s>>>(lview(S, m), lview(S, m + 1), xstore(S, m), xstore(S, m + 1), F.fluid.p, cf);
-    AW_LAUNCH();
+    if (F.ndesc[2]) {
+        k_prolong<<<F.ndesc[2], 256, F.half ? F.smem_x : 0, s>>>(lview(S, m), lview(S, m + 1), xstore(S, m),
+                                                                  xstore(S, m + 1), F.fluid.p, cf, batch(F, 2));
+        AW_LAUNCH();
+    }
     return AW_OK;
 }
 
@@ -1099,7 +1246,7 @@ extern "C" aw_status aw_solver_default_desc(int32_t mode, aw_solver_desc* d) {
         d->block_iterations = 2;
         d->omega = 1.0f;
         d->target_reduction = 0.33f;
-        d->theta = 0.0f;
+        d->theta = -1.0f;  // every block stays active (no residual-threshold deactivation)
     }
     return AW_OK;
 }
@@ -1156,25 +1303,12 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         }
         L.h_res.resize(nb);
         AW_CUDA(cudaMemcpy(L.h_res.data(), L.res.p, nb * sizeof(int), cudaMemcpyDeviceToHost));
-        std::vector<int> lists[2];
-        for (int b = 0; b < nb; ++b) {
-            if (!L.h_res[b]) continue;
-            int c[3];
-            bcoord(G.geo, b, c);
-            lists[(c[0] + c[1] + c[2]) & 1].push_back(b);
-            L.maxres = std::max(L.maxres, L.h_res[b]);
-        }
+        for (int b = 0; b < nb; ++b) L.maxres = std::max(L.maxres, L.h_res[b]);
         if (L.maxres == 0) {
             S->lv.resize(m);
             break;
         }
-        for (int rb = 0; rb < 2; ++rb) {
-            L.nlist[rb] = (int)lists[rb].size();
-            if (L.nlist[rb]) {
-                AW_TRY(L.list[rb].alloc(L.nlist[rb]));
-                AW_CUDA(cudaMemcpy(L.list[rb].p, lists[rb].data(), L.nlist[rb] * sizeof(int), cudaMemcpyHostToDevice));
-            }
-        }
+        AW_TRY(build_batches(L, G.geo));
         AW_TRY(L.status[0].alloc(nb));
         AW_TRY(L.status[1].alloc(nb));
         L.half = (d->precision == AW_PRECISION_MIXED) && m >= 1 && m < M - 1 + (ref ? 0 : 1) && L.maxres > 1;
@@ -1196,7 +1330,7 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
             AW_TRY(L.W[a].alloc(L.nface(a)));
             AW_TRY(L.bbar[a].alloc(L.nface(a)));
         }
-        S->smem_max = std::max(S->smem_max, smooth_smem(L.maxres));
+        S->smem_max = std::max({S->smem_max, L.smem_smooth, L.smem_x, L.smem_x64});
     }
     S->nmsbg = (int)S->lv.size();
     // coefficients of the block-structured levels
@@ -1273,6 +1407,7 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
     size_t nparts = (size_t)nb + 1024;
     AW_TRY(S->partials.alloc(nparts));
     AW_TRY(S->norm.alloc(2));
+    S->use_graph = getenv("AW_NO_GRAPH") == nullptr;
     AW_CUDA(cudaDeviceSynchronize());
     *out = S.release();
     // default setup: every cell fluid
@@ -1361,6 +1496,47 @@ extern "C" aw_status aw_mg_prolongate(aw_solver* S, int32_t m, aw_stream s) {
     AW_CHECK_ARG(S && m >= 0 && m + 1 < (int)S->lv.size(), "bad argument");
     return prolong_level(S, m, (cudaStream_t)s);
 }
+// One V-cycle, replayed from a CUDA graph (captured on first use for the current level-0 x/b).
+static aw_status run_vcycle(aw_solver* S, cudaStream_t s) {
+    if (!S->use_graph) return vcycle(S, 0, s);
+    const void* x0 = S->x0 ? (const void*)S->x0 : (const void*)S->lv[0].x.p;
+    const void* b0 = S->b0 ? (const void*)S->b0 : (const void*)S->lv[0].b.p;
+    if (!S->cycle || S->cycle_x0 != x0 || S->cycle_b0 != b0) {
+        if (S->cycle) {
+            cudaGraphExecDestroy(S->cycle);
+            S->cycle = nullptr;
+        }
+        if (!S->cap) AW_CUDA(cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking));
+        const unsigned long long l0 = g_launches;
+        AW_CUDA(cudaStreamBeginCapture(S->cap, cudaStreamCaptureModeThreadLocal));
+        aw_status st = vcycle(S, 0, S->cap);
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(S->cap, &graph);
+        S->cycle_kernels = g_launches - l0;
+        g_launches = l0;
+        if (st != AW_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return set_error(AW_ERR_CUDA, "V-cycle capture: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&S->cycle, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            S->cycle = nullptr;
+            return set_error(AW_ERR_CUDA, "V-cycle graph instantiate: %s", cudaGetErrorString(e));
+        }
+        S->cycle_x0 = x0;
+        S->cycle_b0 = b0;
+    }
+    AW_CUDA(cudaGraphLaunch(S->cycle, s));
+    g_launches += S->cycle_kernels;
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solver_coarsest_solve(aw_solver* S, aw_stream s) {
+    AW_CHECK_ARG(S, "null solver");
+    return coarsest(S, (int)S->lv.size() - 1, (cudaStream_t)s);
+}
 extern "C" aw_status aw_vcycle_run(aw_solver* S, aw_stream s) {
     AW_CHECK_ARG(S, "null solver");
     return vcycle(S, 0, (cudaStream_t)s);
@@ -1391,7 +1567,7 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
     AW_TRY(read_norm(S, nparts, s, &bn));
     if (!(bn == bn) || std::isinf(bn)) return set_error(AW_ERR_NAN, "right-hand side contains NaN/Inf");
     if (bn == 0.0) bn = 1.0;
-    const int nlist = L0.nlist[0] + L0.nlist[1];
+    const int nlist = L0.ndesc[2];
     int it = 0;
     double rel = 0;
     aw_status st = AW_OK;
@@ -1414,24 +1590,18 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
                 st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d cycles", rel, it);
                 break;
             }
-            st = vcycle(S, 0, s);
+            st = run_vcycle(S, s);
             if (st != AW_OK) break;
         }
         S->x0 = nullptr;
         S->b0 = nullptr;
     } else {
         double* p = (double*)d_p;
-        size_t smem = (size_t)(L0.maxres + 2) * (L0.maxres + 2) * (L0.maxres + 2) * sizeof(double);
         LevelView V = lview(S, 0);
         for (;; ++it) {
-            int off = 0;
-            for (int rb = 0; rb < 2; ++rb) {
-                if (!L0.nlist[rb]) continue;
-                k_residual64<<<L0.nlist[rb], 256, smem, s>>>(V, p, d_b, coef(L0), L0.fluid.p, L0.list[rb].p, cf, L0.b.p,
-                                                             S->partials.p + off);
-                off += L0.nlist[rb];
-                ++g_launches;
-            }
+            k_residual64<<<L0.ndesc[2], 256, L0.smem_x64, s>>>(V, p, d_b, coef(L0), L0.fluid.p, batch(L0, 2), cf,
+                                                                L0.b.p, S->partials.p);
+            ++g_launches;
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) {
                 st = set_error(AW_ERR_CUDA, "k_residual64: %s", cudaGetErrorString(e));
@@ -1452,7 +1622,7 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
             }
             st = zero_x(S, 0, s);
             if (st != AW_OK) break;
-            st = vcycle(S, 0, s);
+            st = run_vcycle(S, s);
             if (st != AW_OK) break;
             k_accum64<<<nblk(nc), 256, 0, s>>>(p, L0.x.p, nc);
             ++g_launches;

@@ -181,7 +181,7 @@ def run_ours(args, ws, rank, local):
     torch.cuda.set_device(local)
     S = scenes.config(WORKLOAD)
     g = aw.build_grid(S)
-    F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_FP32, tolerance=1e-6,
+    F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_MIXED, tolerance=1e-6,
                 max_cycles=100)
     for _ in range(args.warmup):
         F.step()

@@ -92,7 +92,8 @@ aw_status aw_msbg_destroy(aw_msbg* g);
 aw_status aw_msbg_desc(const aw_msbg* g, aw_grid_desc* out);
 /* initRefinementMap (MSBG.cuh:249-254) */
 aw_status aw_msbg_init_refinement_map(aw_msbg* g, uint32_t value, aw_stream s);
-/* device pointer to the refinement map (u32 per block, x-fastest linear order, MSBG.cuh:161) */
+/* device pointer to the refinement map (u32 per block, x-fastest linear order, MSBG.cuh:161).
+ * After writing it, call aw_msbg_enforce_grading and aw_msbg_allocate again. */
 aw_status aw_msbg_refinement_map(aw_msbg* g, uint32_t** d_levels);
 /* initBlockInfo (MSBG.cuh:256-269): d_coord_morton = 4 u32 per block {x, y, z, morton} */
 aw_status aw_msbg_block_info(aw_msbg* g, uint32_t* d_coord_morton, aw_stream s);
@@ -202,6 +203,9 @@ aw_status aw_mg_residual(aw_solver* sv, int32_t level, aw_stream s);
 aw_status aw_mg_restrict(aw_solver* sv, int32_t level, aw_stream s);
 /* MultigridTransfer::prolongateAndCorrect (MultigridTransfer.cuh:129-149): x[level] += P x[level+1] */
 aw_status aw_mg_prolongate(aw_solver* sv, int32_t level, aw_stream s);
+/* coarsest-level solve (VCycle.cuh:252-256): FP64 dense solve of the uniform coarsest level in FV
+ * mode, coarsest_iterations smoother iterations in reference mode */
+aw_status aw_solver_coarsest_solve(aw_solver* sv, aw_stream s);
 /* VCycleSolver::runCycle(mg, 0) (VCycle.cuh:251-304) on the level-0 arrays x, b */
 aw_status aw_vcycle_run(aw_solver* sv, aw_stream s);
 /* Solve A p = b on level 0 to desc.tolerance.  FP32 precision: p is float*, V-cycles in place.

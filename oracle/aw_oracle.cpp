@@ -140,7 +140,7 @@ struct Params {
     int pre = 2, post = 2, coarsest_iters = 50, block_iters = 2, dense_sweeps = 2;
     double omega = 1.0;
     double target = 0.33;
-    double theta = 0.0;
+    double theta = -1.0;
     int max_exact = 1024;
     double lambda = 1.0;  // prolongation scale
     int coarse_all = 1;   // FV: a coarse cell is fluid iff all its children are fluid
@@ -796,7 +796,8 @@ void restrict_level(Ctx& C, int m) {
                     } else {
                         s = F.r[F.off[0][b] + cidx(x, y, z, rf)];
                     }
-                    K.b[K.off[0][b] + cidx(x, y, z, r)] = s;
+                    uint32_t ci = K.off[0][b] + cidx(x, y, z, r);
+                    K.b[ci] = (C.P.mode == 1 || K.fluid[ci]) ? s : 0.0;
                 }
     }
 }
@@ -1275,6 +1276,10 @@ OC_API void oc_residual(void* h, int m) {
 OC_API void oc_restrict(void* h, int m) { restrict_level(*(Ctx*)h, m); }
 OC_API void oc_prolong(void* h, int m) { prolong_level(*(Ctx*)h, m); }
 OC_API void oc_vcycle(void* h) { vcycle(*(Ctx*)h, 0); }
+OC_API void oc_coarsest(void* h) {
+    Ctx* C = (Ctx*)h;
+    coarsest_solve(*C, (int)C->lv.size() - 1);
+}
 
 // Defect-correction solve of A p = b on level 0 to relative residual tol (FP64 throughout).
 // p (in/out), b (in).  history (optional, max_cycles+1 entries) gets ||r||/||b|| per cycle.

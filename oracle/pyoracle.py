@@ -66,6 +66,7 @@ def lib():
         for fn in ("oc_residual", "oc_restrict", "oc_prolong"):
             getattr(L, fn).argtypes = [P, C.c_int]
         L.oc_vcycle.argtypes = [P]
+        L.oc_coarsest.argtypes = [P]
         L.oc_solve.restype = C.c_int
         L.oc_solve.argtypes = [P, f64p, f64p, C.c_double, C.c_int, C.c_void_p]
         L.oc_apply.argtypes = [P, C.c_int, f64p, f64p]
@@ -141,8 +142,15 @@ class Oracle:
         except Exception:
             pass
 
-    def set_params(self, mode=0, pre=2, post=2, coarsest_iters=50, block_iters=10, dense_sweeps=2,
-                   omega=0.85714, target=0.33, theta=0.0, lam=1.0):
+    def set_params(self, mode=0, pre=2, post=2, coarsest_iters=50, block_iters=None, dense_sweeps=2,
+                   omega=None, target=0.33, theta=None, lam=1.0):
+        """Defaults follow the library's: FV mode (block_iters 2, omega 1, theta 0); reference
+        mode (Smoother.cuh:9-11,286: block_iters 10, omega 0.85714, theta 1e-4); FV mode keeps every
+        block active (theta -1)."""
+        ref = mode == 1
+        block_iters = (10 if ref else 2) if block_iters is None else block_iters
+        omega = (0.85714 if ref else 1.0) if omega is None else omega
+        theta = (1e-4 if ref else -1.0) if theta is None else theta
         lib().oc_set_params(self.h, mode, pre, post, coarsest_iters, block_iters, dense_sweeps, omega, target,
                             theta, lam)
 
@@ -210,6 +218,9 @@ class Oracle:
 
     def vcycle(self):
         lib().oc_vcycle(self.h)
+
+    def coarsest(self):
+        lib().oc_coarsest(self.h)
 
     def solve(self, b, tol=1e-6, max_cycles=100, p0=None):
         n = int(self.level_info(0)[4])
