@@ -207,6 +207,16 @@ struct Batch {
     const int* blocks;
 };
 
+// Every thread of a batched CTA only ever touches cells of one slot (G * r^3 == 256, or G == 1).
+// Reduce a per-thread non-negative value over the threads of each slot: shuffle within aligned
+// groups of min(r^3, 32) lanes, then one shared atomicMax per group.
+__device__ inline void slot_max(int* dst, int n3, float v) {
+    const int grp = n3 < 32 ? n3 : 32;
+    int iv = __float_as_int(v);
+    for (int o = 1; o < grp; o <<= 1) iv = max(iv, __shfl_xor_sync(0xffffffffu, iv, o));
+    if ((threadIdx.x & (grp - 1)) == 0 && iv > 0) atomicMax(dst, iv);
+}
+
 __device__ inline float slot_get(const XStore& x, const LevelView& L, int b, uint32_t i) { return x.get(L.off[0][b] + i, b); }
 
 // Stage x of every slot (block interior + halo faces) into xs[slot * X3 + ...].
@@ -254,11 +264,16 @@ __device__ inline void store_slots(const LevelView& L, const XStore& x, const in
     }
     for (int t = threadIdx.x; t < G; t += blockDim.x) smax[t] = 0;
     __syncthreads();
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        if (sb[sl] < 0) continue;
-        const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        atomicMax(&smax[sl], __float_as_int(fabsf(xs[sl * stride + xi3(cx, cy, cz, R2)])));
+    {
+        float m = 0.f;
+        const int sl = (int)threadIdx.x / n3 < G ? (int)threadIdx.x / n3 : 0;
+        for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
+            const int i = t - (t / n3) * n3;
+            if (sb[t / n3] < 0) continue;
+            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+            m = fmaxf(m, fabsf(xs[(t / n3) * stride + xi3(cx, cy, cz, R2)]));
+        }
+        slot_max(&smax[G == 1 ? 0 : sl], n3, m);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
@@ -321,7 +336,9 @@ __global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const flo
     stage_slots(L, x, sb, G, r, sm, per);
     __syncthreads();
     const int sy = R2, sz = R2 * R2;
+    const int my_slot = G == 1 ? 0 : min((int)threadIdx.x / n3, G - 1);
     for (int bi = 0; bi < P.iters; ++bi) {
+        float lmax = 0.f;
         for (int col = 0; col < 2; ++col) {
             for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
                 const int sl = t / n3, i = t - sl * n3;
@@ -345,10 +362,12 @@ __global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const flo
                                  wT * xs[q + sz] + diag * xc;
                 const float res = xs[X3 + i] - Ax;
                 xs[q] = xc + P.omega * (res / diag);
-                atomicMax(&smr[sl], __float_as_int(fabsf(res)));
+                lmax = fmaxf(lmax, fabsf(res));
             }
             __syncthreads();
         }
+        slot_max(&smr[my_slot], n3, lmax);
+        __syncthreads();
         // per-slot early exit (block-uniform); smr keeps the last executed sweep's max
         int more = 0;
         for (int t = threadIdx.x; t < G; t += blockDim.x) {
