@@ -44,9 +44,11 @@ struct MGLevel {
     uint32_t tot[4] = {0, 0, 0, 0};
     // CTA batches: [0]/[1] blocks of one colour, [2] all blocks; each entry {first, count, res, 0}
     DBuf<int4> desc[3];
-    DBuf<int> blocks[3];
+    std::vector<int> h_blocks[3];  // block of every slot, batch order
+    DBuf<int> meta[3];             // slot metadata (NMETA fields x slots, field-major)
     int ndesc[3] = {0, 0, 0};
-    size_t smem_smooth = 0, smem_x = 0, smem_x64 = 0;
+    // dynamic shared memory of the batched kernels on this level
+    size_t smem_smooth = 0, smem_x64 = 0, smem_prolong = 0, smem_meta = 0;
     int maxres = 0;
     DBuf<float> W[3], bbar[3];
     DBuf<uint8_t> fluid;
@@ -77,7 +79,7 @@ struct aw_solver {
     // mixed precision
     aw::DBuf<double> p64tmp;
     aw::DBuf<double> partials, norm;
-    size_t smem_max = 0;
+    size_t smem_max = 0, smem_max64 = 0;
     // the whole V-cycle as a CUDA graph, captured once per (x0, b0) binding
     cudaStream_t cap = nullptr;
     cudaGraphExec_t cycle = nullptr;
@@ -100,66 +102,6 @@ struct SmoothParams {
 };
 
 __host__ __device__ inline int xi3(int x, int y, int z, int R2) { return (x + 1) + R2 * ((y + 1) + R2 * (z + 1)); }
-
-// Ghost value across face (a, s) of cell c in block b: same level -> mirror cell, coarser
-// neighbour -> parent cell, finer neighbour -> mean of the 4 touching cells, outside the domain
-// or absent -> 0 (Dirichlet / air).
-__device__ inline float ghost_val(const LevelView& L, const XStore& x, int b, const int cb[3], const int c[3], int a, int s) {
-    int nc[3] = {cb[0], cb[1], cb[2]};
-    nc[a] += s;
-    if (!inside(L.g, nc)) return 0.f;
-    const int n = bidx(L.g, nc[0], nc[1], nc[2]);
-    const int rn = L.res[n], r = L.res[b];
-    if (!rn) return 0.f;
-    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-    const int na = s > 0 ? 0 : rn - 1;
-    int q[3];
-    q[a] = na;
-    if (rn == r) {
-        q[t1] = c[t1];
-        q[t2] = c[t2];
-        return x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
-    }
-    if (rn < r) {  // coarser neighbour (2:1 grading: rn == r / 2)
-        q[t1] = min(c[t1] >> 1, rn - 1);
-        q[t2] = min(c[t2] >> 1, rn - 1);
-        return x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
-    }
-    float sum = 0.f;  // finer neighbour (rn == 2 r)
-#pragma unroll
-    for (int d1 = 0; d1 < 2; ++d1)
-#pragma unroll
-        for (int d2 = 0; d2 < 2; ++d2) {
-            q[t1] = min(2 * c[t1] + d1, rn - 1);
-            q[t2] = min(2 * c[t2] + d2, rn - 1);
-            sum += x.get(L.off[0][n] + cidx(q[0], q[1], q[2], rn), n);
-        }
-    return 0.25f * sum;
-}
-
-// Stage x (block + 6 halo faces) into xs[(r+2)^3].
-__device__ inline void stage_x(const LevelView& L, const XStore& x, int b, const int cb[3], int r, float* xs) {
-    const int R2 = r + 2, n3 = r * r * r;
-    const uint32_t oc = L.off[0][b];
-    for (int i = threadIdx.x; i < n3; i += blockDim.x) {
-        int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        xs[xi3(cx, cy, cz, R2)] = x.get(oc + i, b);
-    }
-    const int rr = r * r;
-    for (int i = threadIdx.x; i < 6 * rr; i += blockDim.x) {
-        int face = i / rr, rem = i - face * rr;
-        int a = face >> 1, s = (face & 1) ? 1 : -1;
-        int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        int c[3];
-        c[a] = s > 0 ? r - 1 : 0;
-        c[t1] = rem % r;
-        c[t2] = rem / r;
-        float v = ghost_val(L, x, b, cb, c, a, s);
-        int q[3] = {c[0], c[1], c[2]};
-        q[a] += s;
-        xs[xi3(q[0], q[1], q[2], R2)] = v;
-    }
-}
 
 __device__ inline float block_max(float v, float* red) {
     v = warp_max(v);
@@ -203,9 +145,28 @@ struct Coef3 {
 // owns one block.
 // ------------------------------------------------------------------------------------------------
 struct Batch {
-    const int4* desc;  // {first index into blocks, count, res, 0}
-    const int* blocks;
+    const int4* desc;  // {first slot, count, res, 0}
+    const int* meta;   // batch-ordered slot metadata, NMETA fields x nslots (field-major)
+    int nslots;
 };
+
+// Slot metadata fields.  The host lays them out in batch order when the solver is created, so a CTA
+// reads its slots' block ids, offsets and face neighbours with one coalesced round trip after the
+// descriptor instead of chasing block id -> offsets -> neighbour offsets.
+enum {
+    MF_BLOCK = 0,        // block id
+    MF_OFF = 1,          // 4 fields: cells, faces x, y, z of this level
+    MF_NB = 5,           // 6 directions (2a + (s > 0)) x {neighbour cell offset, kind, neighbour block}
+    MF_FINE_OFF = 23,    // cell offset and resolution of the block on the next finer level
+    MF_FINE_RES = 24,
+    MF_COARSE_OFF = 25,  // ... and on the next coarser level
+    MF_COARSE_RES = 26,
+    NMETA = 27
+};
+
+// Face-neighbour kinds: 0 = outside the domain or absent (ghost 0), 2 = same resolution,
+// 3 = coarser neighbour (parent cell), 4 = finer neighbour (mean of the 4 touching cells).
+enum { NB_NONE = 0, NB_SAME = 2, NB_COARSE = 3, NB_FINE = 4 };
 
 // Every thread of a batched CTA only ever touches cells of one slot (G * r^3 == 256, or G == 1).
 // Reduce a per-thread non-negative value over the threads of each slot: shuffle within aligned
@@ -217,177 +178,367 @@ __device__ inline void slot_max(int* dst, int n3, float v) {
     if ((threadIdx.x & (grp - 1)) == 0 && iv > 0) atomicMax(dst, iv);
 }
 
-__device__ inline float slot_get(const XStore& x, const LevelView& L, int b, uint32_t i) { return x.get(L.off[0][b] + i, b); }
+// ---- asynchronous global -> shared copies (completion via cp.async.wait_all) ----
+__device__ inline uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ inline void cp_async4(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ inline void cp_async8(void* s, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
+}
+__device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Stage x of every slot (block interior + halo faces) into xs[slot * X3 + ...].
-__device__ inline void stage_slots(const LevelView& L, const XStore& x, const int* sb, int G, int r, float* xs, int stride) {
-    const int R2 = r + 2, n3 = r * r * r, rr = r * r;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        if (b < 0) continue;
-        const int cx = i % r, cy = (i / r) % r, cz = i / rr;
-        xs[sl * stride + xi3(cx, cy, cz, R2)] = slot_get(x, L, b, (uint32_t)i);
+// Sources of x for staging: FP32 (copied asynchronously), FP16 + per-block scale (decoded in
+// registers), FP64 (copied asynchronously).
+struct SrcX {
+    XStore x;
+    using T = float;
+    __device__ bool async() const { return x.f != nullptr; }
+    __device__ float get(uint32_t i, int b) const { return x.get(i, b); }
+    __device__ void copy(float* dst, uint32_t i) const { cp_async4(dst, x.f + i); }
+};
+struct SrcD {
+    const double* p;
+    using T = double;
+    __device__ bool async() const { return true; }
+    __device__ double get(uint32_t i, int) const { return p[i]; }
+    __device__ void copy(double* dst, uint32_t i) const { cp_async8(dst, p + i); }
+};
+
+// (p0, p1, p2) given along the axes (a, a+1, a+2) mod 3 -> (x, y, z)
+__device__ inline void rot3(int a, int p0, int p1, int p2, int& x, int& y, int& z) {
+    x = a == 0 ? p0 : (a == 1 ? p2 : p1);
+    y = a == 0 ? p1 : (a == 1 ? p0 : p2);
+    z = a == 0 ? p2 : (a == 1 ? p1 : p0);
+}
+
+// Every batched CTA runs NT threads over G slots of one resolution R (a power of two, 1..16), so
+// that G * R^3 <= NT or G == 1.  The kernels switch on R once per CTA and run a body compiled for
+// that R: every index split is then a shift, a mask or a multiply by a constant, and every loop
+// has a fixed trip count.
+constexpr int NT = 256;
+
+template <int R>
+struct Geom {
+    static constexpr int n3 = R * R * R, rr = R * R, nf = (R + 1) * R * R, R2 = R + 2, X3 = R2 * R2 * R2;
+    static constexpr int FS = n3 + 3 * nf;  // b, then the three face-coefficient arrays
+    static constexpr int FW = n3 / 4 + 2;   // 32-bit words that cover a block's fluid bytes
+    static constexpr int GMAX = n3 >= NT ? 1 : NT / n3;
+};
+
+#define AW_SWITCH_RES(r, BODY) \
+    switch (r) {               \
+        case 1: BODY(1); break;  \
+        case 2: BODY(2); break;  \
+        case 4: BODY(4); break;  \
+        case 8: BODY(8); break;  \
+        default: BODY(16); break; \
     }
-    for (int t = threadIdx.x; t < G * 6 * rr; t += blockDim.x) {
-        const int sl = t / (6 * rr), rem0 = t - sl * 6 * rr;
-        const int b = sb[sl];
-        if (b < 0) continue;
-        const int face = rem0 / rr, rem = rem0 - face * rr;
-        const int a = face >> 1, sd = (face & 1) ? 1 : -1;
-        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        int c[3], cb[3];
-        c[a] = sd > 0 ? r - 1 : 0;
-        c[t1] = rem % r;
-        c[t2] = rem / r;
-        bcoord(L.g, b, cb);
-        const float v = ghost_val(L, x, b, cb, c, a, sd);
-        int q[3] = {c[0], c[1], c[2]};
-        q[a] += sd;
-        xs[sl * stride + xi3(q[0], q[1], q[2], R2)] = v;
+
+// Shared-memory image of a batched CTA: per slot x with a one-cell halo (xs, (R+2)^3 values of
+// type T), b and the face coefficients (fs), the fluid words (fw) and the slot metadata.
+template <class T, int R>
+struct SlotImage {
+    using Gm = Geom<R>;
+    T* xs;
+    int* meta;
+    float* fs;
+    uint32_t* fw;
+    int G;
+    __device__ SlotImage(void* base, int G_) : G(G_) {
+        xs = (T*)base;
+        meta = (int*)(xs + G * Gm::X3);
+        fs = (float*)(meta + NMETA * G);
+        fw = (uint32_t*)(fs + G * Gm::FS);
+    }
+    __device__ int m(int f, int sl) const { return meta[f * G + sl]; }
+    __device__ uint32_t off(int k, int sl) const { return (uint32_t)meta[(MF_OFF + k) * G + sl]; }
+    __device__ bool fluid(int sl, int i) const {
+        return ((const uint8_t*)(fw + sl * Gm::FW))[(off(0, sl) & 3u) + i] != 0;
+    }
+};
+
+__host__ __device__ inline size_t slot_image_bytes(int G, int r, size_t tsize) {
+    const size_t n3 = (size_t)r * r * r, nf = (size_t)(r + 1) * r * r, X3 = (size_t)(r + 2) * (r + 2) * (r + 2);
+    return (size_t)G * (X3 * tsize + NMETA * 4 + (n3 + 3 * nf) * 4 + (n3 / 4 + 2) * 4) + 16;
+}
+
+// Stage the metadata of a CTA's G slots into meta[NMETA * G] (one round trip); slots whose block is
+// inactive (status[b] == 0) get block id -1.
+template <int R>
+__device__ inline void stage_meta(int* meta, int G, const Batch& B, int first, const uint8_t* __restrict__ status) {
+    constexpr int GM = Geom<R>::GMAX;
+    const int t = threadIdx.x % GM;
+    if (t < G)
+        for (int f = threadIdx.x / GM; f < NMETA; f += NT / GM)
+            cp_async4(meta + f * G + t, B.meta + (size_t)f * B.nslots + first + t);
+    cp_async_wait_all();
+    __syncthreads();
+    if (status) {
+        for (int s = threadIdx.x; s < G; s += NT)
+            if (!status[meta[s]]) meta[s] = -1;
+        __syncthreads();
     }
 }
 
-// Write every slot's x back: FP32, or FP16 with a fresh per-block scale.
-__device__ inline void store_slots(const LevelView& L, const XStore& x, const int* sb, int G, int r, const float* xs,
-                                   int stride, int* smax) {
-    const int R2 = r + 2, n3 = r * r * r;
+struct MetaView {
+    const int* p;
+    int G;
+    __device__ int m(int f, int sl) const { return p[f * G + sl]; }
+    __device__ uint32_t off(int k, int sl) const { return (uint32_t)p[(MF_OFF + k) * G + sl]; }
+};
+
+// Register-batched staging of values that need a decode or a mean: the FP16 interior cells and the
+// halo cells (0, 1 or 4 sources each).  K items per thread are addressed, then loaded, then
+// stored, so that their loads are in flight together.
+template <int R, class Src, bool HALO>
+__device__ inline void stage_items(SlotImage<typename Src::T, R>& S, const Src& x) {
+    using T = typename Src::T;
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, rr = Gm::rr, K = 4;
+    constexpr int NI = HALO ? GM * 6 * rr : GM * n3;
+#pragma unroll
+    for (int base = 0; base < NI; base += K * NT) {
+        uint32_t src[K][4];
+        int ns[K], blk[K], dst[K];
+        T raw[K][4];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int t = base + k * NT + threadIdx.x;
+            ns[k] = 0;
+            dst[k] = -1;
+            blk[k] = 0;
+            if (t >= NI) continue;
+            if (!HALO) {
+                const int sl = t / n3, i = t % n3;
+                if (sl >= S.G) continue;
+                const int b = S.m(MF_BLOCK, sl);
+                if (b < 0) continue;
+                ns[k] = 1;
+                src[k][0] = S.off(0, sl) + i;
+                blk[k] = b;
+                dst[k] = sl * Gm::X3 + xi3(i % R, (i / R) % R, i / rr, Gm::R2);
+                continue;
+            }
+            const int sl = t / (6 * rr), rem0 = t % (6 * rr);
+            if (sl >= S.G || S.m(MF_BLOCK, sl) < 0) continue;
+            const int face = rem0 / rr, rem = rem0 % rr;
+            const int a = face >> 1, sd = (face & 1) ? 1 : -1;
+            const int u = rem % R, v = rem / R;  // coordinates along the axes a+1 and a+2
+            const int kind = S.m(MF_NB + 3 * face + 1, sl);
+            if (kind != NB_NONE) {
+                const uint32_t o = (uint32_t)S.m(MF_NB + 3 * face, sl);
+                blk[k] = S.m(MF_NB + 3 * face + 2, sl);
+                const int rn = kind == NB_SAME ? R : (kind == NB_COARSE ? R / 2 : 2 * R);
+                const int qa = sd > 0 ? 0 : rn - 1;
+                int qx, qy, qz;
+                if (kind != NB_FINE) {
+                    const int sh = kind == NB_SAME ? 0 : 1;
+                    rot3(a, qa, u >> sh, v >> sh, qx, qy, qz);
+                    ns[k] = 1;
+                    src[k][0] = o + cidx(qx, qy, qz, rn);
+                } else {
+                    ns[k] = 4;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        rot3(a, qa, 2 * u + (e >> 1), 2 * v + (e & 1), qx, qy, qz);
+                        src[k][e] = o + cidx(qx, qy, qz, rn);
+                    }
+                }
+            }
+            int hx, hy, hz;
+            rot3(a, sd > 0 ? R : -1, u, v, hx, hy, hz);
+            dst[k] = sl * Gm::X3 + xi3(hx, hy, hz, Gm::R2);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) raw[k][e] = e < ns[k] ? x.get(src[k][e], blk[k]) : T(0);
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (dst[k] < 0) continue;
+            T v;
+            if (ns[k] == 4) {
+                T sum = T(0);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) sum += raw[k][e];
+                v = T(0.25) * sum;
+            } else {
+                v = raw[k][0];
+            }
+            S.xs[dst[k]] = v;
+        }
+    }
+}
+
+// Stage x (interior + halo), b, the face coefficients and the fluid flags of every live slot.
+// Every global load is issued before the first wait: plain copies go through cp.async, decoded
+// and averaged values through register batches, so that a CTA pays about one memory round trip.
+template <int R, class Src>
+__device__ inline void stage_data(SlotImage<typename Src::T, R>& S, const Src& x, const float* __restrict__ bvec, Coef3 W,
+                                  const uint8_t* __restrict__ fluid) {
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf;
+    const bool xa = x.async();
+#pragma unroll
+    for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+        const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+        if (sl >= S.G || S.m(MF_BLOCK, sl) < 0) continue;
+        const uint32_t oc = S.off(0, sl);
+        if (xa) x.copy(S.xs + sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2), oc + i);
+        cp_async4(S.fs + sl * Gm::FS + i, bvec + oc + i);
+    }
+#pragma unroll 4
+    for (int t0 = 0; t0 < GM * 3 * nf; t0 += NT) {
+        const int t = t0 + threadIdx.x;
+        if (t >= GM * 3 * nf) break;
+        const int sl = t / (3 * nf), j = t % (3 * nf);
+        if (sl >= S.G || S.m(MF_BLOCK, sl) < 0) continue;
+        const int a = j / nf;
+        const float* wa = a == 0 ? W.w[0] : (a == 1 ? W.w[1] : W.w[2]);
+        cp_async4(S.fs + sl * Gm::FS + n3 + j, wa + S.off(1 + a, sl) + (j - a * nf));
+    }
+    if (fluid) {
+        const uint32_t* fwg = (const uint32_t*)fluid;
+#pragma unroll
+        for (int t0 = 0; t0 < GM * Gm::FW; t0 += NT) {
+            const int t = t0 + threadIdx.x;
+            if (t >= GM * Gm::FW) break;
+            const int sl = t / Gm::FW, w = t % Gm::FW;
+            if (sl >= S.G || S.m(MF_BLOCK, sl) < 0) continue;
+            const uint32_t oc = S.off(0, sl);
+            if (w * 4 < (int)(oc & 3u) + n3) cp_async4(S.fw + sl * Gm::FW + w, fwg + (oc >> 2) + w);
+        }
+    }
+    if (!xa) stage_items<R, Src, false>(S, x);
+    stage_items<R, Src, true>(S, x);
+    cp_async_wait_all();
+}
+
+// Write every slot's x back: FP32, or FP16 with a fresh per-block scale.  sb/off0 are per-slot
+// block ids (-1 = skip) and cell offsets in shared memory.
+template <int R>
+__device__ inline void store_slots(const XStore& x, const int* sb, const int* off0, int G, const float* xs, int* smax) {
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3;
     if (x.f) {
-        for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-            const int sl = t / n3, i = t - sl * n3;
-            const int b = sb[sl];
-            if (b < 0) continue;
-            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-            x.f[L.off[0][b] + i] = xs[sl * stride + xi3(cx, cy, cz, R2)];
+#pragma unroll
+        for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+            const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+            if (sl >= G || sb[sl] < 0) continue;
+            x.f[(uint32_t)off0[sl] + i] = xs[sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2)];
         }
         return;
     }
-    for (int t = threadIdx.x; t < G; t += blockDim.x) smax[t] = 0;
+    for (int t = threadIdx.x; t < G; t += NT) smax[t] = 0;
     __syncthreads();
     {
         float m = 0.f;
-        const int sl = (int)threadIdx.x / n3 < G ? (int)threadIdx.x / n3 : 0;
-        for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-            const int i = t - (t / n3) * n3;
-            if (sb[t / n3] < 0) continue;
-            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-            m = fmaxf(m, fabsf(xs[(t / n3) * stride + xi3(cx, cy, cz, R2)]));
+#pragma unroll
+        for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+            const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+            if (sl >= G || sb[sl] < 0) continue;
+            m = fmaxf(m, fabsf(xs[sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2)]));
         }
-        slot_max(&smax[G == 1 ? 0 : sl], n3, m);
+        const int sl = GM == 1 ? 0 : min((int)threadIdx.x / n3, G - 1);
+        slot_max(&smax[sl], n3, m);
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        if (b < 0) continue;
+#pragma unroll
+    for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+        const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+        if (sl >= G || sb[sl] < 0) continue;
         const float m = __int_as_float(smax[sl]);
         const float inv = m > 0.f ? 32768.f / m : 0.f;
-        const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-        x.h[L.off[0][b] + i] = __float2half_rn(xs[sl * stride + xi3(cx, cy, cz, R2)] * inv);
+        x.h[(uint32_t)off0[sl] + i] = __float2half_rn(xs[sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2)] * inv);
     }
-    for (int t = threadIdx.x; t < G; t += blockDim.x)
+    for (int t = threadIdx.x; t < G; t += NT)
         if (sb[t] >= 0) {
             const float m = __int_as_float(smax[t]);
             x.scale[sb[t]] = m > 0.f ? m * (1.f / 32768.f) : 0.f;
         }
 }
 
-__host__ __device__ inline int smooth_slot_floats(int r) {
-    return (r + 2) * (r + 2) * (r + 2) + r * r * r + 3 * (r + 1) * r * r;
-}
+// Shared smoother state of one CTA (one entry per slot).
+struct SmoothShared {
+    int smr[NT], sdone[NT];
+    float sinit[NT];
+};
 
-// smoothActiveBlocks (Smoother.cuh:105-202) for one block colour, batched.
-__global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
-                                                const uint8_t* __restrict__ fluid, Batch B,
-                                                const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
-                                                SmoothParams P) {
-    extern __shared__ float sm[];
-    __shared__ int sb[256], smr[256], sdone[256];
-    __shared__ float sinit[256];
-    const int4 d = B.desc[blockIdx.x];
-    const int G = d.y, r = d.z;
-    const int R2 = r + 2, n3 = r * r * r, nf = (r + 1) * r * r, X3 = R2 * R2 * R2;
-    const int per = smooth_slot_floats(r);
-    uint8_t* fsb = (uint8_t*)(sm + G * per);
-    for (int t = threadIdx.x; t < G; t += blockDim.x) {
-        const int b = B.blocks[d.x + t];
-        sb[t] = status[b] ? b : -1;
-        smr[t] = 0;
-        sdone[t] = 0;
-        sinit[t] = -1.f;
-    }
-    __syncthreads();
+template <int R>
+__device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z, const LevelView& L, const XStore& x,
+                                   const float* __restrict__ bvec, const Coef3& W, const uint8_t* __restrict__ fluid,
+                                   const Batch& B, const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
+                                   const SmoothParams& P) {
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
+    SlotImage<float, R> S(smraw, d.y);
+    const int G = S.G;
+    stage_meta<R>(S.meta, G, B, d.x, status);
+    const int* sb = S.meta + MF_BLOCK * G;
     if (!__syncthreads_or(threadIdx.x < G && sb[threadIdx.x] >= 0)) return;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        if (b < 0) continue;
-        const uint32_t oc = L.off[0][b];
-        sm[sl * per + X3 + i] = bvec[oc + i];
-        fsb[sl * n3 + i] = fluid[oc + i];
+    for (int t = threadIdx.x; t < G; t += NT) {
+        Z.smr[t] = 0;
+        Z.sdone[t] = 0;
+        Z.sinit[t] = -1.f;
     }
-    for (int t = threadIdx.x; t < G * 3 * nf; t += blockDim.x) {
-        const int sl = t / (3 * nf), j = t - sl * 3 * nf;
-        const int b = sb[sl];
-        if (b < 0) continue;
-        const int a = j / nf;
-        sm[sl * per + X3 + n3 + j] = W.w[a][L.off[1 + a][b] + (j - a * nf)];
-    }
-    stage_slots(L, x, sb, G, r, sm, per);
+    stage_data<R>(S, SrcX{x}, bvec, W, P.check_fluid ? fluid : nullptr);
     __syncthreads();
-    const int sy = R2, sz = R2 * R2;
-    const int my_slot = G == 1 ? 0 : min((int)threadIdx.x / n3, G - 1);
+    const int my_slot = GM == 1 ? 0 : min((int)threadIdx.x / n3, G - 1);
     for (int bi = 0; bi < P.iters; ++bi) {
         float lmax = 0.f;
+#pragma unroll
         for (int col = 0; col < 2; ++col) {
-            for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-                const int sl = t / n3, i = t - sl * n3;
-                if (sb[sl] < 0 || sdone[sl]) continue;
-                const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
+#pragma unroll
+            for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+                const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+                if (sl >= G || sb[sl] < 0 || Z.sdone[sl]) continue;
+                const int cx = i % R, cy = (i / R) % R, cz = i / Gm::rr;
                 if (((cx + cy + cz) & 1) != col) continue;
-                if (P.check_fluid && !fsb[sl * n3 + i]) continue;
-                float* xs = sm + sl * per;
-                const float* Ws = xs + X3 + n3;
-                const float wW = Ws[fidx(0, cx, cy, cz, r)];
-                const float wE = Ws[fidx(0, cx + 1, cy, cz, r)];
-                const float wS = Ws[nf + fidx(1, cx, cy, cz, r)];
-                const float wN = Ws[nf + fidx(1, cx, cy + 1, cz, r)];
-                const float wB = Ws[2 * nf + fidx(2, cx, cy, cz, r)];
-                const float wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, r)];
+                if (P.check_fluid && !S.fluid(sl, i)) continue;
+                float* xs = S.xs + sl * Gm::X3;
+                const float* bs = S.fs + sl * Gm::FS;
+                const float* Ws = bs + n3;
+                const float wW = Ws[fidx(0, cx, cy, cz, R)];
+                const float wE = Ws[fidx(0, cx + 1, cy, cz, R)];
+                const float wS = Ws[nf + fidx(1, cx, cy, cz, R)];
+                const float wN = Ws[nf + fidx(1, cx, cy + 1, cz, R)];
+                const float wB = Ws[2 * nf + fidx(2, cx, cy, cz, R)];
+                const float wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, R)];
                 const float diag = -(wW + wE + wS + wN + wB + wT);
                 if (fabsf(diag) < 1e-9f) continue;
                 const int q = xi3(cx, cy, cz, R2);
                 const float xc = xs[q];
                 const float Ax = wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] + wB * xs[q - sz] +
                                  wT * xs[q + sz] + diag * xc;
-                const float res = xs[X3 + i] - Ax;
+                const float res = bs[i] - Ax;
                 xs[q] = xc + P.omega * (res / diag);
                 lmax = fmaxf(lmax, fabsf(res));
             }
             __syncthreads();
         }
-        slot_max(&smr[my_slot], n3, lmax);
+        slot_max(&Z.smr[my_slot], n3, lmax);
         __syncthreads();
         // per-slot early exit (block-uniform); smr keeps the last executed sweep's max
         int more = 0;
-        for (int t = threadIdx.x; t < G; t += blockDim.x) {
-            if (sb[t] < 0 || sdone[t]) continue;
-            const float mr = __int_as_float(smr[t]);
-            if (bi == 0) sinit[t] = mr;
-            if (sinit[t] > 1e-9f && mr < sinit[t] * P.target) sdone[t] = 1;
+        for (int t = threadIdx.x; t < G; t += NT) {
+            if (sb[t] < 0 || Z.sdone[t]) continue;
+            const float mr = __int_as_float(Z.smr[t]);
+            if (bi == 0) Z.sinit[t] = mr;
+            if (Z.sinit[t] > 1e-9f && mr < Z.sinit[t] * P.target) Z.sdone[t] = 1;
             else if (bi + 1 < P.iters) {
-                smr[t] = 0;
+                Z.smr[t] = 0;
                 more = 1;
             }
         }
         if (!__syncthreads_or(more)) break;
     }
     __syncthreads();
-    int* smax = sdone;  // reused as per-slot |x| max for FP16 storage
-    store_slots(L, x, sb, G, r, sm, per, smax);
-    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+    store_slots<R>(x, sb, S.meta + MF_OFF * G, G, S.xs, Z.sdone);  // sdone reused as per-slot |x| max
+    if (!status_next) return;
+    for (int t = threadIdx.x; t < G; t += NT) {
         const int b = sb[t];
-        if (b < 0 || !(__int_as_float(smr[t]) > P.theta)) continue;
+        if (b < 0 || !(__int_as_float(Z.smr[t]) > P.theta)) continue;
         status_next[b] = 1;
         int cb[3];
         bcoord(L.g, b, cb);
@@ -400,45 +551,56 @@ __global__ void __launch_bounds__(256) k_smooth(LevelView L, XStore x, const flo
     }
 }
 
-// computeExplicitResidual (VCycle.cuh:81-131), batched: r = b - A x on every cell (0 on air cells
-// in FV mode); optional per-CTA partial sums of r^2.
-__global__ void __launch_bounds__(256) k_residual(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
-                                                  const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
-                                                  float* __restrict__ rout, double* __restrict__ part) {
-    extern __shared__ float sm[];
-    __shared__ int sb[256];
-    __shared__ double dred[32];
+// smoothActiveBlocks (Smoother.cuh:105-202) for one block colour, batched.  status == nullptr
+// means every block is active (no residual-threshold deactivation) and no activation is written.
+__global__ void __launch_bounds__(NT, 4) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
+                                               const uint8_t* __restrict__ fluid, Batch B,
+                                               const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
+                                               SmoothParams P) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ SmoothShared Z;
     const int4 d = B.desc[blockIdx.x];
-    const int G = d.y, r = d.z;
-    const int R2 = r + 2, n3 = r * r * r, X3 = R2 * R2 * R2;
-    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
+#define AW_SMOOTH(R) smooth_body<R>(d, smraw, Z, L, x, bvec, W, fluid, B, status, status_next, P)
+    AW_SWITCH_RES(d.z, AW_SMOOTH)
+#undef AW_SMOOTH
+}
+
+template <int R, class Src>
+__device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred, const Src& x, const float* __restrict__ bvec,
+                                     const Coef3& W, const uint8_t* __restrict__ fluid, const Batch& B, int check_fluid,
+                                     float* __restrict__ rout, double* __restrict__ part) {
+    using T = typename Src::T;
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
+    SlotImage<T, R> S(smraw, d.y);
+    const int G = S.G;
+    stage_meta<R>(S.meta, G, B, d.x, nullptr);
+    stage_data<R>(S, x, bvec, W, check_fluid ? fluid : nullptr);
     __syncthreads();
-    stage_slots(L, x, sb, G, r, sm, X3);
-    __syncthreads();
-    const int sy = R2, sz = R2 * R2;
     double acc = 0.0;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        const uint32_t oc = L.off[0][b];
-        float rv = 0.f;
-        if (!check_fluid || fluid[oc + i]) {
-            const int cx = i % r, cy = (i / r) % r, cz = i / (r * r);
-            const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
-            const float wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
-            const float wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
-            const float wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
-            const float wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
-            const float wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
-            const float wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
-            const float diag = -(wW + wE + wS + wN + wB + wT);
-            const float* xs = sm + sl * X3;
+#pragma unroll
+    for (int t0 = 0; t0 < GM * n3; t0 += NT) {
+        const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+        if (sl >= G) continue;
+        T rv = T(0);
+        const float* bs = S.fs + sl * Gm::FS;
+        if (!check_fluid || S.fluid(sl, i)) {
+            const int cx = i % R, cy = (i / R) % R, cz = i / Gm::rr;
+            const float* Ws = bs + n3;
+            const T wW = Ws[fidx(0, cx, cy, cz, R)];
+            const T wE = Ws[fidx(0, cx + 1, cy, cz, R)];
+            const T wS = Ws[nf + fidx(1, cx, cy, cz, R)];
+            const T wN = Ws[nf + fidx(1, cx, cy + 1, cz, R)];
+            const T wB = Ws[2 * nf + fidx(2, cx, cy, cz, R)];
+            const T wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, R)];
+            const T diag = -(wW + wE + wS + wN + wB + wT);
+            const T* xs = S.xs + sl * Gm::X3;
             const int q = xi3(cx, cy, cz, R2);
-            const float Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
-                             wB * xs[q - sz] + wT * xs[q + sz];
-            rv = bvec[oc + i] - Ax;
+            const T Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                         wB * xs[q - sz] + wT * xs[q + sz];
+            rv = (T)bs[i] - Ax;
         }
-        rout[oc + i] = rv;
+        rout[S.off(0, sl) + i] = (float)rv;
         acc += (double)rv * (double)rv;
     }
     if (part) {
@@ -447,97 +609,141 @@ __global__ void __launch_bounds__(256) k_residual(LevelView L, XStore x, const f
     }
 }
 
-// FP64 residual of the outer defect correction, batched: r = b - A p with p in FP64, stored as
-// FP32 into the V-cycle right-hand side, with per-CTA partial sums of r^2.
-__global__ void __launch_bounds__(256) k_residual64(LevelView L, const double* __restrict__ p,
-                                                    const float* __restrict__ bvec, Coef3 W,
-                                                    const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
-                                                    float* __restrict__ rout, double* __restrict__ part) {
-    extern __shared__ double smd[];
-    __shared__ int sb[256];
+// computeExplicitResidual (VCycle.cuh:81-131), batched: r = b - A x on every cell (0 on air cells
+// in FV mode); optional per-CTA partial sums of r^2.  Src::T = float for the V-cycle's own
+// residual, double for the FP64 residual of the outer defect correction (stored as FP32 into the
+// V-cycle right-hand side).
+template <class Src>
+__global__ void __launch_bounds__(NT, 4) k_residual(Src x, const float* __restrict__ bvec, Coef3 W,
+                                                 const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
+                                                 float* __restrict__ rout, double* __restrict__ part) {
+    extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double dred[32];
     const int4 d = B.desc[blockIdx.x];
-    const int G = d.y, r = d.z;
-    const int R2 = r + 2, n3 = r * r * r, rr = r * r, X3 = R2 * R2 * R2;
-    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
-    __syncthreads();
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int cx = i % r, cy = (i / r) % r, cz = i / rr;
-        smd[sl * X3 + xi3(cx, cy, cz, R2)] = p[L.off[0][sb[sl]] + i];
-    }
-    for (int t = threadIdx.x; t < G * 6 * rr; t += blockDim.x) {
-        const int sl = t / (6 * rr), rem0 = t - sl * 6 * rr;
-        const int b = sb[sl];
-        const int face = rem0 / rr, rem = rem0 - face * rr;
-        const int a = face >> 1, sd = (face & 1) ? 1 : -1;
-        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        int c[3], cb[3];
-        c[a] = sd > 0 ? r - 1 : 0;
-        c[t1] = rem % r;
-        c[t2] = rem / r;
-        bcoord(L.g, b, cb);
-        int nc[3] = {cb[0], cb[1], cb[2]};
-        nc[a] += sd;
-        double v = 0.0;
-        if (inside(L.g, nc)) {
-            const int n = bidx(L.g, nc[0], nc[1], nc[2]);
-            const int rn = L.res[n];
-            if (rn) {
-                int q[3];
-                q[a] = sd > 0 ? 0 : rn - 1;
-                if (rn == r) {
-                    q[t1] = c[t1];
-                    q[t2] = c[t2];
-                    v = p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
-                } else if (rn < r) {
-                    q[t1] = min(c[t1] >> 1, rn - 1);
-                    q[t2] = min(c[t2] >> 1, rn - 1);
-                    v = p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
-                } else {
-                    for (int d1 = 0; d1 < 2; ++d1)
-                        for (int d2 = 0; d2 < 2; ++d2) {
-                            q[t1] = min(2 * c[t1] + d1, rn - 1);
-                            q[t2] = min(2 * c[t2] + d2, rn - 1);
-                            v += p[L.off[0][n] + cidx(q[0], q[1], q[2], rn)];
-                        }
-                    v *= 0.25;
-                }
+#define AW_RESID(R) residual_body<R>(d, smraw, dred, x, bvec, W, fluid, B, check_fluid, rout, part)
+    AW_SWITCH_RES(d.z, AW_RESID)
+#undef AW_RESID
+}
+
+template <int R>
+__device__ inline void restrict_body(int4 d, unsigned char* smraw, const float* __restrict__ r, float* __restrict__ bc,
+                                     const uint8_t* __restrict__ fluid_c, int check_fluid, const Batch& B) {
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, K = 2;
+    const int G = d.y;
+    int* meta = (int*)smraw;
+    stage_meta<R>(meta, G, B, d.x, nullptr);
+    const MetaView S{meta, G};
+#pragma unroll
+    for (int base = 0; base < GM * n3; base += K * NT) {
+        float v[K][8];
+        uint8_t fl[K];
+        uint32_t dst[K];
+        bool ok[K], full[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int t = base + k * NT + threadIdx.x, sl = t / n3, i = t % n3;
+            ok[k] = t < GM * n3 && sl < G;
+            full[k] = false;
+            dst[k] = 0;
+            fl[k] = 1;
+            if (!ok[k]) continue;
+            const int rf = S.m(MF_FINE_RES, sl);
+            const uint32_t of = (uint32_t)S.m(MF_FINE_OFF, sl);
+            dst[k] = S.off(0, sl) + i;
+            if (check_fluid) fl[k] = fluid_c[dst[k]];
+            full[k] = rf == 2 * R;
+            if (full[k]) {
+                const int x = i % R, y = (i / R) % R, z = i / Gm::rr;
+#pragma unroll
+                for (int c = 0; c < 8; ++c)
+                    v[k][c] = r[of + cidx(2 * x + (c & 1), 2 * y + ((c >> 1) & 1), 2 * z + (c >> 2), 2 * R)];
+            } else {
+                v[k][0] = r[of + i];
             }
         }
-        int q[3] = {c[0], c[1], c[2]};
-        q[a] += sd;
-        smd[sl * X3 + xi3(q[0], q[1], q[2], R2)] = v;
-    }
-    __syncthreads();
-    const int sy = R2, sz = R2 * R2;
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        const uint32_t oc = L.off[0][b];
-        double rv = 0.0;
-        if (!check_fluid || fluid[oc + i]) {
-            const int cx = i % r, cy = (i / r) % r, cz = i / rr;
-            const uint32_t ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
-            const double wW = W.w[0][ox + fidx(0, cx, cy, cz, r)];
-            const double wE = W.w[0][ox + fidx(0, cx + 1, cy, cz, r)];
-            const double wS = W.w[1][oy + fidx(1, cx, cy, cz, r)];
-            const double wN = W.w[1][oy + fidx(1, cx, cy + 1, cz, r)];
-            const double wB = W.w[2][oz + fidx(2, cx, cy, cz, r)];
-            const double wT = W.w[2][oz + fidx(2, cx, cy, cz + 1, r)];
-            const double diag = -(wW + wE + wS + wN + wB + wT);
-            const double* xs = smd + sl * X3;
-            const int q = xi3(cx, cy, cz, R2);
-            const double Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
-                              wB * xs[q - sz] + wT * xs[q + sz];
-            rv = (double)bvec[oc + i] - Ax;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            if (!ok[k]) continue;
+            float s = v[k][0];
+            if (full[k]) {
+#pragma unroll
+                for (int c = 1; c < 8; ++c) s += v[k][c];
+            }
+            bc[dst[k]] = fl[k] ? s : 0.f;
         }
-        rout[oc + i] = (float)rv;
-        acc += rv * rv;
     }
-    double tsum = block_sum(acc, dred);
-    if (threadIdx.x == 0) part[blockIdx.x] = tsum;
+}
+
+// restrictResidualsKernel (MultigridTransfer.cuh:9-59), batched over the coarse level's blocks:
+// 8-child sum, or a copy for a block that keeps one cell.  Coarse air cells get 0.
+__global__ void __launch_bounds__(NT) k_restrict(const float* __restrict__ r, float* __restrict__ bc,
+                                                 const uint8_t* __restrict__ fluid_c, int check_fluid, Batch B) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int4 d = B.desc[blockIdx.x];
+#define AW_RESTR(R) restrict_body<R>(d, smraw, r, bc, fluid_c, check_fluid, B)
+    AW_SWITCH_RES(d.z, AW_RESTR)
+#undef AW_RESTR
+}
+
+template <int R>
+__device__ inline void prolong_body(int4 d, unsigned char* smraw, int* smax, const XStore& xf, const XStore& xc,
+                                    const uint8_t* __restrict__ fluid_f, int check_fluid, const Batch& B) {
+    using Gm = Geom<R>;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, K = 2;
+    const int G = d.y;
+    // FP16 fine storage keeps the updated block in shared memory for the re-encode
+    float* xs = (float*)smraw;
+    int* meta = (int*)(xs + (xf.f ? 0 : G * Gm::X3));
+    stage_meta<R>(meta, G, B, d.x, nullptr);
+    const MetaView S{meta, G};
+#pragma unroll
+    for (int base = 0; base < GM * n3; base += K * NT) {
+        float add[K], cur[K];
+        int sl_[K], i_[K];
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int t = base + k * NT + threadIdx.x, sl = t / n3, i = t % n3;
+            sl_[k] = -1;
+            i_[k] = i;
+            add[k] = 0.f;
+            cur[k] = 0.f;
+            if (t >= GM * n3 || sl >= G) continue;
+            sl_[k] = sl;
+            const int b = S.m(MF_BLOCK, sl);
+            const int rc = S.m(MF_COARSE_RES, sl);
+            const uint32_t of = S.off(0, sl), oc = (uint32_t)S.m(MF_COARSE_OFF, sl);
+            if (rc && (!check_fluid || fluid_f[of + i])) {
+                const uint32_t ci = (R == 2 * rc) ? cidx((i % R) >> 1, ((i / R) % R) >> 1, (i / Gm::rr) >> 1, R / 2)
+                                                  : (uint32_t)i;
+                add[k] = xc.get(oc + ci, b);
+            }
+            cur[k] = xf.get(of + i, b);
+        }
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            const int sl = sl_[k];
+            if (sl < 0) continue;
+            const int i = i_[k];
+            if (xf.f) xf.f[S.off(0, sl) + i] = cur[k] + add[k];
+            else xs[sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2)] = cur[k] + add[k];
+        }
+    }
+    if (xf.f) return;
+    __syncthreads();
+    store_slots<R>(xf, meta + MF_BLOCK * G, meta + MF_OFF * G, G, xs, smax);
+}
+
+// prolongateCorrection (MultigridTransfer.cuh:63-102), batched over the fine level's blocks:
+// x_f += x_c[parent] on fluid cells (FP16 fine storage is decoded, updated and re-encoded).
+__global__ void __launch_bounds__(NT) k_prolong(XStore xf, XStore xc, const uint8_t* __restrict__ fluid_f,
+                                                int check_fluid, Batch B) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ int smax[NT];
+    const int4 d = B.desc[blockIdx.x];
+#define AW_PROL(R) prolong_body<R>(d, smraw, smax, xf, xc, fluid_f, check_fluid, B)
+    AW_SWITCH_RES(d.z, AW_PROL)
+#undef AW_PROL
 }
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
@@ -562,67 +768,6 @@ __global__ void k_sumsq(const float* __restrict__ v, const uint8_t* __restrict__
         if (!check_fluid || fluid[i]) acc += (double)v[i] * (double)v[i];
     double t = block_sum(acc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = t;
-}
-
-// restrictResidualsKernel (MultigridTransfer.cuh:9-59), batched over the coarse level's blocks:
-// 8-child sum, or a copy for a block that keeps one cell.  Coarse air cells get 0.
-__global__ void __launch_bounds__(256) k_restrict(LevelView F, LevelView K, const float* __restrict__ r,
-                                                  float* __restrict__ bc, const uint8_t* __restrict__ fluid_c,
-                                                  int check_fluid, Batch B) {
-    const int4 d = B.desc[blockIdx.x];
-    const int G = d.y, rc = d.z, n3 = rc * rc * rc;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = B.blocks[d.x + sl];
-        const int rf = F.res[b];
-        const uint32_t of = F.off[0][b], oc = K.off[0][b];
-        float s;
-        if (rf == 2 * rc) {
-            const int x = i % rc, y = (i / rc) % rc, z = i / (rc * rc);
-            const int fx = 2 * x, fy = 2 * y, fz = 2 * z;
-            s = r[of + cidx(fx, fy, fz, rf)];
-            s += r[of + cidx(fx + 1, fy, fz, rf)];
-            s += r[of + cidx(fx, fy + 1, fz, rf)];
-            s += r[of + cidx(fx + 1, fy + 1, fz, rf)];
-            s += r[of + cidx(fx, fy, fz + 1, rf)];
-            s += r[of + cidx(fx + 1, fy, fz + 1, rf)];
-            s += r[of + cidx(fx, fy + 1, fz + 1, rf)];
-            s += r[of + cidx(fx + 1, fy + 1, fz + 1, rf)];
-        } else {
-            s = r[of + i];
-        }
-        bc[oc + i] = (!check_fluid || fluid_c[oc + i]) ? s : 0.f;
-    }
-}
-
-// prolongateCorrection (MultigridTransfer.cuh:63-102), batched over the fine level's blocks:
-// x_f += x_c[parent] on fluid cells (FP16 fine storage is decoded, updated and re-encoded).
-__global__ void __launch_bounds__(256) k_prolong(LevelView F, LevelView K, XStore xf, XStore xc,
-                                                 const uint8_t* __restrict__ fluid_f, int check_fluid, Batch B) {
-    extern __shared__ float sm[];
-    __shared__ int sb[256], smax[256];
-    const int4 d = B.desc[blockIdx.x];
-    const int G = d.y, rf = d.z, n3 = rf * rf * rf;
-    for (int t = threadIdx.x; t < G; t += blockDim.x) sb[t] = B.blocks[d.x + t];
-    __syncthreads();
-    const int R2 = rf + 2, X3 = R2 * R2 * R2;
-    for (int t = threadIdx.x; t < G * n3; t += blockDim.x) {
-        const int sl = t / n3, i = t - sl * n3;
-        const int b = sb[sl];
-        const int rc = K.res[b];
-        const uint32_t of = F.off[0][b], oc = K.off[0][b];
-        const int x = i % rf, y = (i / rf) % rf, z = i / (rf * rf);
-        float add = 0.f;
-        if (rc && (!check_fluid || fluid_f[of + i])) {
-            const uint32_t ci = (rf == 2 * rc) ? cidx(x >> 1, y >> 1, z >> 1, rc) : (uint32_t)i;
-            add = xc.get(oc + ci, b);
-        }
-        if (xf.f) xf.f[of + i] += add;
-        else sm[sl * X3 + xi3(x, y, z, R2)] = xf.get(of + i, b) + add;
-    }
-    if (xf.f) return;
-    __syncthreads();
-    store_slots(F, xf, sb, G, rf, sm, X3, smax);
 }
 
 __global__ void k_zero_scale(float* s, int n) {
@@ -1071,23 +1216,76 @@ static aw_status build_batches(MGLevel& L, const Geo& geo) {
                 for (int j = 0; j < cnt; ++j) blocks.push_back(by_res[r][i + j]);
             }
             if (!by_res[r].empty()) {
-                const size_t Gm = (size_t)std::min<int>(G, (int)by_res[r].size());
-                L.smem_smooth = std::max(L.smem_smooth, Gm * (smooth_slot_floats(r) * sizeof(float) + (size_t)r * r * r) + 16);
-                L.smem_x = std::max(L.smem_x, Gm * (size_t)(r + 2) * (r + 2) * (r + 2) * sizeof(float));
-                L.smem_x64 = std::max(L.smem_x64, Gm * (size_t)(r + 2) * (r + 2) * (r + 2) * sizeof(double));
+                const int Gm = std::min<int>(G, (int)by_res[r].size());
+                const size_t X3 = (size_t)(r + 2) * (r + 2) * (r + 2);
+                L.smem_smooth = std::max(L.smem_smooth, slot_image_bytes(Gm, r, sizeof(float)));
+                L.smem_x64 = std::max(L.smem_x64, slot_image_bytes(Gm, r, sizeof(double)));
+                L.smem_meta = std::max(L.smem_meta, (size_t)Gm * NMETA * 4 + 16);
+                L.smem_prolong = std::max(L.smem_prolong, (size_t)Gm * (X3 * 4 + NMETA * 4) + 16);
             }
         }
         L.ndesc[k] = (int)desc.size();
+        L.h_blocks[k] = std::move(blocks);
         if (L.ndesc[k]) {
             AW_TRY(L.desc[k].alloc(desc.size()));
-            AW_TRY(L.blocks[k].alloc(blocks.size()));
             AW_CUDA(cudaMemcpy(L.desc[k].p, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice));
-            AW_CUDA(cudaMemcpy(L.blocks[k].p, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
         }
     }
     return AW_OK;
 }
-static Batch batch(const MGLevel& L, int k) { return Batch{L.desc[k].p, L.blocks[k].p}; }
+static Batch batch(const MGLevel& L, int k) { return Batch{L.desc[k].p, L.meta[k].p, (int)L.h_blocks[k].size()}; }
+
+// Per-level host copy of what the slot metadata needs.
+struct HostLevel {
+    std::vector<int> res;
+    std::vector<uint32_t> off[4];
+};
+
+// Lay out the slot metadata of level m in batch order (field-major): block id, offsets, the six
+// face neighbours (cell offset, kind, block) and the block's cells on the adjacent levels.
+static aw_status build_meta(MGLevel& L, const Geo& geo, const HostLevel& h, const HostLevel* finer,
+                            const HostLevel* coarser) {
+    for (int k = 0; k < 3; ++k) {
+        const std::vector<int>& blocks = L.h_blocks[k];
+        const size_t n = blocks.size();
+        if (!n) continue;
+        std::vector<int> mt(NMETA * n, 0);
+        for (size_t j = 0; j < n; ++j) {
+            const int b = blocks[j];
+            const int r = h.res[b];
+            auto F = [&](int f) -> int& { return mt[(size_t)f * n + j]; };
+            F(MF_BLOCK) = b;
+            for (int q = 0; q < 4; ++q) F(MF_OFF + q) = (int)h.off[q][b];
+            int c[3];
+            bcoord(geo, b, c);
+            for (int a = 0; a < 3; ++a)
+                for (int sd = 0; sd < 2; ++sd) {
+                    const int f = MF_NB + 3 * (2 * a + sd);
+                    int nc[3] = {c[0], c[1], c[2]};
+                    nc[a] += sd ? 1 : -1;
+                    F(f + 1) = NB_NONE;
+                    if (!inside(geo, nc)) continue;
+                    const int nbk = bidx(geo, nc[0], nc[1], nc[2]);
+                    const int rn = h.res[nbk];
+                    if (!rn) continue;
+                    F(f) = (int)h.off[0][nbk];
+                    F(f + 1) = rn == r ? NB_SAME : (rn < r ? NB_COARSE : NB_FINE);
+                    F(f + 2) = nbk;
+                }
+            if (finer) {
+                F(MF_FINE_OFF) = (int)finer->off[0][b];
+                F(MF_FINE_RES) = finer->res[b];
+            }
+            if (coarser) {
+                F(MF_COARSE_OFF) = (int)coarser->off[0][b];
+                F(MF_COARSE_RES) = coarser->res[b];
+            }
+        }
+        AW_TRY(L.meta[k].alloc(mt.size()));
+        AW_CUDA(cudaMemcpy(L.meta[k].p, mt.data(), mt.size() * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    return AW_OK;
+}
 static bool fv(const aw_solver* S) { return S->d.operator_mode == AW_OPERATOR_FV; }
 
 static Uniform uniform_of(aw_solver* S, int m) {
@@ -1135,17 +1333,20 @@ static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t 
         return AW_OK;
     }
     const int nb = S->g->st.nb;
-    AW_CUDA(cudaMemsetAsync(L.status[0].p, 1, nb, s));
+    // a negative activation threshold keeps every block active: no status arrays
+    const bool act = S->d.theta >= 0.f;
+    if (act) AW_CUDA(cudaMemsetAsync(L.status[0].p, 1, nb, s));
     SmoothParams P{S->d.omega, S->d.target_reduction, S->d.theta, S->d.block_iterations, cf};
     LevelView V = lview(S, m);
     XStore x = xstore(S, m);
     int cur = 0;
     for (int it = 0; it < iterations; ++it) {
-        AW_CUDA(cudaMemsetAsync(L.status[cur ^ 1].p, 0, nb, s));
+        if (act) AW_CUDA(cudaMemsetAsync(L.status[cur ^ 1].p, 0, nb, s));
         for (int rb = 0; rb < 2; ++rb) {
             if (!L.ndesc[rb]) continue;
             k_smooth<<<L.ndesc[rb], 256, L.smem_smooth, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, rb),
-                                                              L.status[cur].p, L.status[cur ^ 1].p, P);
+                                                              act ? L.status[cur].p : nullptr,
+                                                              act ? L.status[cur ^ 1].p : nullptr, P);
             AW_LAUNCH();
         }
         cur ^= 1;
@@ -1162,10 +1363,10 @@ static aw_status residual_level(aw_solver* S, int m, double* part, cudaStream_t 
         AW_LAUNCH();
         return AW_OK;
     }
-    LevelView V = lview(S, m);
     XStore x = xstore(S, m);
     if (L.ndesc[2]) {
-        k_residual<<<L.ndesc[2], 256, L.smem_x, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, 2), cf, L.r.p, part);
+        k_residual<SrcX><<<L.ndesc[2], 256, L.smem_smooth, s>>>(SrcX{x}, bptr(S, m), coef(L), L.fluid.p, batch(L, 2), cf,
+                                                                 L.r.p, part);
         AW_LAUNCH();
     }
     return AW_OK;
@@ -1183,7 +1384,7 @@ static aw_status restrict_level(aw_solver* S, int m, cudaStream_t s) {
         return AW_OK;
     }
     if (K.ndesc[2]) {
-        k_restrict<<<K.ndesc[2], 256, 0, s>>>(lview(S, m), lview(S, m + 1), F.r.p, K.b.p, K.fluid.p, cf, batch(K, 2));
+        k_restrict<<<K.ndesc[2], 256, K.smem_meta, s>>>(F.r.p, K.b.p, K.fluid.p, cf, batch(K, 2));
         AW_LAUNCH();
     }
     return AW_OK;
@@ -1204,8 +1405,8 @@ static aw_status prolong_level(aw_solver* S, int m, cudaStream_t s) {
         return AW_OK;
     }
     if (F.ndesc[2]) {
-        k_prolong<<<F.ndesc[2], 256, F.half ? F.smem_x : 0, s>>>(lview(S, m), lview(S, m + 1), xstore(S, m),
-                                                                  xstore(S, m + 1), F.fluid.p, cf, batch(F, 2));
+        k_prolong<<<F.ndesc[2], 256, F.half ? F.smem_prolong : F.smem_meta, s>>>(xstore(S, m), xstore(S, m + 1), F.fluid.p,
+                                                                                 cf, batch(F, 2));
         AW_LAUNCH();
     }
     return AW_OK;
@@ -1335,10 +1536,10 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         AW_TRY(L.x.alloc(nc));
         AW_TRY(L.b.alloc(nc));
         AW_TRY(L.r.alloc(nc));
-        AW_TRY(L.fluid.alloc(nc));
+        AW_TRY(L.fluid.alloc(nc + 16));  // whole 32-bit words are staged
         AW_CUDA(cudaMemset(L.x.p, 0, nc * sizeof(float)));
         AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
-        AW_CUDA(cudaMemset(L.fluid.p, 1, nc));
+        AW_CUDA(cudaMemset(L.fluid.p, 1, nc + 16));
         if (L.half) {
             AW_TRY(L.xh.alloc(nc));
             AW_TRY(L.xscale.alloc(nb));
@@ -1349,9 +1550,25 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
             AW_TRY(L.W[a].alloc(L.nface(a)));
             AW_TRY(L.bbar[a].alloc(L.nface(a)));
         }
-        S->smem_max = std::max({S->smem_max, L.smem_smooth, L.smem_x, L.smem_x64});
     }
     S->nmsbg = (int)S->lv.size();
+    {
+        std::vector<HostLevel> hl(S->nmsbg);
+        for (int m = 0; m < S->nmsbg; ++m) {
+            MGLevel& L = S->lv[m];
+            hl[m].res = L.h_res;
+            for (int k = 0; k < 4; ++k) {
+                hl[m].off[k].resize(nb);
+                AW_CUDA(cudaMemcpy(hl[m].off[k].data(), L.off[k].p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+            }
+        }
+        for (int m = 0; m < S->nmsbg; ++m) {
+            MGLevel& L = S->lv[m];
+            AW_TRY(build_meta(L, G.geo, hl[m], m > 0 ? &hl[m - 1] : nullptr, m + 1 < S->nmsbg ? &hl[m + 1] : nullptr));
+            S->smem_max = std::max({S->smem_max, L.smem_smooth, L.smem_prolong, L.smem_meta});
+            S->smem_max64 = std::max(S->smem_max64, L.smem_x64);
+        }
+    }
     // coefficients of the block-structured levels
     for (int m = 0; m < S->nmsbg; ++m) {
         MGLevel& L = S->lv[m];
@@ -1419,10 +1636,12 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
     }
     if (S->smem_max > 48 * 1024) {
         AW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
-        AW_CUDA(cudaFuncSetAttribute(k_residual, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
+        AW_CUDA(cudaFuncSetAttribute(k_residual<SrcX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_prolong, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
-        AW_CUDA(cudaFuncSetAttribute(k_residual64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * S->smem_max)));
+        AW_CUDA(cudaFuncSetAttribute(k_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
     }
+    if (S->smem_max64 > 48 * 1024)
+        AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
     size_t nparts = (size_t)nb + 1024;
     AW_TRY(S->partials.alloc(nparts));
     AW_TRY(S->norm.alloc(2));
@@ -1616,10 +1835,9 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
         S->b0 = nullptr;
     } else {
         double* p = (double*)d_p;
-        LevelView V = lview(S, 0);
         for (;; ++it) {
-            k_residual64<<<L0.ndesc[2], 256, L0.smem_x64, s>>>(V, p, d_b, coef(L0), L0.fluid.p, batch(L0, 2), cf,
-                                                                L0.b.p, S->partials.p);
+            k_residual<SrcD><<<L0.ndesc[2], 256, L0.smem_x64, s>>>(SrcD{p}, d_b, coef(L0), L0.fluid.p, batch(L0, 2), cf,
+                                                                    L0.b.p, S->partials.p);
             ++g_launches;
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) {
