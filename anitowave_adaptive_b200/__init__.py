@@ -95,6 +95,7 @@ SIGNATURES = {
     "aw_p2g": (C.c_int, [_VP, _VP, _VP, _I64, _VP]),
     "aw_backup_grid_velocity": (C.c_int, [_VP, _VP]),
     "aw_g2p": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
+    "aw_g2p_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
     "aw_advect": (C.c_int, [_VP, _VP, _I64, _F, _VP]),
     "aw_sample_velocity": (C.c_int, [_VP, _VP, _I64, _I32, _VP, _VP]),
     "aw_sort_particles": (C.c_int, [_VP, _VP, _I64, _VP, _VP, _VP]),

@@ -232,6 +232,12 @@ aw_status sort_core_soa(MsbgState& G, const float* soa_pos, int64_t n, cudaStrea
 aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_soa, const uint32_t* ids_in,
                      uint32_t* ids_out, cudaStream_t s);
 aw_status advect_launch(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* u[3], cudaStream_t s);
+// G2P (same arithmetic as aw_g2p) through caller-provided tile storage: toff holds nb offsets
+// (written here), tn and to at least the grid's total tile size in floats each.
+aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t n, float alpha, uint32_t* toff,
+                         float* tn, float* to, cudaStream_t s);
+// total tile floats of a grid whose blocks have resolutions h_res (one velocity field)
+uint64_t tile_total(const std::vector<int>& h_res);
 
 }  // namespace aw
 

@@ -874,6 +874,51 @@ aw_status advect_launch(MsbgState& G, float* pos, int pos_soa, int64_t n, float 
     return AW_OK;
 }
 
+// Exclusive scan of the per-block tile sizes in one CTA (same order and sums as the host-side
+// offsets of the grid's own tiles).
+__global__ void __launch_bounds__(1024) k_tile_offsets(const int* __restrict__ res, int nb, uint32_t* __restrict__ toff) {
+    __shared__ uint32_t part[1024];
+    const int per = (nb + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int b0 = (int)threadIdx.x * per, b1 = min(nb, b0 + per);
+    uint32_t own = 0;
+    for (int b = b0; b < b1; ++b) own += tile_block(res[b]);
+    part[threadIdx.x] = own;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        const uint32_t v = (int)threadIdx.x >= o ? part[threadIdx.x - o] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t acc = part[threadIdx.x] - own;
+    for (int b = b0; b < b1; ++b) {
+        toff[b] = acc;
+        acc += tile_block(res[b]);
+    }
+}
+
+uint64_t tile_total(const std::vector<int>& h_res) {
+    uint64_t acc = 0;
+    for (int r : h_res) acc += tile_block(r);
+    return acc;
+}
+
+aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t n, float alpha, uint32_t* toff,
+                         float* tn, float* to, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    k_tile_offsets<<<1, 1024, 0, s>>>(G.res.p, G.nb, toff);
+    AW_LAUNCH();
+    Field3 un{{G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]}};
+    Field3 uo{{G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]}};
+    k_build_tiles<<<G.nb, 128, 0, s>>>(G.view0(), un, toff, tn);
+    AW_LAUNCH();
+    k_build_tiles<<<G.nb, 128, 0, s>>>(G.view0(), uo, toff, to);
+    AW_LAUNCH();
+    k_g2p_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), PArr{d_pos, 3, 1}, PArrW{d_vel, 3, 1}, n, alpha, toff, tn, to);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 }  // namespace aw
 
 using namespace aw;

@@ -136,6 +136,16 @@ aw_status aw_backup_grid_velocity(aw_msbg* g, aw_stream s);
 /* G2PManager::performG2P (G2P.cuh:198-211): v = alpha (v + u_new - u_old) + (1 - alpha) u_new,
  * trilinear MAC samples with the staggering corrected. */
 aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_t n, float alpha, aw_stream s);
+/* No counterpart in the reference.  aw_g2p with the same arguments and results, for callers that
+ * cannot let a library allocate device memory (an allocator that owns the whole GPU, a fixed device
+ * budget, code where cudaMalloc's implicit device synchronisation is not allowed): its tile scratch
+ * is a fixed static device array (16.25 MiB, held by every device that loads it until exit).
+ * Limits: at most 65,536 blocks and 2,097,152 tile floats per velocity field (sum over active
+ * blocks of 3 (r+1) (r+2)^2, rounded up to a multiple of 4); larger grids return
+ * AW_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array (with that device
+ * current) and should come before any stream capture.  All calls share the array: calls that
+ * overlap on the GPU race. */
+aw_status aw_g2p_noalloc(aw_msbg* g, float* d_vel, const float* d_pos, int64_t n, float alpha, aw_stream s);
 /* G2PManager::advect (G2P.cuh:216-227): Ralston RK3 through VELOCITY_*, clamped to the domain
  * interior (margin 0.01 finest cells). */
 aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw_stream s);
