@@ -23,6 +23,7 @@ __global__ void k_face_sync(LevelView L, float* u0, float* u1, float* u2) {
     int cb[3];
     bcoord(L.g, b, cb);
     float* U[3] = {u0, u1, u2};
+#pragma unroll
     for (int dir = 0; dir < 6; ++dir) {
         const int a = dir >> 1, s = (dir & 1) ? 1 : -1;
         int nc[3] = {cb[0], cb[1], cb[2]};
@@ -175,8 +176,9 @@ __global__ void k_gradient(LevelView L, const PT* __restrict__ p, const uint8_t*
     const float* Wa[3] = {W0, W1, W2};
     float* U[3] = {u0, u1, u2};
     const int nf = (r + 1) * r * r;
-    for (int t = threadIdx.x; t < 3 * nf; t += blockDim.x) {
-        const int a = t / nf, fi = t - a * nf;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    for (int fi = threadIdx.x; fi < nf; fi += blockDim.x) {
         int f[3];
         if (a == 0) { f[0] = fi % (r + 1); int rem = fi / (r + 1); f[1] = rem % r; f[2] = rem / r; }
         else if (a == 1) { f[0] = fi % r; int rem = fi / r; f[1] = rem % (r + 1); f[2] = rem / (r + 1); }

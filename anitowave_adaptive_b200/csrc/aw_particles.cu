@@ -419,13 +419,16 @@ __global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* _
         }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < 3 * nf; t += blockDim.x) {
-        const int a = t / nf, fi = t - a * nf;
-        const float m = am[t], P = ap[t];
-        const uint32_t oi = L.off[1 + a][b] + (uint32_t)fi;
-        out.m[a][oi] = m;
-        if (out.mom[a]) out.mom[a][oi] = P;
-        out.u[a][oi] = m > 1e-6f ? P / m : 0.f;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const uint32_t ob = L.off[1 + a][b];
+        for (int fi = threadIdx.x; fi < nf; fi += blockDim.x) {
+            const float m = am[a * nf + fi], P = ap[a * nf + fi];
+            const uint32_t oi = ob + (uint32_t)fi;
+            out.m[a][oi] = m;
+            if (out.mom[a]) out.mom[a][oi] = P;
+            out.u[a][oi] = m > 1e-6f ? P / m : 0.f;
+        }
     }
 }
 
@@ -603,14 +606,17 @@ __global__ void k_build_tiles(LevelView L, Field3 u, const uint32_t* __restrict_
     const int R1 = r + 1, R2 = r + 2;
     const int TA = (int)tile_axis(r);
     float* out = tiles + toff[b];
-    for (int t = threadIdx.x; t < 3 * TA; t += blockDim.x) {
-        const int a = t / TA, rem = t - a * TA;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
         const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        int fi[3];
-        fi[a] = rem % R1;
-        fi[t1] = (rem / R1) % R2 - 1;
-        fi[t2] = rem / (R1 * R2) - 1;
-        out[t] = face_value(L, u.c[a], a, b, cb, r, fi);
+        const float* ua = u.c[a];
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            int fi[3];
+            fi[a] = rem % R1;
+            fi[t1] = (rem / R1) % R2 - 1;
+            fi[t2] = rem / (R1 * R2) - 1;
+            out[a * TA + rem] = face_value(L, ua, a, b, cb, r, fi);
+        }
     }
 }
 
