@@ -380,7 +380,7 @@ __global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* _
             const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
             const int ia = (int)floorf(q[a]);
             const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
-            // squared distances per candidate index, +inf where the index is outside the block
+            // squared distances per candidate index, 4 (weight 0) where the index is outside the block
             float dA2[2], dB2[2], dC2[2];
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
@@ -391,26 +391,28 @@ __global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* _
                 dB2[k] = (j1 + k >= 0 && j1 + k < r) ? dB * dB : 4.f;
                 dC2[k] = (j2 + k >= 0 && j2 + k < r) ? dC * dC : 4.f;
             }
+            // strides of the axis-a face layout (fidx) along x, y, z
+            const int sx = 1, sy = a == 0 ? r + 1 : r, sz = a == 0 ? (r + 1) * r : (a == 1 ? r * (r + 1) : r * r);
+            const int sA = a == 0 ? sx : (a == 1 ? sy : sz);
+            const int s1 = t1 == 0 ? sx : (t1 == 1 ? sy : sz);
+            const int s2 = t2 == 0 ? sx : (t2 == 1 ? sy : sz);
+            const int base = ia * sA + j1 * s1 + j2 * s2;  // index of candidate (0,0,0); may lie outside
             float* Am = am + a * nf;
             float* Ap = ap + a * nf;
             const float va = vel[a];
+            // all 8 candidates, no branches: a candidate with d^2 >= 1 (or outside the block) has
+            // t <= 0 and its two atomics are predicated off
 #pragma unroll
             for (int da = 0; da < 2; ++da)
 #pragma unroll
                 for (int d1 = 0; d1 < 2; ++d1) {
                     const float dAB = dA2[da] + dB2[d1];
-                    if (dAB >= 1.f) continue;
 #pragma unroll
                     for (int d2 = 0; d2 < 2; ++d2) {
-                        const float d2s = dAB + dC2[d2];
-                        if (d2s < 1.f) {
-                            const float tt = 1.f - d2s;
-                            const float wgt = tt * tt * tt;
-                            int f[3];
-                            f[a] = ia + da;
-                            f[t1] = j1 + d1;
-                            f[t2] = j2 + d2;
-                            const uint32_t fi = fidx(a, f[0], f[1], f[2], r);
+                        const float tt = 1.f - (dAB + dC2[d2]);
+                        const float wgt = tt * tt * tt;
+                        const int fi = base + da * sA + d1 * s1 + d2 * s2;
+                        if (tt > 0.f) {
                             atomicAdd(&Am[fi], wgt);
                             atomicAdd(&Ap[fi], wgt * va);
                         }
@@ -469,12 +471,14 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
 // oracle reproduces every choice); outside the domain or in an inactive block the index is
 // clamped back into the block.
 // ------------------------------------------------------------------------------------------------
-__device__ inline float face_value(const LevelView& L, const float* __restrict__ u, int a, int b, const int cb[3], int r,
-                                   const int fi[3]) {
+// Source face of a (possibly ghost) face index fi of block b: the face itself, the nearest face of the
+// same axis in the neighbouring block, or (outside the domain / inactive neighbour) the clamped
+// face of b.
+__device__ inline uint32_t face_source(const LevelView& L, int a, int b, const int cb[3], int r, const int fi[3]) {
     const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
     const int o1 = fi[t1] < 0 ? -1 : (fi[t1] >= r ? 1 : 0);
     const int o2 = fi[t2] < 0 ? -1 : (fi[t2] >= r ? 1 : 0);
-    if (!o1 && !o2) return u[L.off[1 + a][b] + fidx(a, fi[0], fi[1], fi[2], r)];
+    if (!o1 && !o2) return L.off[1 + a][b] + fidx(a, fi[0], fi[1], fi[2], r);
     int nc[3] = {cb[0], cb[1], cb[2]};
     nc[t1] += o1;
     nc[t2] += o2;
@@ -487,15 +491,21 @@ __device__ inline float face_value(const LevelView& L, const float* __restrict__
         int q[3] = {fi[0], fi[1], fi[2]};
         q[t1] = min(max(q[t1], 0), r - 1);
         q[t2] = min(max(q[t2], 0), r - 1);
-        return u[L.off[1 + a][b] + fidx(a, q[0], q[1], q[2], r)];
+        return L.off[1 + a][b] + fidx(a, q[0], q[1], q[2], r);
     }
+    const int sh = __ffs(2 * r) - 1;
     int q[3];
-    q[a] = (2 * fi[a] * rn + r) / (2 * r);
+    q[a] = (2 * fi[a] * rn + r) >> sh;
     const int rel1 = 2 * fi[t1] + 1 - o1 * 2 * r;
     const int rel2 = 2 * fi[t2] + 1 - o2 * 2 * r;
-    q[t1] = min(max((rel1 * rn) / (2 * r), 0), rn - 1);
-    q[t2] = min(max((rel2 * rn) / (2 * r), 0), rn - 1);
-    return u[L.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn)];
+    q[t1] = min(max((rel1 * rn) >> sh, 0), rn - 1);
+    q[t2] = min(max((rel2 * rn) >> sh, 0), rn - 1);
+    return L.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn);
+}
+
+__device__ inline float face_value(const LevelView& L, const float* __restrict__ u, int a, int b, const int cb[3], int r,
+                                   const int fi[3]) {
+    return u[face_source(L, a, b, cb, r, fi)];
 }
 
 __device__ inline float sample_comp(const LevelView& L, const float* __restrict__ u, int a, const float X[3]) {
@@ -616,6 +626,33 @@ __global__ void k_build_tiles(LevelView L, Field3 u, const uint32_t* __restrict_
             fi[t1] = (rem / R1) % R2 - 1;
             fi[t2] = rem / (R1 * R2) - 1;
             out[a * TA + rem] = face_value(L, ua, a, b, cb, r, fi);
+        }
+    }
+}
+
+// Both ghosted tiles of G2P (u_new and u_old) in one pass: every entry's source face is located
+// once and read from the two fields.
+__global__ void k_build_tiles2(LevelView L, Field3 un, Field3 uo, const uint32_t* __restrict__ toff,
+                               float* __restrict__ tn, float* __restrict__ to) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const int R1 = r + 1, R2 = r + 2;
+    const int TA = (int)tile_axis(r);
+    const uint32_t o = toff[b];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            int fi[3];
+            fi[a] = rem % R1;
+            fi[t1] = (rem / R1) % R2 - 1;
+            fi[t2] = rem / (R1 * R2) - 1;
+            const uint32_t src = face_source(L, a, b, cb, r, fi);
+            tn[o + a * TA + rem] = un.c[a][src];
+            to[o + a * TA + rem] = uo.c[a][src];
         }
     }
 }
@@ -771,6 +808,15 @@ aw_status build_tiles(MsbgState& G, const float* u[3], float* tiles, cudaStream_
     return AW_OK;
 }
 
+// u_new into G.tiles_new and u_old into G.tiles_old, one launch
+aw_status build_tiles2(MsbgState& G, const float* un[3], const float* uo[3], cudaStream_t s) {
+    AW_CHECK_ARG(G.tile_off.p && G.tiles_new.p && G.tiles_old.p, "tiles not allocated");
+    Field3 a{{un[0], un[1], un[2]}}, b{{uo[0], uo[1], uo[2]}};
+    k_build_tiles2<<<G.nb, 128, 0, s>>>(G.view0(), a, b, G.tile_off.p, G.tiles_new.p, G.tiles_old.p);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
     if (!G.err.p) return AW_OK;
     int h[4];
@@ -787,8 +833,7 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
                      const float* uo[3], cudaStream_t s) {
     if (n <= 0) return AW_OK;
     AW_TRY(ensure_tiles(G));
-    AW_TRY(build_tiles(G, un, G.tiles_new.p, s));
-    AW_TRY(build_tiles(G, uo, G.tiles_old.p, s));
+    AW_TRY(build_tiles2(G, un, uo, s));
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
     const size_t smem = g2p_smem(maxres);
@@ -982,8 +1027,7 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
     if (n == 0) return AW_OK;
     cudaStream_t s = (cudaStream_t)s_;
     AW_TRY(ensure_tiles(G));
-    AW_TRY(build_tiles(G, un, G.tiles_new.p, s));
-    AW_TRY(build_tiles(G, uo, G.tiles_old.p, s));
+    AW_TRY(build_tiles2(G, un, uo, s));
     k_g2p_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), PArr{d_pos, 3, 1}, PArrW{d_vel, 3, 1}, n, alpha, G.tile_off.p,
                                         G.tiles_new.p, G.tiles_old.p);
     AW_LAUNCH();

@@ -1331,13 +1331,17 @@ OC_API void oc_particle_keys(void* h, const float* pos, int64_t n, uint32_t* key
 
 // P2G (gather form) on sorted or unsorted particles.  u/m per axis (level-0 face layout).
 // cell_count: particles per level-0 cell.
-OC_API void oc_p2g(void* h, const float* pos, const float* vel, int64_t n, double* ux, double* uy, double* uz,
-                   double* mx, double* my, double* mz, uint32_t* cell_count) {
-    Ctx* C = (Ctx*)h;
+namespace {
+template <class PT>
+void p2g_impl(Ctx* C, const PT* pos, const PT* vel, int64_t n, double* ux, double* uy, double* uz, double* mx,
+              double* my, double* mz, uint32_t* cell_count) {
     const Geo& g = C->g;
     PartGrid PG = make_pgrid(*C);
     std::vector<uint32_t> k(n);
-    for (int64_t i = 0; i < n; ++i) k[i] = particle_key(PG, pos + 3 * i);
+    for (int64_t i = 0; i < n; ++i) {
+        const float pf[3] = {(float)pos[3 * i], (float)pos[3 * i + 1], (float)pos[3 * i + 2]};
+        k[i] = particle_key(PG, pf);
+    }
     std::vector<int64_t> idx(n);
     std::iota(idx.begin(), idx.end(), 0);
     std::stable_sort(idx.begin(), idx.end(), [&](int64_t a, int64_t b) { return k[a] < k[b]; });
@@ -1413,6 +1417,18 @@ OC_API void oc_p2g(void* h, const float* pos, const float* vel, int64_t n, doubl
                     }
         }
     }
+}
+
+}  // namespace
+
+OC_API void oc_p2g(void* h, const float* pos, const float* vel, int64_t n, double* ux, double* uy, double* uz,
+                   double* mx, double* my, double* mz, uint32_t* cell_count) {
+    p2g_impl((Ctx*)h, pos, vel, n, ux, uy, uz, mx, my, mz, cell_count);
+}
+// P2G on FP64 particle state (the differentiable rollout); cells of particles from float(pos)
+OC_API void oc_p2g64(void* h, const double* pos, const double* vel, int64_t n, double* ux, double* uy, double* uz,
+                     double* mx, double* my, double* mz, uint32_t* cell_count) {
+    p2g_impl((Ctx*)h, pos, vel, n, ux, uy, uz, mx, my, mz, cell_count);
 }
 
 // T-junction sync: a coarse block's boundary face := mean of the 4 fine faces it covers.
@@ -1618,6 +1634,437 @@ OC_API void oc_advect(void* h, const double* u[3], double dt, const double* xin,
             double v = (2.0 / 9.0) * k1[a] + (3.0 / 9.0) * k2[a] + (4.0 / 9.0) * k3[a];
             double y = x[a] + dt * v;
             xout[3 * i + a] = std::min(std::max(y, lo[a]), hi[a]);
+        }
+    }
+}
+
+// ================================================================================================
+// Adjoint of the FLIP step (vector-Jacobian products), FP64.
+//
+// The forward map differentiated is the step above with its discrete decisions held fixed: the
+// cell of every particle, the fluid flags, each kernel's support, the clamp branches of the
+// trilinear sample and of the advection.  Every VJP accumulates (+=) into its output adjoints.
+// The projection's adjoint reuses the forward solve: the FV operator is symmetric, so
+// b_bar = A^{-1} p_bar is one more solve with the same hierarchy.
+// ================================================================================================
+namespace {
+
+// index (into the axis-a face array) of the face that supplies ghost face fi of block b — the
+// rule of face_value_at
+uint32_t face_src(const Ctx& C, const PartGrid& PG, int a, int b, const int cb[3], int r, const int fi[3]) {
+    const Geo& g = C.g;
+    int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
+    int o1 = fi[t1] < 0 ? -1 : (fi[t1] >= r ? 1 : 0);
+    int o2 = fi[t2] < 0 ? -1 : (fi[t2] >= r ? 1 : 0);
+    if (!o1 && !o2) return PG.off[1 + a][b] + fidx(a, fi[0], fi[1], fi[2], r);
+    int nc[3] = {cb[0], cb[1], cb[2]};
+    nc[t1] += o1;
+    nc[t2] += o2;
+    int rn = 0, n = 0;
+    if (inside(g, nc)) {
+        n = bidx(g, nc[0], nc[1], nc[2]);
+        rn = PG.res[n];
+    }
+    if (!rn) {
+        int q[3] = {fi[0], fi[1], fi[2]};
+        q[t1] = std::min(std::max(q[t1], 0), r - 1);
+        q[t2] = std::min(std::max(q[t2], 0), r - 1);
+        return PG.off[1 + a][b] + fidx(a, q[0], q[1], q[2], r);
+    }
+    int q[3];
+    q[a] = (2 * fi[a] * rn + r) / (2 * r);
+    int rel1 = 2 * fi[t1] + 1 - o1 * 2 * r;
+    int rel2 = 2 * fi[t2] + 1 - o2 * 2 * r;
+    q[t1] = std::min(std::max((rel1 * rn) / (2 * r), 0), rn - 1);
+    q[t2] = std::min(std::max((rel2 * rn) / (2 * r), 0), rn - 1);
+    return PG.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn);
+}
+
+// Trilinear MAC sample of component a at X as a stencil: 8 source faces, their weights and the
+// derivative of each weight with respect to X (zero along a clamped axis).
+struct Stencil {
+    int n = 0;
+    uint32_t idx[8];
+    double w[8];
+    double dw[8][3];
+};
+
+Stencil sample_stencil(const Ctx& C, const PartGrid& PG, int a, const double X[3]) {
+    Stencil S;
+    const Geo& g = C.g;
+    float Xf[3] = {(float)X[0], (float)X[1], (float)X[2]};
+    int cb[3];
+    point_block(g, Xf, cb);
+    int b = bidx(g, cb[0], cb[1], cb[2]);
+    int r = PG.res[b];
+    if (!r) return S;
+    double h = (double)fcell(g, r);
+    int i0[3];
+    double f[3], df[3];
+    for (int k = 0; k < 3; ++k) {
+        double o = (double)forigin(g, k, cb[k]);
+        double s = (X[k] - o) / h;
+        int lo = 0, hi = r;
+        if (k != a) { s -= 0.5; lo = -1; }
+        df[k] = (s > lo && s < hi) ? 1.0 / h : 0.0;
+        s = std::min(std::max(s, (double)lo), (double)hi);
+        int i = (int)std::floor(s);
+        i = std::min(std::max(i, lo), hi - 1);
+        i0[k] = i;
+        f[k] = s - i;
+    }
+    S.n = 8;
+    int k = 0;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx, ++k) {
+                int fi[3] = {i0[0] + dx, i0[1] + dy, i0[2] + dz};
+                double wx = dx ? f[0] : 1 - f[0], wy = dy ? f[1] : 1 - f[1], wz = dz ? f[2] : 1 - f[2];
+                double sx = dx ? 1.0 : -1.0, sy = dy ? 1.0 : -1.0, sz = dz ? 1.0 : -1.0;
+                S.idx[k] = face_src(C, PG, a, b, cb, r, fi);
+                S.w[k] = wx * wy * wz;
+                S.dw[k][0] = sx * wy * wz * df[0];
+                S.dw[k][1] = wx * sy * wz * df[1];
+                S.dw[k][2] = wx * wy * sz * df[2];
+            }
+    return S;
+}
+
+inline void atomic_add(double* p, double v) {
+#pragma omp atomic
+    *p += v;
+}
+
+// y = I(u, X) for one component: ubar[idx] += w * ybar; Xbar += ybar * sum_k dw_k u[idx_k]
+void sample_vjp(const Ctx& C, const PartGrid& PG, const double* u, int a, const double X[3], double ybar,
+                double* ubar, double* Xbar) {
+    Stencil S = sample_stencil(C, PG, a, X);
+    for (int k = 0; k < S.n; ++k) {
+        if (ubar) atomic_add(&ubar[S.idx[k]], S.w[k] * ybar);
+        if (Xbar)
+            for (int j = 0; j < 3; ++j) Xbar[j] += ybar * S.dw[k][j] * u[S.idx[k]];
+    }
+}
+
+double sample_val(const Ctx& C, const PartGrid& PG, const double* u, int a, const double X[3]) {
+    Stencil S = sample_stencil(C, PG, a, X);
+    double acc = 0;
+    for (int k = 0; k < S.n; ++k) acc += S.w[k] * u[S.idx[k]];
+    return acc;
+}
+
+}  // namespace
+
+// Sample (3 components) at FP64 points through the stencil form (equals oc_sample).
+OC_API void oc_sample_stencil(void* h, const double* X, int64_t n, const double* u[3], double* out) {
+    Ctx* C = (Ctx*)h;
+    PartGrid PG = make_pgrid(*C);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) out[3 * i + a] = sample_val(*C, PG, u[a], a, X + 3 * i);
+}
+
+// VJP of y = sample(u, X): ubar += I^T ybar; Xbar += (dI/dX)^T ybar (Xbar may be null)
+OC_API void oc_sample_vjp(void* h, const double* X, int64_t n, const double* u[3], const double* ybar, double* ubar[3],
+                          double* Xbar) {
+    Ctx* C = (Ctx*)h;
+    PartGrid PG = make_pgrid(*C);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a)
+            sample_vjp(*C, PG, u[a], a, X + 3 * i, ybar[3 * i + a], ubar[a], Xbar ? Xbar + 3 * i : nullptr);
+}
+
+// G2P on FP64 state: v' = alpha (v + I(un) - I(uo)) + (1 - alpha) I(un)
+OC_API void oc_g2p64(void* h, const double* X, int64_t n, const double* un[3], const double* uo[3], double alpha,
+                     const double* vin, double* vout) {
+    Ctx* C = (Ctx*)h;
+    PartGrid PG = make_pgrid(*C);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            double vn = sample_val(*C, PG, un[a], a, X + 3 * i);
+            double vo = sample_val(*C, PG, uo[a], a, X + 3 * i);
+            vout[3 * i + a] = alpha * (vin[3 * i + a] + (vn - vo)) + (1.0 - alpha) * vn;
+        }
+}
+
+// VJP of oc_g2p64.  vbar: adjoint of v' on input, adjoint of v on output.  Xbar, unbar, uobar +=.
+OC_API void oc_g2p_vjp(void* h, const double* X, int64_t n, const double* un[3], const double* uo[3], double alpha,
+                       double* vbar, double* Xbar, double* unbar[3], double* uobar[3]) {
+    Ctx* C = (Ctx*)h;
+    PartGrid PG = make_pgrid(*C);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            const double g = vbar[3 * i + a];
+            sample_vjp(*C, PG, un[a], a, X + 3 * i, g, unbar[a], Xbar + 3 * i);
+            sample_vjp(*C, PG, uo[a], a, X + 3 * i, -alpha * g, uobar[a], Xbar + 3 * i);
+            vbar[3 * i + a] = alpha * g;
+        }
+}
+
+// VJP of oc_advect (Ralston RK3 + clamp).  xbar: adjoint of x' on input, of x on output.
+OC_API void oc_advect_vjp(void* h, const double* u[3], double dt, const double* xin, int64_t n, double* xbar,
+                          double* ubar[3]) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    PartGrid PG = make_pgrid(*C);
+    double h0 = (double)g.bs / g.R0;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = g.dmin[a] + 0.01 * h0;
+        hi[a] = g.dmin[a] + (double)g.D[a] * g.bs - 0.01 * h0;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        const double* x = xin + 3 * i;
+        double k1[3], k2[3], k3[3], y1[3], y2[3];
+        for (int a = 0; a < 3; ++a) k1[a] = sample_val(*C, PG, u[a], a, x);
+        for (int a = 0; a < 3; ++a) y1[a] = x[a] + 0.5 * dt * k1[a];
+        for (int a = 0; a < 3; ++a) k2[a] = sample_val(*C, PG, u[a], a, y1);
+        for (int a = 0; a < 3; ++a) y2[a] = x[a] + 0.75 * dt * k2[a];
+        for (int a = 0; a < 3; ++a) k3[a] = sample_val(*C, PG, u[a], a, y2);
+        double gx[3], k1b[3], k2b[3], k3b[3], y1b[3] = {0, 0, 0}, y2b[3] = {0, 0, 0};
+        for (int a = 0; a < 3; ++a) {
+            double v = (2.0 / 9.0) * k1[a] + (3.0 / 9.0) * k2[a] + (4.0 / 9.0) * k3[a];
+            double y = x[a] + dt * v;
+            double gb = (y > lo[a] && y < hi[a]) ? xbar[3 * i + a] : 0.0;
+            gx[a] = gb;
+            k1b[a] = (2.0 / 9.0) * dt * gb;
+            k2b[a] = (3.0 / 9.0) * dt * gb;
+            k3b[a] = (4.0 / 9.0) * dt * gb;
+        }
+        for (int a = 0; a < 3; ++a) sample_vjp(*C, PG, u[a], a, y2, k3b[a], ubar[a], y2b);
+        for (int a = 0; a < 3; ++a) {
+            gx[a] += y2b[a];
+            k2b[a] += 0.75 * dt * y2b[a];
+        }
+        for (int a = 0; a < 3; ++a) sample_vjp(*C, PG, u[a], a, y1, k2b[a], ubar[a], y1b);
+        for (int a = 0; a < 3; ++a) {
+            gx[a] += y1b[a];
+            k1b[a] += 0.5 * dt * y1b[a];
+        }
+        for (int a = 0; a < 3; ++a) sample_vjp(*C, PG, u[a], a, x, k1b[a], ubar[a], gx);
+        for (int a = 0; a < 3; ++a) xbar[3 * i + a] = gx[a];
+    }
+}
+
+// VJP of oc_p2g64 through the normalisation u = P/m (m > 1e-6): given ubar per face and the
+// forward u, m, accumulate pos_bar and vel_bar per particle.  Every particle gathers from the
+// faces within one cell size (of the face's block) of it, in its own and the 26 neighbouring
+// blocks.
+OC_API void oc_p2g_vjp(void* h, const double* pos, const double* vel, int64_t n, const double* u[3],
+                       const double* m[3], const double* ubar[3], double* pos_bar, double* vel_bar) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    PartGrid PG = make_pgrid(*C);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t i = 0; i < n; ++i) {
+        const double* X = pos + 3 * i;
+        float Xf[3] = {(float)X[0], (float)X[1], (float)X[2]};
+        int pc[3];
+        point_block(g, Xf, pc);
+        double xb[3] = {0, 0, 0}, vb[3] = {0, 0, 0};
+        for (int d = 0; d < 27; ++d) {
+            int nc[3] = {pc[0] + d % 3 - 1, pc[1] + (d / 3) % 3 - 1, pc[2] + d / 9 - 1};
+            if (!inside(g, nc)) continue;
+            int b = bidx(g, nc[0], nc[1], nc[2]);
+            int r = PG.res[b];
+            if (!r) continue;
+            double hh = (double)fcell(g, r);
+            double q[3];
+            for (int k = 0; k < 3; ++k) q[k] = (X[k] - (double)forigin(g, k, nc[k])) / hh;
+            bool out = false;
+            for (int k = 0; k < 3; ++k) out |= q[k] <= -1.0 || q[k] >= r + 1.0;
+            if (out) continue;
+            for (int a = 0; a < 3; ++a) {
+                int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+                int ia = (int)std::floor(q[a]);
+                int j1 = (int)std::floor(q[t1] - 0.5), j2 = (int)std::floor(q[t2] - 0.5);
+                for (int da = 0; da < 2; ++da)
+                    for (int d1 = 0; d1 < 2; ++d1)
+                        for (int d2 = 0; d2 < 2; ++d2) {
+                            int f[3];
+                            f[a] = ia + da;
+                            f[t1] = j1 + d1;
+                            f[t2] = j2 + d2;
+                            if (f[a] < 0 || f[a] > r || f[t1] < 0 || f[t1] >= r || f[t2] < 0 || f[t2] >= r) continue;
+                            double Q[3];
+                            for (int k = 0; k < 3; ++k) Q[k] = f[k] + (k == a ? 0.0 : 0.5);
+                            double dq[3] = {q[0] - Q[0], q[1] - Q[1], q[2] - Q[2]};
+                            double d2s = dq[0] * dq[0] + dq[1] * dq[1] + dq[2] * dq[2];
+                            if (d2s >= 1.0) continue;
+                            uint32_t fi = PG.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r);
+                            double mf = m[a][fi];
+                            if (!(mf > 1e-6)) continue;
+                            double Pbar = ubar[a][fi] / mf;
+                            double mbar = -ubar[a][fi] * u[a][fi] / mf;
+                            double t = 1.0 - d2s;
+                            double w = t * t * t;
+                            double coef = -6.0 * t * t / hh * (Pbar * vel[3 * i + a] + mbar);
+                            vb[a] += w * Pbar;
+                            for (int k = 0; k < 3; ++k) xb[k] += coef * dq[k];
+                        }
+            }
+        }
+        for (int k = 0; k < 3; ++k) {
+            pos_bar[3 * i + k] += xb[k];
+            vel_bar[3 * i + k] += vb[k];
+        }
+    }
+}
+
+// VJP of oc_face_sync: fine faces receive a quarter of each synced coarse face's adjoint, which
+// is then cleared.  In place on ubar.
+OC_API void oc_face_sync_vjp(void* h, double* ux, double* uy, double* uz) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    PartGrid PG = make_pgrid(*C);
+    double* U[3] = {ux, uy, uz};
+    for (int b = 0; b < g.nb(); ++b) {
+        int r = PG.res[b];
+        if (!r) continue;
+        int cb[3];
+        bcoord(g, b, cb);
+        for (int a = 0; a < 3; ++a) {
+            int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            for (int s = -1; s <= 1; s += 2) {
+                int nc[3] = {cb[0], cb[1], cb[2]};
+                nc[a] += s;
+                if (!inside(g, nc)) continue;
+                int n = bidx(g, nc[0], nc[1], nc[2]);
+                int rn = PG.res[n];
+                if (rn != 2 * r) continue;
+                for (int u1 = 0; u1 < r; ++u1)
+                    for (int u2 = 0; u2 < r; ++u2) {
+                        int f[3];
+                        f[a] = s > 0 ? r : 0;
+                        f[t1] = u1;
+                        f[t2] = u2;
+                        uint32_t ci = PG.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r);
+                        double gbar = U[a][ci];
+                        U[a][ci] = 0.0;
+                        for (int d1 = 0; d1 < 2; ++d1)
+                            for (int d2 = 0; d2 < 2; ++d2) {
+                                int q[3];
+                                q[a] = s > 0 ? 0 : rn;
+                                q[t1] = 2 * u1 + d1;
+                                q[t2] = 2 * u2 + d2;
+                                U[a][PG.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn)] += 0.25 * gbar;
+                            }
+                    }
+            }
+        }
+    }
+}
+
+// VJP of oc_divergence: ubar += D^T bbar (fluid cells only)
+OC_API void oc_divergence_vjp(void* h, const double* bbar, const uint8_t* fluid, double inv_dt, double* ux, double* uy,
+                              double* uz) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    PartGrid PG = make_pgrid(*C);
+    double* U[3] = {ux, uy, uz};
+    for (int b = 0; b < g.nb(); ++b) {
+        int r = PG.res[b];
+        if (!r) continue;
+        double H = (double)g.bs / r;
+        for (int z = 0; z < r; ++z)
+            for (int y = 0; y < r; ++y)
+                for (int x = 0; x < r; ++x) {
+                    uint32_t ci = PG.off[0][b] + cidx(x, y, z, r);
+                    if (!fluid[ci]) continue;
+                    double s = bbar[ci] * H * H * inv_dt;
+                    int c[3] = {x, y, z};
+                    for (int a = 0; a < 3; ++a) {
+                        int hi[3] = {c[0], c[1], c[2]};
+                        hi[a] += 1;
+                        U[a][PG.off[1 + a][b] + fidx(a, hi[0], hi[1], hi[2], r)] += s;
+                        U[a][PG.off[1 + a][b] + fidx(a, c[0], c[1], c[2], r)] -= s;
+                    }
+                }
+    }
+}
+
+// VJP of oc_gradient_update: ubar (in place) := ubar with wall faces cleared; pbar += -dt (W/area)
+// (d(p_high - p_low)/dp)^T ubar on faces with a fluid cell on either side.
+OC_API void oc_gradient_vjp(void* h, double dt, double* ux, double* uy, double* uz, double* pbar) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    Lvl& L = C->lv[0];
+    double* U[3] = {ux, uy, uz};
+    for (int b = 0; b < g.nb(); ++b) {
+        int r = L.res[b];
+        if (!r) continue;
+        int cb[3];
+        bcoord(g, b, cb);
+        double H = (double)g.bs / r;
+        double area = H * H;
+        for (int a = 0; a < 3; ++a) {
+            int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            for (int fa = 0; fa <= r; ++fa)
+                for (int u1 = 0; u1 < r; ++u1)
+                    for (int u2 = 0; u2 < r; ++u2) {
+                        int f[3];
+                        f[a] = fa; f[t1] = u1; f[t2] = u2;
+                        uint32_t fi = L.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r);
+                        // cells (and weights) of the low and high pressure values
+                        uint32_t cells[2][4];
+                        double cw[2][4];
+                        int nc_[2] = {0, 0};
+                        bool fl[2] = {false, false};
+                        bool wall = false;
+                        for (int side = 0; side < 2; ++side) {
+                            int c[3] = {f[0], f[1], f[2]};
+                            if (side == 0) c[a] -= 1;
+                            if (c[a] >= 0 && c[a] < r) {
+                                uint32_t ci = L.off[0][b] + cidx(c[0], c[1], c[2], r);
+                                cells[side][0] = ci;
+                                cw[side][0] = 1.0;
+                                nc_[side] = 1;
+                                fl[side] = L.fluid[ci];
+                                continue;
+                            }
+                            int cin[3] = {f[0], f[1], f[2]};
+                            cin[a] = side == 0 ? 0 : r - 1;
+                            int s = side == 0 ? -1 : 1;
+                            int nb3[3] = {cb[0], cb[1], cb[2]};
+                            nb3[a] += s;
+                            if (!inside(g, nb3)) { wall = true; continue; }
+                            int n = bidx(g, nb3[0], nb3[1], nb3[2]);
+                            int rn = L.res[n];
+                            if (!rn) continue;
+                            int na = s > 0 ? 0 : rn - 1;
+                            if (rn == r || 2 * rn == r) {
+                                int sh = rn == r ? 0 : 1;
+                                int q[3];
+                                q[a] = na; q[t1] = cin[t1] >> sh; q[t2] = cin[t2] >> sh;
+                                uint32_t ci = L.off[0][n] + cidx(q[0], q[1], q[2], rn);
+                                cells[side][0] = ci;
+                                cw[side][0] = 1.0;
+                                nc_[side] = 1;
+                                fl[side] = L.fluid[ci];
+                            } else {
+                                int k = 0;
+                                for (int d1 = 0; d1 < 2; ++d1)
+                                    for (int d2 = 0; d2 < 2; ++d2, ++k) {
+                                        int q[3];
+                                        q[a] = na; q[t1] = 2 * cin[t1] + d1; q[t2] = 2 * cin[t2] + d2;
+                                        uint32_t ci = L.off[0][n] + cidx(q[0], q[1], q[2], rn);
+                                        cells[side][k] = ci;
+                                        cw[side][k] = 0.25;
+                                        fl[side] = fl[side] || L.fluid[ci];
+                                    }
+                                nc_[side] = 4;
+                            }
+                        }
+                        if (wall) { U[a][fi] = 0.0; continue; }
+                        if (!fl[0] && !fl[1]) continue;
+                        double coef = -dt * (L.W[a][fi] / area) * U[a][fi];
+                        for (int k = 0; k < nc_[1]; ++k) pbar[cells[1][k]] += coef * cw[1][k];
+                        for (int k = 0; k < nc_[0]; ++k) pbar[cells[0][k]] -= coef * cw[0][k];
+                    }
         }
     }
 }

@@ -79,6 +79,21 @@ def lib():
         L.oc_g2p.argtypes = [P, f32p, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_double, f32p, f64p]
         L.oc_sample.argtypes = [P, f64p, C.c_int64, C.POINTER(C.c_void_p), f64p]
         L.oc_advect.argtypes = [P, C.POINTER(C.c_void_p), C.c_double, f64p, C.c_int64, f64p]
+        # FP64 particle state and the adjoint (VJP) of the FLIP step
+        L.oc_p2g64.argtypes = [P, f64p, f64p, C.c_int64, f64p, f64p, f64p, f64p, f64p, f64p, u32p]
+        L.oc_g2p64.argtypes = [P, f64p, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_double, f64p,
+                               f64p]
+        L.oc_sample_stencil.argtypes = [P, f64p, C.c_int64, C.POINTER(C.c_void_p), f64p]
+        L.oc_sample_vjp.argtypes = [P, f64p, C.c_int64, C.POINTER(C.c_void_p), f64p, C.POINTER(C.c_void_p),
+                                    C.c_void_p]
+        L.oc_g2p_vjp.argtypes = [P, f64p, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_double, f64p,
+                                 f64p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]
+        L.oc_advect_vjp.argtypes = [P, C.POINTER(C.c_void_p), C.c_double, f64p, C.c_int64, f64p, C.POINTER(C.c_void_p)]
+        L.oc_p2g_vjp.argtypes = [P, f64p, f64p, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                 C.POINTER(C.c_void_p), f64p, f64p]
+        L.oc_face_sync_vjp.argtypes = [P, f64p, f64p, f64p]
+        L.oc_divergence_vjp.argtypes = [P, f64p, u8p, C.c_double, f64p, f64p, f64p]
+        L.oc_gradient_vjp.argtypes = [P, C.c_double, f64p, f64p, f64p, f64p]
         _lib = L
     return _lib
 
@@ -290,6 +305,66 @@ class Oracle:
         lib().oc_sample(self.h, X, X.shape[0], _ptrs(u), out)
         return out
 
+    # ---- FP64 particle state and VJPs (the differentiable rollout) ------------------------------
+    def _faces(self):
+        t = self.tot0
+        return [np.zeros(int(t[1 + a])) for a in range(3)]
+
+    def p2g64(self, pos, vel):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float64).reshape(-1, 3)
+        u, m = self._faces(), self._faces()
+        cnt = np.zeros(int(self.tot0[0]), np.uint32)
+        lib().oc_p2g64(self.h, pos, vel, pos.shape[0], u[0], u[1], u[2], m[0], m[1], m[2], cnt)
+        return u, m, cnt
+
+    def g2p64(self, pos, un, uo, alpha, vel):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        un = [np.ascontiguousarray(x, np.float64) for x in un]
+        uo = [np.ascontiguousarray(x, np.float64) for x in uo]
+        out = np.zeros_like(pos)
+        lib().oc_g2p64(self.h, pos, pos.shape[0], _ptrs(un), _ptrs(uo), alpha,
+                       np.ascontiguousarray(vel, np.float64).reshape(-1, 3), out)
+        return out
+
+    def sample_vjp(self, X, u, ybar, ubar, Xbar=None):
+        X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+        u = [np.ascontiguousarray(x, np.float64) for x in u]
+        lib().oc_sample_vjp(self.h, X, X.shape[0], _ptrs(u), np.ascontiguousarray(ybar, np.float64).reshape(-1, 3),
+                            _ptrs(ubar), None if Xbar is None else Xbar.ctypes.data)
+
+    def g2p_vjp(self, X, un, uo, alpha, vbar, Xbar, unbar, uobar):
+        X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+        un = [np.ascontiguousarray(x, np.float64) for x in un]
+        uo = [np.ascontiguousarray(x, np.float64) for x in uo]
+        lib().oc_g2p_vjp(self.h, X, X.shape[0], _ptrs(un), _ptrs(uo), alpha, vbar, Xbar, _ptrs(unbar), _ptrs(uobar))
+
+    def advect_vjp(self, u, dt, X, xbar, ubar):
+        X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
+        u = [np.ascontiguousarray(x, np.float64) for x in u]
+        lib().oc_advect_vjp(self.h, _ptrs(u), dt, X, X.shape[0], xbar, _ptrs(ubar))
+
+    def p2g_vjp(self, pos, vel, u, m, ubar, pos_bar, vel_bar):
+        pos = np.ascontiguousarray(pos, np.float64).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float64).reshape(-1, 3)
+        u = [np.ascontiguousarray(x, np.float64) for x in u]
+        m = [np.ascontiguousarray(x, np.float64) for x in m]
+        ubar = [np.ascontiguousarray(x, np.float64) for x in ubar]
+        lib().oc_p2g_vjp(self.h, pos, vel, pos.shape[0], _ptrs(u), _ptrs(m), _ptrs(ubar), pos_bar, vel_bar)
+
+    def face_sync_vjp(self, ubar):
+        ubar = [np.ascontiguousarray(x, np.float64).copy() for x in ubar]
+        lib().oc_face_sync_vjp(self.h, *ubar)
+        return ubar
+
+    def divergence_vjp(self, bbar, fluid, dt, ubar):
+        lib().oc_divergence_vjp(self.h, np.ascontiguousarray(bbar, np.float64), np.ascontiguousarray(fluid, np.uint8),
+                                1.0 / dt, *ubar)
+
+    def gradient_vjp(self, dt, ubar, pbar):
+        """In place on ubar (wall faces cleared); pbar += gradient^T ubar.  Needs build() of the step."""
+        lib().oc_gradient_vjp(self.h, dt, ubar[0], ubar[1], ubar[2], pbar)
+
     def advect(self, u, dt, X):
         X = np.ascontiguousarray(X, np.float64).reshape(-1, 3)
         u = [np.ascontiguousarray(x, np.float64) for x in u]
@@ -322,3 +397,69 @@ def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=2
     vnew = O.g2p(ps, un, uo, alpha, vs)
     xnew = O.advect(un, dt, ps.astype(np.float64))
     return xnew, vnew, perm, dict(u_star=u, u_old=uo, u_new=un, p=p, b=b, fluid=fluid, hist=hist, count=cnt)
+
+
+# ------------------------------------------------------------------------------------------------
+# Differentiable rollout in FP64 (the oracle gradient).  State x, v in particle-id order.
+# ------------------------------------------------------------------------------------------------
+def flip_step64(O: "Oracle", x, v, dt, alpha, gravity, tol=1e-12, max_cycles=200, fluid=None):
+    """One FLIP step on FP64 state, the GPU step's order.  Returns x', v' and the record the VJP
+    needs.  `fluid` (optional) replaces the fluid flags derived from the particle counts."""
+    u1, m, cnt = O.p2g64(x, v)
+    u2 = O.face_sync(u1)
+    uo = [a.copy() for a in u2]
+    u4 = O.wall_bc([u2[a] + dt * gravity[a] for a in range(3)])
+    fl = (cnt > 0).astype(np.uint8) if fluid is None else fluid
+    b = O.divergence(u4, fl, dt)
+    O.set_params(mode=0)
+    O.build(fluid=fl)
+    p, _ = O.solve(b, tol=tol, max_cycles=max_cycles)
+    u6 = O.wall_bc(O.face_sync(O.gradient_update(p, dt, u4)))
+    v2 = O.g2p64(x, u6, uo, alpha, v)
+    x2 = O.advect(u6, dt, x)
+    return x2, v2, dict(x=x, v=v, u1=u1, m=m, uo=uo, u6=u6, fluid=fl)
+
+
+def flip_step64_vjp(O: "Oracle", rec, xbar, vbar, dt, alpha, tol=1e-12, max_cycles=200):
+    """Adjoint of flip_step64: (xbar', vbar') -> (xbar, vbar)."""
+    x, v, u6, uo = rec["x"], rec["v"], rec["u6"], rec["uo"]
+    unb, uob = O._faces(), O._faces()
+    xb = np.array(xbar, np.float64).reshape(-1, 3)
+    O.advect_vjp(u6, dt, x, xb, unb)
+    vb = np.array(vbar, np.float64).reshape(-1, 3)
+    O.g2p_vjp(x, u6, uo, alpha, vb, xb, unb, uob)
+    g = O.face_sync_vjp(O.wall_bc(unb))
+    O.set_params(mode=0)
+    O.build(fluid=rec["fluid"])
+    pbar = np.zeros(int(O.tot0[0]))
+    O.gradient_vjp(dt, g, pbar)
+    bbar, _ = O.solve(pbar * rec["fluid"], tol=tol, max_cycles=max_cycles)
+    O.divergence_vjp(bbar, rec["fluid"], dt, g)
+    g = O.wall_bc(g)
+    g = O.face_sync_vjp([g[a] + uob[a] for a in range(3)])
+    O.p2g_vjp(x, v, rec["u1"], rec["m"], g, xb, vb)
+    return xb, vb
+
+
+def rollout64(O: "Oracle", x0, u0, steps, dt, alpha, gravity, target, tol=1e-12, fluids=None):
+    """v0 = MAC sample of u0 at x0, then `steps` FLIP steps; loss = mean |x_N - target|^2."""
+    x = np.ascontiguousarray(x0, np.float64).reshape(-1, 3)
+    v = O.sample(x, u0)
+    recs = []
+    for k in range(steps):
+        x, v, rec = flip_step64(O, x, v, dt, alpha, gravity, tol, fluid=None if fluids is None else fluids[k])
+        recs.append(rec)
+    loss = float(((x - target) ** 2).sum(1).mean())
+    return loss, x, recs
+
+
+def rollout64_grad(O: "Oracle", x0, u0, recs, xN, target, dt, alpha, tol=1e-12):
+    """d loss / d u0 (three face arrays) by the adjoint of rollout64."""
+    n = xN.shape[0]
+    xb = 2.0 * (xN - target) / n
+    vb = np.zeros_like(xb)
+    for rec in reversed(recs):
+        xb, vb = flip_step64_vjp(O, rec, xb, vb, dt, alpha, tol)
+    ub = O._faces()
+    O.sample_vjp(np.ascontiguousarray(x0, np.float64).reshape(-1, 3), u0, vb, ub, None)
+    return ub
