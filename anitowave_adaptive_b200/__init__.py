@@ -124,6 +124,18 @@ SIGNATURES = {
     "aw_flip_stats_get": (C.c_int, [_VP, C.POINTER(FlipStats)]),
     "aw_flip_particles": (C.c_int, [_VP, _VP, _VP]),
     "aw_flip_solver": (C.c_int, [_VP, _PP]),
+    "aw_solver_precision": (C.c_int, [_VP, C.POINTER(_I32)]),
+    "aw_project": (C.c_int, [_VP, _VP, _VP, _F, _VP]),
+    "aw_vjp_project": (C.c_int, [_VP, _VP, _VP, _F, _PP, _VP]),
+    "aw_vjp_p2g": (C.c_int, [_VP, _VP, _VP, _I64, _PP, _VP, _VP, _VP]),
+    "aw_vjp_g2p": (C.c_int, [_VP, _VP, _I64, _F, _VP, _VP, _PP, _PP, _VP]),
+    "aw_vjp_advect": (C.c_int, [_VP, _VP, _I64, _F, _VP, _PP, _VP]),
+    "aw_vjp_sample": (C.c_int, [_VP, _VP, _I64, _I32, _VP, _PP, _VP, _VP]),
+    "aw_rollout_create": (C.c_int, [_VP, C.POINTER(FlipDesc), _VP, _I64, _I32, _I32, _PP]),
+    "aw_rollout_destroy": (C.c_int, [_VP]),
+    "aw_rollout_forward": (C.c_int, [_VP, _VP, _VP, _I32, C.POINTER(_D), _VP]),
+    "aw_rollout_final_positions": (C.c_int, [_VP, _VP, _VP]),
+    "aw_vjp_rollout": (C.c_int, [_VP, _VP, _VP]),
 }
 
 _lib = None
@@ -345,6 +357,41 @@ class MSBG:
         check(lib().aw_pressure_gradient(self.h, solver.h, _ptr(p), int(p.dtype == torch.float64), _ptr(fluid),
                                          float(dt), _stream(stream)))
 
+    # projection and adjoints -----------------------------------------------------------------
+    def face_arrays(self, dtype=None):
+        """three zeroed torch arrays shaped like the VELOCITY_* channels"""
+        import torch
+        t = self.totals()
+        return [torch.zeros(int(t[1 + a]), dtype=dtype or torch.float32, device="cuda") for a in range(3)]
+
+    def project(self, solver, fluid, dt, stream=None):
+        check(lib().aw_project(self.h, solver.h, _ptr(fluid), float(dt), _stream(stream)))
+
+    def vjp_project(self, solver, fluid, dt, u_bar, stream=None):
+        ub = (C.c_void_p * 3)(*[_ptr(x) for x in u_bar])
+        check(lib().aw_vjp_project(self.h, solver.h, _ptr(fluid), float(dt), ub, _stream(stream)))
+
+    def vjp_p2g(self, pos, vel, u_bar, pos_bar, vel_bar, stream=None):
+        ub = (C.c_void_p * 3)(*[_ptr(x) for x in u_bar])
+        check(lib().aw_vjp_p2g(self.h, _ptr(pos), _ptr(vel), int(pos.shape[0]), ub, _ptr(pos_bar), _ptr(vel_bar),
+                               _stream(stream)))
+
+    def vjp_g2p(self, pos, alpha, vel_bar, pos_bar, un_bar, uo_bar, stream=None):
+        a = (C.c_void_p * 3)(*[_ptr(x) for x in un_bar])
+        b = (C.c_void_p * 3)(*[_ptr(x) for x in uo_bar])
+        check(lib().aw_vjp_g2p(self.h, _ptr(pos), int(pos.shape[0]), float(alpha), _ptr(vel_bar), _ptr(pos_bar), a, b,
+                               _stream(stream)))
+
+    def vjp_advect(self, pos, dt, pos_bar, u_bar, stream=None):
+        ub = (C.c_void_p * 3)(*[_ptr(x) for x in u_bar])
+        check(lib().aw_vjp_advect(self.h, _ptr(pos), int(pos.shape[0]), float(dt), _ptr(pos_bar), ub,
+                                  _stream(stream)))
+
+    def vjp_sample(self, pts, out_bar, u_bar, pts_bar=None, old=False, stream=None):
+        ub = (C.c_void_p * 3)(*[_ptr(x) for x in u_bar])
+        check(lib().aw_vjp_sample(self.h, _ptr(pts), int(pts.shape[0]), int(bool(old)), _ptr(out_bar), ub,
+                                  _ptr(pts_bar), _stream(stream)))
+
     def sort_particles(self, pos, stream=None):
         import torch
         n = int(pos.shape[0])
@@ -471,6 +518,59 @@ class Flip:
         vel = np.zeros((self.n, 3), np.float32)
         check(lib().aw_flip_particles(self.h, pos.ctypes.data, vel.ctypes.data))
         return pos, vel
+
+
+class Rollout:
+    """Differentiable FLIP rollout with checkpointing (aw_rollout_* / aw_vjp_rollout).
+
+    Particles start at `pos0` with velocities sampled from a MAC face field u0; loss = mean over
+    particles of |x_final - target|^2.  u0 and its gradient are flat float32 CUDA tensors holding
+    the three face arrays of the grid one after the other."""
+
+    def __init__(self, grid: MSBG, pos0, steps, dt, alpha=0.95, gravity=(0.0, -9.81, 0.0),
+                 precision=PRECISION_MIXED, tolerance=1e-6, max_cycles=100, checkpoint_every=10):
+        import torch
+        d = FlipDesc()
+        d.dt, d.alpha = float(dt), float(alpha)
+        d.gravity[:] = [float(g) for g in gravity]
+        d.precision, d.tolerance, d.max_cycles = int(precision), float(tolerance), int(max_cycles)
+        p = torch.as_tensor(np.ascontiguousarray(pos0, np.float32), device="cuda")
+        self.n = int(p.shape[0])
+        self.grid = grid
+        h = C.c_void_p()
+        check(lib().aw_rollout_create(grid.h, C.byref(d), p.data_ptr(), self.n, int(steps), int(checkpoint_every),
+                                      C.byref(h)))
+        self.h = h
+        self.nfaces = sum(grid.totals()[1:])
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().aw_rollout_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def forward(self, u0, target, freeze_fluid=False, stream=None):
+        loss = C.c_double()
+        check(lib().aw_rollout_forward(self.h, _ptr(u0), _ptr(target), int(bool(freeze_fluid)), C.byref(loss),
+                                       _stream(stream)))
+        return loss.value
+
+    def final_positions(self, stream=None):
+        import torch
+        out = torch.empty((self.n, 3), dtype=torch.float32, device="cuda")
+        check(lib().aw_rollout_final_positions(self.h, out.data_ptr(), _stream(stream)))
+        return out
+
+    def vjp(self, stream=None):
+        import torch
+        g = torch.empty(self.nfaces, dtype=torch.float32, device="cuda")
+        check(lib().aw_vjp_rollout(self.h, g.data_ptr(), _stream(stream)))
+        return g
 
 
 # ------------------------------------------------------------------------------------------------

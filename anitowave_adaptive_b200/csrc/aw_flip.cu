@@ -210,6 +210,180 @@ __global__ void k_gradient(LevelView L, const PT* __restrict__ p, const uint8_t*
     }
 }
 
+// ---- adjoints of the grid-side linear maps (no counterpart in the reference) -----------------
+// k_face_sync^T: a synced coarse face hands a quarter of its adjoint to each of the 4 fine faces
+// it was averaged from and keeps none.  Each fine face belongs to one synced coarse face only.
+__global__ void k_face_sync_vjp(LevelView L, float* u0, float* u1, float* u2) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    float* U[3] = {u0, u1, u2};
+#pragma unroll
+    for (int dir = 0; dir < 6; ++dir) {
+        const int a = dir >> 1, s = (dir & 1) ? 1 : -1;
+        int nc[3] = {cb[0], cb[1], cb[2]};
+        nc[a] += s;
+        if (!inside(L.g, nc)) continue;
+        const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+        const int rn = L.res[n];
+        if (rn != 2 * r) continue;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int i = threadIdx.x; i < r * r; i += blockDim.x) {
+            const int u1 = i % r, u2 = i / r;
+            int f[3];
+            f[a] = s > 0 ? r : 0;
+            f[t1] = u1;
+            f[t2] = u2;
+            float* cf = &U[a][L.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r)];
+            const float g = 0.25f * *cf;
+            *cf = 0.f;
+            for (int d1 = 0; d1 < 2; ++d1)
+                for (int d2 = 0; d2 < 2; ++d2) {
+                    int q[3];
+                    q[a] = s > 0 ? 0 : rn;
+                    q[t1] = 2 * u1 + d1;
+                    q[t2] = 2 * u2 + d2;
+                    U[a][L.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn)] += g;
+                }
+        }
+    }
+}
+
+// k_divergence^T: ubar_f += (H^2 / dt) (bbar[low cell] - bbar[high cell]) over the fluid cells of the
+// face's block (one thread per face, no atomics)
+template <class BT>
+__global__ void k_divergence_vjp(LevelView L, const BT* __restrict__ bbar, const uint8_t* __restrict__ fluid,
+                                 float inv_dt, float* u0, float* u1, float* u2) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    const float H = L.g.bs / (float)r;
+    const double sc = (double)H * H * inv_dt;
+    float* U[3] = {u0, u1, u2};
+    const uint32_t oc = L.off[0][b];
+    const int nf = (r + 1) * r * r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int fi = threadIdx.x; fi < nf; fi += blockDim.x) {
+            int f[3];
+            if (a == 0) { f[0] = fi % (r + 1); int rem = fi / (r + 1); f[1] = rem % r; f[2] = rem / r; }
+            else if (a == 1) { f[0] = fi % r; int rem = fi / r; f[1] = rem % (r + 1); f[2] = rem / (r + 1); }
+            else { f[0] = fi % r; int rem = fi / r; f[1] = rem % r; f[2] = rem / r; }
+            double acc = 0.0;
+            if (f[a] > 0) {  // the face is the high face of the cell below
+                int c[3] = {f[0], f[1], f[2]};
+                c[a] -= 1;
+                const uint32_t ci = oc + cidx(c[0], c[1], c[2], r);
+                if (fluid[ci]) acc += (double)bbar[ci];
+            }
+            if (f[a] < r) {  // and the low face of the cell above
+                const uint32_t ci = oc + cidx(f[0], f[1], f[2], r);
+                if (fluid[ci]) acc -= (double)bbar[ci];
+            }
+            if (acc != 0.0) {
+                float* p = &U[a][L.off[1 + a][b] + (uint32_t)fi];
+                *p = (float)((double)*p + sc * acc);
+            }
+        }
+}
+
+// cells (and their weights) whose pressure forms the value across face (a, s) of cell c (the
+// dependence of ghost_p on p); returns the count, 0 for a wall or an absent neighbour
+__device__ inline int ghost_cells(const LevelView& L, const uint8_t* __restrict__ fluid, int b, const int cb[3],
+                                  const int c[3], int a, int s, uint32_t cells[4], float* w, bool* fl, bool* wall) {
+    int nc[3] = {cb[0], cb[1], cb[2]};
+    nc[a] += s;
+    *fl = false;
+    *wall = false;
+    if (!inside(L.g, nc)) {
+        *wall = true;
+        return 0;
+    }
+    const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+    const int rn = L.res[n], r = L.res[b];
+    if (!rn) return 0;
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    int q[3];
+    q[a] = s > 0 ? 0 : rn - 1;
+    if (rn <= r) {
+        const int sh = rn == r ? 0 : 1;
+        q[t1] = min(c[t1] >> sh, rn - 1);
+        q[t2] = min(c[t2] >> sh, rn - 1);
+        cells[0] = L.off[0][n] + cidx(q[0], q[1], q[2], rn);
+        *w = 1.f;
+        *fl = fluid[cells[0]] != 0;
+        return 1;
+    }
+    int k = 0;
+    for (int d1 = 0; d1 < 2; ++d1)
+        for (int d2 = 0; d2 < 2; ++d2, ++k) {
+            q[t1] = min(2 * c[t1] + d1, rn - 1);
+            q[t2] = min(2 * c[t2] + d2, rn - 1);
+            cells[k] = L.off[0][n] + cidx(q[0], q[1], q[2], rn);
+            *fl = *fl || fluid[cells[k]] != 0;
+        }
+    *w = 0.25f;
+    return 4;
+}
+
+// k_gradient^T: ubar on wall faces is cleared; pbar += -dt (W / area) ubar d(p_high - p_low)/dp on
+// faces with a fluid cell on either side (float atomics: cells receive from up to 6 faces and from
+// neighbouring blocks)
+__global__ void k_gradient_vjp(LevelView L, const uint8_t* __restrict__ fluid, const float* W0, const float* W1,
+                               const float* W2, float dt, float* u0, float* u1, float* u2, float* pbar) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const float H = L.g.bs / (float)r;
+    const double scale = (double)dt / ((double)H * H);
+    const float* Wa[3] = {W0, W1, W2};
+    float* U[3] = {u0, u1, u2};
+    const int nf = (r + 1) * r * r;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        for (int fi = threadIdx.x; fi < nf; fi += blockDim.x) {
+            int f[3];
+            if (a == 0) { f[0] = fi % (r + 1); int rem = fi / (r + 1); f[1] = rem % r; f[2] = rem / r; }
+            else if (a == 1) { f[0] = fi % r; int rem = fi / r; f[1] = rem % (r + 1); f[2] = rem / (r + 1); }
+            else { f[0] = fi % r; int rem = fi / r; f[1] = rem % r; f[2] = rem / r; }
+            uint32_t cells[2][4];
+            float cw[2] = {1.f, 1.f};
+            int nc[2] = {0, 0};
+            bool fl[2] = {false, false};
+            bool wall = false;
+            for (int side = 0; side < 2; ++side) {
+                int c[3] = {f[0], f[1], f[2]};
+                if (side == 0) c[a] -= 1;
+                if (c[a] >= 0 && c[a] < r) {
+                    cells[side][0] = L.off[0][b] + cidx(c[0], c[1], c[2], r);
+                    nc[side] = 1;
+                    fl[side] = fluid[cells[side][0]] != 0;
+                } else {
+                    int cin[3] = {f[0], f[1], f[2]};
+                    cin[a] = side == 0 ? 0 : r - 1;
+                    bool wl;
+                    nc[side] = ghost_cells(L, fluid, b, cb, cin, a, side == 0 ? -1 : 1, cells[side], &cw[side],
+                                           &fl[side], &wl);
+                    wall = wall || wl;
+                }
+            }
+            const uint32_t oi = L.off[1 + a][b] + (uint32_t)fi;
+            if (wall) {
+                U[a][oi] = 0.f;
+                continue;
+            }
+            if (!fl[0] && !fl[1]) continue;
+            const float coef = (float)(-scale * (double)Wa[a][oi] * (double)U[a][oi]);
+            if (coef == 0.f) continue;
+            for (int k = 0; k < nc[1]; ++k) atomicAdd(&pbar[cells[1][k]], coef * cw[1]);
+            for (int k = 0; k < nc[0]; ++k) atomicAdd(&pbar[cells[0][k]], -coef * cw[0]);
+        }
+}
+
 template <class PT>
 __global__ void k_mask_air(PT* p, const uint8_t* fluid, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -246,6 +420,219 @@ aw_status wall_bc(MsbgState& G, float* u[3], cudaStream_t s) {
     AW_LAUNCH();
     return AW_OK;
 }
+aw_status face_sync_vjp(MsbgState& G, float* ubar[3], cudaStream_t s) {
+    k_face_sync_vjp<<<G.nb, 64, 0, s>>>(G.view0(), ubar[0], ubar[1], ubar[2]);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+static aw_status level0_W(aw_solver* sv, float* W[3]) {
+    for (int a = 0; a < 3; ++a) {
+        void* p;
+        uint32_t cnt;
+        AW_TRY(aw_solver_level_array(sv, 0, 3 + a, &p, &cnt));
+        W[a] = (float*)p;
+    }
+    return AW_OK;
+}
+
+aw_status project_forward(MsbgState& G, aw_solver* sv, const uint8_t* fluid, float dt, int precision, FlipBufs& B,
+                          cudaStream_t s) {
+    AW_TRY(B.ensure(G));
+    float* U[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
+    k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], fluid, 1.f / dt, B.rhs.p, nullptr);
+    AW_LAUNCH();
+    const bool mixed = precision == AW_PRECISION_MIXED;
+    void* p = mixed ? (void*)B.p64.p : (void*)B.p32.p;
+    AW_CUDA(cudaMemsetAsync(p, 0, G.tot[0] * (mixed ? sizeof(double) : sizeof(float)), s));
+    int32_t cycles;
+    double rel;
+    AW_TRY(aw_solve(sv, B.rhs.p, p, &cycles, &rel, (aw_stream)s));
+    float* W[3];
+    AW_TRY(level0_W(sv, W));
+    if (mixed)
+        k_gradient<double><<<G.nb, 128, 0, s>>>(G.view0(), B.p64.p, fluid, W[0], W[1], W[2], dt, U[0], U[1], U[2]);
+    else
+        k_gradient<float><<<G.nb, 128, 0, s>>>(G.view0(), B.p32.p, fluid, W[0], W[1], W[2], dt, U[0], U[1], U[2]);
+    AW_LAUNCH();
+    AW_TRY(face_sync(G, U, s));
+    return wall_bc(G, U, s);
+}
+
+aw_status project_vjp(MsbgState& G, aw_solver* sv, const uint8_t* fluid, float dt, int precision, float* ubar[3],
+                      FlipBufs& B, cudaStream_t s) {
+    AW_TRY(B.ensure(G));
+    // walls and the T-junction sync, transposed
+    AW_TRY(wall_bc(G, ubar, s));
+    AW_TRY(face_sync_vjp(G, ubar, s));
+    // pressure-gradient update, transposed: pbar (into B.rhs) and the wall faces of ubar
+    float* W[3];
+    AW_TRY(level0_W(sv, W));
+    AW_CUDA(cudaMemsetAsync(B.rhs.p, 0, G.tot[0] * sizeof(float), s));
+    k_gradient_vjp<<<G.nb, 128, 0, s>>>(G.view0(), fluid, W[0], W[1], W[2], dt, ubar[0], ubar[1], ubar[2], B.rhs.p);
+    AW_LAUNCH();
+    k_mask_air<float><<<nblk(G.tot[0]), 256, 0, s>>>(B.rhs.p, fluid, G.tot[0]);
+    AW_LAUNCH();
+    // the operator is symmetric: bbar = A^-1 pbar is one more solve with the same hierarchy
+    const bool mixed = precision == AW_PRECISION_MIXED;
+    void* bb = mixed ? (void*)B.p64.p : (void*)B.p32.p;
+    AW_CUDA(cudaMemsetAsync(bb, 0, G.tot[0] * (mixed ? sizeof(double) : sizeof(float)), s));
+    int32_t cycles;
+    double rel;
+    AW_TRY(aw_solve(sv, B.rhs.p, bb, &cycles, &rel, (aw_stream)s));
+    // divergence, transposed
+    if (mixed)
+        k_divergence_vjp<double><<<G.nb, 128, 0, s>>>(G.view0(), B.p64.p, fluid, 1.f / dt, ubar[0], ubar[1], ubar[2]);
+    else
+        k_divergence_vjp<float><<<G.nb, 128, 0, s>>>(G.view0(), B.p32.p, fluid, 1.f / dt, ubar[0], ubar[1], ubar[2]);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+aw_status FlipBufs::ensure(const MsbgState& G) {
+    AW_TRY(p32.ensure(std::max<uint32_t>(G.tot[0], 1)));
+    AW_TRY(p64.ensure(std::max<uint32_t>(G.tot[0], 1)));
+    AW_TRY(rhs.ensure(std::max<uint32_t>(G.tot[0], 1)));
+    AW_TRY(fluid.ensure(std::max<uint32_t>(G.tot[0], 1)));
+    AW_TRY(divmax.ensure(2));
+    return AW_OK;
+}
+
+aw_status StepRecord::ensure(const MsbgState& G, int64_t n) {
+    const size_t np = (size_t)std::max<int64_t>(n, 1);
+    AW_TRY(perm.ensure(np));
+    AW_TRY(soa.ensure(6 * np));
+    for (int a = 0; a < 3; ++a) {
+        const size_t nf = std::max<uint32_t>(G.tot[1 + a], 1);
+        AW_TRY(u1[a].ensure(nf));
+        AW_TRY(m[a].ensure(nf));
+        AW_TRY(uo[a].ensure(nf));
+        AW_TRY(u6[a].ensure(nf));
+    }
+    AW_TRY(fluid.ensure(std::max<uint32_t>(G.tot[0], 1)));
+    return AW_OK;
+}
+
+static aw_status copy_d2d(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes) AW_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, s));
+    return AW_OK;
+}
+
+aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
+                        const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
+                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s) {
+    float* U[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
+    float* UO[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
+    float* Mm[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
+    const size_t fb[3] = {G.tot[1] * sizeof(float), G.tot[2] * sizeof(float), G.tot[3] * sizeof(float)};
+    AW_TRY(B.ensure(G));
+    if (rec) AW_TRY(rec->ensure(G, n));
+    if (ev) AW_CUDA(cudaEventRecord(ev[0], s));
+    // 1. sort by (block, cell)
+    AW_TRY(sort_core_soa(G, soa_in, n, s));
+    AW_TRY(gather_soa(G, soa_in, n, soa_out, ids_in, ids_out, s));
+    if (rec) {
+        AW_TRY(copy_d2d(rec->perm.p, G.pw.sorted, (size_t)n * sizeof(uint32_t), s));
+        AW_TRY(copy_d2d(rec->soa.p, soa_out, (size_t)n * 6 * sizeof(float), s));
+    }
+    if (ev) AW_CUDA(cudaEventRecord(ev[1], s));
+    // 2. P2G (+ normalise) and fluid flags
+    float* nomom[3] = {nullptr, nullptr, nullptr};
+    AW_TRY(p2g_sorted(G, soa_out, n, G.pw.cell_start.p, U, Mm, nomom, nullptr, s));
+    if (ev) AW_CUDA(cudaEventRecord(ev[2], s));
+    k_fluid_from_count<<<nblk(G.tot[0]), 256, 0, s>>>(G.pw.cell_start.p, G.tot[0], B.fluid.p, G.ch[AW_CELL_TYPE]);
+    AW_LAUNCH();
+    if (fluid_in) AW_TRY(copy_d2d(B.fluid.p, fluid_in, G.tot[0], s));
+    if (rec) {
+        for (int a = 0; a < 3; ++a) {
+            AW_TRY(copy_d2d(rec->u1[a].p, U[a], fb[a], s));
+            AW_TRY(copy_d2d(rec->m[a].p, Mm[a], fb[a], s));
+        }
+        AW_TRY(copy_d2d(rec->fluid.p, B.fluid.p, G.tot[0], s));
+    }
+    AW_TRY(face_sync(G, U, s));
+    // 3. backup, gravity, walls
+    for (int a = 0; a < 3; ++a) AW_TRY(copy_d2d(UO[a], U[a], fb[a], s));
+    for (int a = 0; a < 3; ++a)
+        if (d.gravity[a] != 0.f && G.tot[1 + a]) {
+            k_add_const<<<nblk(G.tot[1 + a]), 256, 0, s>>>(U[a], G.tot[1 + a], d.dt * d.gravity[a]);
+            AW_LAUNCH();
+        }
+    AW_TRY(wall_bc(G, U, s));
+    // 4. divergence
+    AW_CUDA(cudaMemsetAsync(B.divmax.p, 0, 2 * sizeof(float), s));
+    k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], B.fluid.p, 1.f / d.dt, B.rhs.p, B.divmax.p);
+    AW_LAUNCH();
+    if (ev) AW_CUDA(cudaEventRecord(ev[3], s));
+    // 5. projection
+    AW_TRY(aw_solver_setup(solver, B.fluid.p, (aw_stream)s));
+    void* p;
+    if (d.precision == AW_PRECISION_MIXED) {
+        AW_CUDA(cudaMemsetAsync(B.p64.p, 0, G.tot[0] * sizeof(double), s));
+        p = B.p64.p;
+    } else {
+        AW_CUDA(cudaMemsetAsync(B.p32.p, 0, G.tot[0] * sizeof(float), s));
+        p = B.p32.p;
+    }
+    int32_t cycles = 0;
+    double rel = 0;
+    aw_status sst = aw_solve(solver, B.rhs.p, p, &cycles, &rel, (aw_stream)s);
+    if (st) {
+        st->cycles = cycles;
+        st->residual = rel;
+    }
+    if (sst != AW_OK) return sst;
+    if (ev) AW_CUDA(cudaEventRecord(ev[4], s));
+    // 6. pressure-gradient update, sync, walls
+    void* W[3];
+    uint32_t cnt;
+    for (int a = 0; a < 3; ++a) AW_TRY(aw_solver_level_array(solver, 0, 3 + a, &W[a], &cnt));
+    if (d.precision == AW_PRECISION_MIXED)
+        k_gradient<double><<<G.nb, 128, 0, s>>>(G.view0(), B.p64.p, B.fluid.p, (float*)W[0], (float*)W[1],
+                                                (float*)W[2], d.dt, U[0], U[1], U[2]);
+    else
+        k_gradient<float><<<G.nb, 128, 0, s>>>(G.view0(), B.p32.p, B.fluid.p, (float*)W[0], (float*)W[1], (float*)W[2],
+                                               d.dt, U[0], U[1], U[2]);
+    AW_LAUNCH();
+    AW_TRY(face_sync(G, U, s));
+    AW_TRY(wall_bc(G, U, s));
+    k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], B.fluid.p, 1.f / d.dt, nullptr, B.divmax.p + 1);
+    AW_LAUNCH();
+    if (rec)
+        for (int a = 0; a < 3; ++a) {
+            AW_TRY(copy_d2d(rec->u6[a].p, U[a], fb[a], s));
+            AW_TRY(copy_d2d(rec->uo[a].p, UO[a], fb[a], s));
+        }
+    if (ev) AW_CUDA(cudaEventRecord(ev[5], s));
+    // 7. G2P (FLIP blend) on the sorted SoA particles
+    const float* un[3] = {U[0], U[1], U[2]};
+    const float* uo[3] = {UO[0], UO[1], UO[2]};
+    AW_TRY(g2p_sorted(G, soa_out, n, G.pw.cell_start.p, d.alpha, un, uo, s));
+    if (ev) AW_CUDA(cudaEventRecord(ev[6], s));
+    // 8. RK3 advection through the u_new tiles built for G2P
+    AW_TRY(advect_tiles(G, soa_out, 1, n, d.dt, G.tiles_new.p, s));
+    if (ev) AW_CUDA(cudaEventRecord(ev[7], s));
+    if (st) {
+        if (ev) AW_CUDA(cudaEventSynchronize(ev[7]));
+        AW_TRY(check_device_errors(G, s));
+        float dm[2];
+        AW_CUDA(cudaMemcpyAsync(dm, B.divmax.p, sizeof dm, cudaMemcpyDeviceToHost, s));
+        AW_CUDA(cudaStreamSynchronize(s));
+        st->div_before = dm[0];
+        st->div_after = dm[1];
+        if (ev) {
+            float t[7];
+            for (int k = 0; k < 7; ++k) AW_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+            st->ms_sort = t[0];
+            st->ms_p2g = t[1];
+            st->ms_other = t[2] + t[4];
+            st->ms_solve = t[3];
+            st->ms_g2p = t[5];
+            st->ms_advect = t[6];
+        }
+    }
+    return AW_OK;
+}
 
 }  // namespace aw
 
@@ -259,9 +646,7 @@ struct aw_flip {
     DBuf<uint32_t> ids[2];
     int cur = 0;
     aw_solver* solver = nullptr;
-    DBuf<float> p32, rhs, divmax;
-    DBuf<double> p64;
-    DBuf<uint8_t> fluid;
+    FlipBufs B;
     aw_flip_stats stats{};
     cudaEvent_t ev[8] = {};
     ~aw_flip() {
@@ -305,11 +690,7 @@ extern "C" aw_status aw_flip_create(aw_msbg* g, const aw_flip_desc* d, const flo
     sd.tolerance = d->tolerance;
     sd.max_cycles = d->max_cycles;
     AW_TRY(aw_solver_create(g, &sd, &F->solver));
-    AW_TRY(F->p32.alloc(G.tot[0]));
-    AW_TRY(F->p64.alloc(G.tot[0]));
-    AW_TRY(F->rhs.alloc(G.tot[0]));
-    AW_TRY(F->fluid.alloc(G.tot[0]));
-    AW_TRY(F->divmax.alloc(2));
+    AW_TRY(F->B.ensure(G));
     for (auto& e : F->ev) AW_CUDA(cudaEventCreate(&e));
     *out = F.release();
     return AW_OK;
@@ -329,97 +710,11 @@ extern "C" aw_status aw_flip_solver(aw_flip* f, aw_solver** out) {
 extern "C" aw_status aw_flip_step(aw_flip* F, aw_stream s_) {
     AW_CHECK_ARG(F, "null simulation");
     cudaStream_t s = (cudaStream_t)s_;
-    MsbgState& G = F->g->st;
-    const int64_t n = F->n;
-    float* U[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
-    float* UO[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
-    float* Mm[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
-    float* Mo[3] = {G.ch[AW_MOMENTUM_X], G.ch[AW_MOMENTUM_Y], G.ch[AW_MOMENTUM_Z]};
-    AW_CUDA(cudaEventRecord(F->ev[0], s));
-    // 1. sort by (block, cell)
-    AW_TRY(sort_core_soa(G, F->soa[F->cur].p, n, s));
-    AW_TRY(gather_soa(G, F->soa[F->cur].p, n, F->soa[F->cur ^ 1].p, F->ids[F->cur].p, F->ids[F->cur ^ 1].p, s));
-    F->cur ^= 1;
-    float* soa = F->soa[F->cur].p;
-    AW_CUDA(cudaEventRecord(F->ev[1], s));
-    // 2. P2G (+ normalise) and fluid flags
-    float* nomom[3] = {nullptr, nullptr, nullptr};
-    (void)Mo;
-    AW_TRY(p2g_sorted(G, soa, n, G.pw.cell_start.p, U, Mm, nomom, nullptr, s));
-    AW_CUDA(cudaEventRecord(F->ev[2], s));
-    k_fluid_from_count<<<nblk(G.tot[0]), 256, 0, s>>>(G.pw.cell_start.p, G.tot[0], F->fluid.p, G.ch[AW_CELL_TYPE]);
-    AW_LAUNCH();
-    AW_TRY(face_sync(G, U, s));
-    // 3. backup, gravity, walls
-    for (int a = 0; a < 3; ++a)
-        AW_CUDA(cudaMemcpyAsync(UO[a], U[a], G.tot[1 + a] * sizeof(float), cudaMemcpyDeviceToDevice, s));
-    for (int a = 0; a < 3; ++a)
-        if (F->d.gravity[a] != 0.f) {
-            k_add_const<<<nblk(G.tot[1 + a]), 256, 0, s>>>(U[a], G.tot[1 + a], F->d.dt * F->d.gravity[a]);
-            AW_LAUNCH();
-        }
-    AW_TRY(wall_bc(G, U, s));
-    // 4. divergence
-    AW_CUDA(cudaMemsetAsync(F->divmax.p, 0, 2 * sizeof(float), s));
-    k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], F->fluid.p, 1.f / F->d.dt, F->rhs.p, F->divmax.p);
-    AW_LAUNCH();
-    AW_CUDA(cudaEventRecord(F->ev[3], s));
-    // 5. projection
-    AW_TRY(aw_solver_setup(F->solver, F->fluid.p, s_));
-    void* p;
-    if (F->d.precision == AW_PRECISION_MIXED) {
-        AW_CUDA(cudaMemsetAsync(F->p64.p, 0, G.tot[0] * sizeof(double), s));
-        p = F->p64.p;
-    } else {
-        AW_CUDA(cudaMemsetAsync(F->p32.p, 0, G.tot[0] * sizeof(float), s));
-        p = F->p32.p;
-    }
-    int32_t cycles = 0;
-    double rel = 0;
-    aw_status st = aw_solve(F->solver, F->rhs.p, p, &cycles, &rel, s_);
-    F->stats.cycles = cycles;
-    F->stats.residual = rel;
-    if (st != AW_OK) return st;
-    AW_CUDA(cudaEventRecord(F->ev[4], s));
-    // 6. pressure-gradient update, sync, walls
-    void* W[3];
-    uint32_t cnt;
-    for (int a = 0; a < 3; ++a) AW_TRY(aw_solver_level_array(F->solver, 0, 3 + a, &W[a], &cnt));
-    if (F->d.precision == AW_PRECISION_MIXED)
-        k_gradient<double><<<G.nb, 128, 0, s>>>(G.view0(), F->p64.p, F->fluid.p, (float*)W[0], (float*)W[1],
-                                                (float*)W[2], F->d.dt, U[0], U[1], U[2]);
-    else
-        k_gradient<float><<<G.nb, 128, 0, s>>>(G.view0(), F->p32.p, F->fluid.p, (float*)W[0], (float*)W[1], (float*)W[2],
-                                               F->d.dt, U[0], U[1], U[2]);
-    AW_LAUNCH();
-    AW_TRY(face_sync(G, U, s));
-    AW_TRY(wall_bc(G, U, s));
-    k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], F->fluid.p, 1.f / F->d.dt, nullptr, F->divmax.p + 1);
-    AW_LAUNCH();
-    AW_CUDA(cudaEventRecord(F->ev[5], s));
-    // 7. G2P (FLIP blend) on the sorted SoA particles
-    const float* un[3] = {U[0], U[1], U[2]};
-    const float* uo[3] = {UO[0], UO[1], UO[2]};
-    AW_TRY(g2p_sorted(G, soa, n, G.pw.cell_start.p, F->d.alpha, un, uo, s));
-    AW_CUDA(cudaEventRecord(F->ev[6], s));
-    // 8. RK3 advection through the u_new tiles built for G2P
-    AW_TRY(advect_tiles(G, soa, 1, n, F->d.dt, G.tiles_new.p, s));
-    AW_CUDA(cudaEventRecord(F->ev[7], s));
-    AW_CUDA(cudaEventSynchronize(F->ev[7]));
-    AW_TRY(check_device_errors(G, s));
-    float dm[2];
-    AW_CUDA(cudaMemcpy(dm, F->divmax.p, sizeof dm, cudaMemcpyDeviceToHost));
-    F->stats.div_before = dm[0];
-    F->stats.div_after = dm[1];
-    float t[7];
-    for (int k = 0; k < 7; ++k) AW_CUDA(cudaEventElapsedTime(&t[k], F->ev[k], F->ev[k + 1]));
-    F->stats.ms_sort = t[0];
-    F->stats.ms_p2g = t[1];
-    F->stats.ms_other = t[2] + t[4];
-    F->stats.ms_solve = t[3];
-    F->stats.ms_g2p = t[5];
-    F->stats.ms_advect = t[6];
-    return AW_OK;
+    const int c = F->cur;
+    aw_status st = flip_step_soa(F->g->st, F->solver, F->d, F->B, F->soa[c].p, F->ids[c].p, F->soa[c ^ 1].p,
+                                 F->ids[c ^ 1].p, F->n, nullptr, nullptr, F->ev, &F->stats, s);
+    F->cur ^= 1;  // the sorted state lives in the other buffer from the gather on
+    return st;
 }
 
 extern "C" aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out) {

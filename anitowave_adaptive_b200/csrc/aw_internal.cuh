@@ -179,6 +179,16 @@ struct ParticleWork {
     aw_status ensure(int64_t np, uint32_t ncell);
 };
 
+struct MsbgState;
+// Work buffers of one FLIP step / projection: pressure (FP32 or FP64), right-hand side, fluid
+// flags, max |div u| before and after.
+struct FlipBufs {
+    DBuf<float> p32, rhs, divmax;
+    DBuf<double> p64;
+    DBuf<uint8_t> fluid;
+    aw_status ensure(const MsbgState& G);
+};
+
 struct MsbgState {
     aw_grid_desc desc;
     Geo geo;
@@ -200,6 +210,9 @@ struct MsbgState {
     std::vector<uint32_t> h_tile_off;
     uint32_t tile_tot = 0;
     DBuf<float> tiles_new, tiles_old;
+    DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
+    DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
+    FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
     DBuf<int> err;  // device error flags: [0] P2G row overflow, [1] TMA wait timeout
     DBuf<uint8_t> occ;
     DBuf<int> flag;
@@ -238,6 +251,58 @@ aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t
                          float* tn, float* to, cudaStream_t s);
 // total tile floats of a grid whose blocks have resolutions h_res (one velocity field)
 uint64_t tile_total(const std::vector<int>& h_res);
+aw_status build_tiles2(MsbgState& G, const float* un[3], const float* uo[3], cudaStream_t s);
+
+// Adjoint of the particle side (aw_particles.cu).  Particle arrays are AoS (soa = 0) or SoA over n.
+aw_status ensure_adjoint_tiles(MsbgState& G);
+aw_status tile_fold(MsbgState& G, const float* tb, float* ubar[3], cudaStream_t s);
+// RK3 (when do_advect) and the FLIP blend of one step: xbar/vbar in -> out; unbar/uobar += (uobar may be null)
+aw_status step_particles_vjp(MsbgState& G, const float* pos, int pos_soa, int64_t n, float alpha, float dt,
+                             const float* un[3], const float* uo[3], float* xbar, float* vbar, int bar_soa,
+                             int do_advect, float* unbar[3], float* uobar[3], cudaStream_t s);
+// y = sample(u, pts): ubar += I^T ybar; xbar += (dI/dx)^T ybar when xbar is given
+aw_status sample_vjp(MsbgState& G, const float* pts, int pts_soa, int64_t n, const float* u[3], const float* ybar,
+                     int ybar_soa, float* ubar[3], float* xbar, cudaStream_t s);
+// P2G + normalisation: xbar, vbar += given ubar and the forward u, m
+aw_status p2g_vjp(MsbgState& G, const float* pos, const float* vel, int soa, int64_t n, const float* u[3],
+                  const float* m[3], const float* ubar[3], float* xbar, float* vbar, cudaStream_t s);
+aw_status unsort6(const uint32_t* perm, int64_t n, const float* in, float* out, cudaStream_t s);
+// MAC sample of u at SoA points into SoA out
+aw_status sample_soa(MsbgState& G, const float* pts_soa, int64_t n, const float* u[3], float* out_soa, cudaStream_t s);
+// Grid side (aw_flip.cu).  project_forward: VELOCITY_* <- Wall(Sync(Grad(u, A^-1 Div u))) with the
+// solver set up for `fluid`; project_vjp: ubar (in place) from the adjoint of the projected
+// velocity to the adjoint of its input, one more solve with the same operator.
+aw_status face_sync(MsbgState& G, float* u[3], cudaStream_t s);
+aw_status wall_bc(MsbgState& G, float* u[3], cudaStream_t s);
+aw_status face_sync_vjp(MsbgState& G, float* ubar[3], cudaStream_t s);
+aw_status project_forward(MsbgState& G, aw_solver* sv, const uint8_t* fluid, float dt, int precision, FlipBufs& B,
+                          cudaStream_t s);
+aw_status project_vjp(MsbgState& G, aw_solver* sv, const uint8_t* fluid, float dt, int precision, float* ubar[3],
+                      FlipBufs& B, cudaStream_t s);
+
+// ------------------------------------------------------------------------------------------------
+// FLIP step on SoA particle state (aw_flip.cu), shared by aw_flip_step and the differentiable
+// rollout (aw_adjoint.cu).
+// ------------------------------------------------------------------------------------------------
+
+// What the adjoint of one step needs, all in the step's sorted particle order.
+struct StepRecord {
+    DBuf<uint32_t> perm;  // sorted slot -> slot of the step's input state
+    DBuf<float> soa;      // x, v at the start of the step (6 n, SoA)
+    DBuf<float> u1[3];    // P2G velocity before the T-junction sync
+    DBuf<float> m[3];     // P2G mass
+    DBuf<float> uo[3];    // backup velocity (G2P's u_old)
+    DBuf<float> u6[3];    // projected velocity (G2P's u_new, the advection field)
+    DBuf<uint8_t> fluid;  // fluid flags of the projection
+    aw_status ensure(const MsbgState& G, int64_t n);
+};
+
+// soa_in/ids_in: state in any order; soa_out/ids_out: the stepped state, sorted by cell.
+// fluid_in (optional) replaces the fluid flags derived from the particle counts.  ev (optional,
+// 8 events) and st (optional) receive phase timings and solver statistics; st syncs the stream.
+aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
+                        const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
+                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s);
 
 }  // namespace aw
 

@@ -970,6 +970,354 @@ aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t
     return AW_OK;
 }
 
+// ================================================================================================
+// Adjoint (vector-Jacobian products) of P2G, G2P, RK3 advection and MAC sampling.  No counterpart
+// in the reference.  The forward map is differentiated with its discrete decisions held: the cell
+// and block of every particle and sample point, each kernel's support, the clamp branches.
+// ================================================================================================
+
+// Trilinear tile sample of component a at X (tile_interp) with its adjoint: adds gbar * dI/dX to
+// dX and, when tb is given, gbar * weight into the adjoint tile tb (same layout as t).
+__device__ inline void tile_interp_vjp(const float* __restrict__ t, float* tb, int a, int r, const float o[3], float h,
+                                       const float X[3], float gbar, float dX[3]) {
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    float sA = (X[a] - o[a]) / h;
+    float s1 = (X[t1] - o[t1]) / h - 0.5f;
+    float s2 = (X[t2] - o[t2]) / h - 0.5f;
+    const float rf = (float)r, invh = 1.f / h;
+    const float gA = (sA > 0.f && sA < rf) ? invh : 0.f;
+    const float g1 = (s1 > -1.f && s1 < rf) ? invh : 0.f;
+    const float g2 = (s2 > -1.f && s2 < rf) ? invh : 0.f;
+    sA = fminf(fmaxf(sA, 0.f), rf);
+    s1 = fminf(fmaxf(s1, -1.f), rf);
+    s2 = fminf(fmaxf(s2, -1.f), rf);
+    const int iA = min(max((int)floorf(sA), 0), r - 1);
+    const int i1 = min(max((int)floorf(s1), -1), r - 1);
+    const int i2 = min(max((int)floorf(s2), -1), r - 1);
+    const float fA = sA - (float)iA, f1 = s1 - (float)i1, f2 = s2 - (float)i2;
+    const int R1 = r + 1, R2 = r + 2;
+    const int base = a * (int)tile_axis(r) + iA + R1 * ((i1 + 1) + R2 * (i2 + 1));
+    const int s_1 = R1, s_2 = R1 * R2;
+    const float* p = t + base;
+    const float p000 = p[0], p100 = p[1], p010 = p[s_1], p110 = p[s_1 + 1];
+    const float p001 = p[s_2], p101 = p[s_2 + 1], p011 = p[s_1 + s_2], p111 = p[s_1 + s_2 + 1];
+    const float dfA = (1.f - f1) * (1.f - f2) * (p100 - p000) + f1 * (1.f - f2) * (p110 - p010) +
+                      (1.f - f1) * f2 * (p101 - p001) + f1 * f2 * (p111 - p011);
+    const float df1 = (1.f - f2) * ((1.f - fA) * (p010 - p000) + fA * (p110 - p100)) +
+                      f2 * ((1.f - fA) * (p011 - p001) + fA * (p111 - p101));
+    const float df2 = (1.f - f1) * ((1.f - fA) * (p001 - p000) + fA * (p101 - p100)) +
+                      f1 * ((1.f - fA) * (p011 - p010) + fA * (p111 - p110));
+    dX[a] += gbar * dfA * gA;
+    dX[t1] += gbar * df1 * g1;
+    dX[t2] += gbar * df2 * g2;
+    if (tb && gbar != 0.f) {
+        float* q = tb + base;
+        const float wA[2] = {1.f - fA, fA}, w1[2] = {1.f - f1, f1}, w2[2] = {1.f - f2, f2};
+#pragma unroll
+        for (int k2 = 0; k2 < 2; ++k2)
+#pragma unroll
+            for (int k1 = 0; k1 < 2; ++k1)
+#pragma unroll
+                for (int kA = 0; kA < 2; ++kA) atomicAdd(q + kA + k1 * s_1 + k2 * s_2, gbar * wA[kA] * w1[k1] * w2[k2]);
+    }
+}
+
+// sample_tiles with its adjoint (the block of X is found as in the forward)
+__device__ inline void sample_tiles_vjp(const LevelView& L, const uint32_t* __restrict__ toff,
+                                        const float* __restrict__ tiles, float* tb, int a, const float X[3], float gbar,
+                                        float dX[3]) {
+    int cb[3];
+    point_block(L.g, X, cb);
+    const int b = bidx(L.g, cb[0], cb[1], cb[2]);
+    const int r = L.res[b];
+    if (!r) return;
+    const float h = fcell(L.g, r);
+    float o[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) o[k] = forigin(L.g, k, cb[k]);
+    tile_interp_vjp(tiles + toff[b], tb ? tb + toff[b] : nullptr, a, r, o, h, X, gbar, dX);
+}
+
+// Adjoint of one step's particle update: RK3 advection x' = RK3(x; u6) and the FLIP blend
+// v' = alpha v + I(u6, x) - alpha I(uo, x).  xbar/vbar hold the adjoints of x', v' on entry and of
+// x, v on exit; the adjoints of the u6 and uo tiles are accumulated into tnb / tob.
+__global__ void k_step_particles_vjp(LevelView L, PArr pos, int64_t n, float alpha, float dt,
+                                     const uint32_t* __restrict__ toff, const float* __restrict__ tn,
+                                     const float* __restrict__ to, float* tnb, float* tob, PArrW xbar, PArrW vbar,
+                                     int do_advect, int do_g2p) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Geo& g = L.g;
+    const float x[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
+    float gx[3] = {0.f, 0.f, 0.f};
+    if (do_advect) {
+        const float h0 = g.bs / (float)g.R0;
+        float k1[3], k2[3], k3[3], y1[3], y2[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k1[a] = sample_tiles(L, toff, tn, a, x);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) y1[a] = x[a] + 0.5f * dt * k1[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k2[a] = sample_tiles(L, toff, tn, a, y1);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) y2[a] = x[a] + 0.75f * dt * k2[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k3[a] = sample_tiles(L, toff, tn, a, y2);
+        float k1b[3], k2b[3], k3b[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float v = (2.f / 9.f) * k1[a] + (3.f / 9.f) * k2[a] + (4.f / 9.f) * k3[a];
+            const float lo = g.dmin[a] + 0.01f * h0;
+            const float hi = g.dmin[a] + (float)g.D[a] * g.bs - 0.01f * h0;
+            const float y = x[a] + dt * v;
+            const float gb = (y > lo && y < hi) ? xbar(i, a) : 0.f;
+            gx[a] = gb;
+            k1b[a] = (2.f / 9.f) * dt * gb;
+            k2b[a] = (3.f / 9.f) * dt * gb;
+            k3b[a] = (4.f / 9.f) * dt * gb;
+        }
+        float y2b[3] = {0.f, 0.f, 0.f}, y1b[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sample_tiles_vjp(L, toff, tn, tnb, a, y2, k3b[a], y2b);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            gx[a] += y2b[a];
+            k2b[a] += 0.75f * dt * y2b[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sample_tiles_vjp(L, toff, tn, tnb, a, y1, k2b[a], y1b);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            gx[a] += y1b[a];
+            k1b[a] += 0.5f * dt * y1b[a];
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) sample_tiles_vjp(L, toff, tn, tnb, a, x, k1b[a], gx);
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) gx[a] = xbar(i, a);
+    }
+    // FLIP blend
+    if (do_g2p)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float gv = vbar(i, a);
+            sample_tiles_vjp(L, toff, tn, tnb, a, x, gv, gx);
+            sample_tiles_vjp(L, toff, to, tob, a, x, -alpha * gv, gx);
+            vbar(i, a) = alpha * gv;
+        }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) xbar(i, a) = gx[a];
+}
+
+// Adjoint of y = sample(u, x): adds ybar * weights into the adjoint tile tb and, when xbar is
+// given, ybar * dI/dx into xbar.
+__global__ void k_sample_vjp(LevelView L, PArr pts, int64_t n, const uint32_t* __restrict__ toff,
+                             const float* __restrict__ tiles, PArr ybar, float* tb, PArrW xbar, int with_x) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x[3] = {pts(i, 0), pts(i, 1), pts(i, 2)};
+    float gx[3] = {0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) sample_tiles_vjp(L, toff, tiles, tb, a, x, ybar(i, a), gx);
+    if (with_x)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) xbar(i, a) += gx[a];
+}
+
+// Adjoint tile -> face adjoints: every tile entry adds into the face that supplied it.
+__global__ void k_tile_fold(LevelView L, const uint32_t* __restrict__ toff, const float* __restrict__ tb, float* u0,
+                            float* u1, float* u2) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const int R1 = r + 1, R2 = r + 2;
+    const int TA = (int)tile_axis(r);
+    const float* in = tb + toff[b];
+    float* U[3] = {u0, u1, u2};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            const float v = in[a * TA + rem];
+            if (v == 0.f) continue;
+            int fi[3];
+            fi[a] = rem % R1;
+            fi[t1] = (rem / R1) % R2 - 1;
+            fi[t2] = rem / (R1 * R2) - 1;
+            atomicAdd(&U[a][face_source(L, a, b, cb, r, fi)], v);
+        }
+    }
+}
+
+// Adjoint of P2G with the normalisation u = P / m (m > 1e-6): each particle gathers, from every
+// face within one cell size (of the face's block) of it, in its own and the 26 neighbouring
+// blocks, P_bar = u_bar / m and m_bar = -u_bar u / m, and accumulates
+//   vbar_a += w P_bar,   xbar += dw/dx (P_bar v_a + m_bar),   w = (1 - d^2/h^2)^3.
+__global__ void k_p2g_vjp(LevelView L, PArr pos, PArr vel, int64_t n, Field3 u, Field3 m, Field3 ub, PArrW xbar,
+                          PArrW vbar) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Geo& g = L.g;
+    const float X[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
+    const float V[3] = {vel(i, 0), vel(i, 1), vel(i, 2)};
+    int pc[3];
+    point_block(g, X, pc);
+    float xb[3] = {0.f, 0.f, 0.f}, vb[3] = {0.f, 0.f, 0.f};
+    for (int d = 0; d < 27; ++d) {
+        const int nc[3] = {pc[0] + d % 3 - 1, pc[1] + (d / 3) % 3 - 1, pc[2] + d / 9 - 1};
+        if (!inside(g, nc)) continue;
+        const int b = bidx(g, nc[0], nc[1], nc[2]);
+        const int r = L.res[b];
+        if (!r) continue;
+        const float h = fcell(g, r);
+        const float invh = 1.f / h;
+        float q[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) q[k] = (X[k] - forigin(g, k, nc[k])) * invh;
+        const float rf = (float)r;
+        if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f)
+            continue;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            const int ia = (int)floorf(q[a]);
+            const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
+            const uint32_t ob = L.off[1 + a][b];
+            for (int da = 0; da < 2; ++da)
+                for (int d1 = 0; d1 < 2; ++d1)
+                    for (int d2 = 0; d2 < 2; ++d2) {
+                        int f[3];
+                        f[a] = ia + da;
+                        f[t1] = j1 + d1;
+                        f[t2] = j2 + d2;
+                        if (f[a] < 0 || f[a] > r || f[t1] < 0 || f[t1] >= r || f[t2] < 0 || f[t2] >= r) continue;
+                        float dq[3];
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) dq[k] = q[k] - ((float)f[k] + (k == a ? 0.f : 0.5f));
+                        const float d2s = dq[0] * dq[0] + dq[1] * dq[1] + dq[2] * dq[2];
+                        if (d2s >= 1.f) continue;
+                        const uint32_t fi = ob + fidx(a, f[0], f[1], f[2], r);
+                        const float mf = m.c[a][fi];
+                        if (!(mf > 1e-6f)) continue;
+                        const float gb = ub.c[a][fi];
+                        if (gb == 0.f) continue;
+                        const float Pbar = gb / mf;
+                        const float mbar = -gb * u.c[a][fi] / mf;
+                        const float t = 1.f - d2s;
+                        vb[a] += t * t * t * Pbar;
+                        const float coef = -6.f * t * t * invh * (Pbar * V[a] + mbar);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) xb[k] += coef * dq[k];
+                    }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        xbar(i, k) += xb[k];
+        vbar(i, k) += vb[k];
+    }
+}
+
+// out[perm[j]] = in[j] for the 6 SoA arrays (adjoint of the gather of the sort)
+__global__ void k_unsort6(const uint32_t* __restrict__ perm, int64_t n, const float* __restrict__ in, float* __restrict__ out) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t i = perm[j];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) out[(int64_t)k * n + i] = in[(int64_t)k * n + j];
+}
+
+aw_status ensure_adjoint_tiles(MsbgState& G) {
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(G.tiles_bar_new.ensure(std::max<uint32_t>(G.tile_tot, 4)));
+    AW_TRY(G.tiles_bar_old.ensure(std::max<uint32_t>(G.tile_tot, 4)));
+    return AW_OK;
+}
+
+aw_status tile_fold(MsbgState& G, const float* tb, float* ubar[3], cudaStream_t s) {
+    k_tile_fold<<<G.nb, 128, 0, s>>>(G.view0(), G.tile_off.p, tb, ubar[0], ubar[1], ubar[2]);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+aw_status step_particles_vjp(MsbgState& G, const float* pos, int pos_soa, int64_t n, float alpha, float dt,
+                             const float* un[3], const float* uo[3], float* xbar, float* vbar, int bar_soa,
+                             int do_advect, float* unbar[3], float* uobar[3], cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    AW_TRY(ensure_adjoint_tiles(G));
+    const int do_g2p = vbar != nullptr;
+    if (do_g2p) AW_TRY(build_tiles2(G, un, uo, s));
+    else AW_TRY(build_tiles(G, un, G.tiles_new.p, s));
+    AW_CUDA(cudaMemsetAsync(G.tiles_bar_new.p, 0, (size_t)G.tile_tot * sizeof(float), s));
+    AW_CUDA(cudaMemsetAsync(G.tiles_bar_old.p, 0, (size_t)G.tile_tot * sizeof(float), s));
+    PArr P = pos_soa ? PArr{pos, 1, n} : PArr{pos, 3, 1};
+    PArrW XB = bar_soa ? PArrW{xbar, 1, n} : PArrW{xbar, 3, 1};
+    PArrW VB = bar_soa ? PArrW{vbar, 1, n} : PArrW{vbar, 3, 1};
+    k_step_particles_vjp<<<nblk(n), 256, 0, s>>>(G.view0(), P, n, alpha, dt, G.tile_off.p, G.tiles_new.p, G.tiles_old.p,
+                                                 G.tiles_bar_new.p, G.tiles_bar_old.p, XB, VB, do_advect, do_g2p);
+    AW_LAUNCH();
+    AW_TRY(tile_fold(G, G.tiles_bar_new.p, unbar, s));
+    if (uobar && do_g2p) AW_TRY(tile_fold(G, G.tiles_bar_old.p, uobar, s));
+    return AW_OK;
+}
+
+__global__ void k_sample_tiles_w(LevelView L, PArr pts, int64_t n, const uint32_t* __restrict__ toff,
+                                 const float* __restrict__ tiles, PArrW out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float X[3] = {pts(i, 0), pts(i, 1), pts(i, 2)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out(i, a) = sample_tiles(L, toff, tiles, a, X);
+}
+
+aw_status sample_soa(MsbgState& G, const float* pts_soa, int64_t n, const float* u[3], float* out_soa, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, u, G.tiles_new.p, s));
+    k_sample_tiles_w<<<nblk(n), 256, 0, s>>>(G.view0(), PArr{pts_soa, 1, n}, n, G.tile_off.p, G.tiles_new.p,
+                                             PArrW{out_soa, 1, n});
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+aw_status sample_vjp(MsbgState& G, const float* pts, int pts_soa, int64_t n, const float* u[3], const float* ybar,
+                     int ybar_soa, float* ubar[3], float* xbar, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    AW_TRY(ensure_adjoint_tiles(G));
+    AW_TRY(build_tiles(G, u, G.tiles_new.p, s));
+    AW_CUDA(cudaMemsetAsync(G.tiles_bar_new.p, 0, (size_t)G.tile_tot * sizeof(float), s));
+    PArr P = pts_soa ? PArr{pts, 1, n} : PArr{pts, 3, 1};
+    PArr Y = ybar_soa ? PArr{ybar, 1, n} : PArr{ybar, 3, 1};
+    PArrW XB = pts_soa ? PArrW{xbar, 1, n} : PArrW{xbar, 3, 1};
+    k_sample_vjp<<<nblk(n), 256, 0, s>>>(G.view0(), P, n, G.tile_off.p, G.tiles_new.p, Y, G.tiles_bar_new.p, XB,
+                                         xbar ? 1 : 0);
+    AW_LAUNCH();
+    return tile_fold(G, G.tiles_bar_new.p, ubar, s);
+}
+
+aw_status p2g_vjp(MsbgState& G, const float* pos, const float* vel, int soa, int64_t n, const float* u[3],
+                  const float* m[3], const float* ubar[3], float* xbar, float* vbar, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    PArr P = soa ? PArr{pos, 1, n} : PArr{pos, 3, 1};
+    PArr V = soa ? PArr{vel, 1, n} : PArr{vel, 3, 1};
+    PArrW XB = soa ? PArrW{xbar, 1, n} : PArrW{xbar, 3, 1};
+    PArrW VB = soa ? PArrW{vbar, 1, n} : PArrW{vbar, 3, 1};
+    Field3 fu{{u[0], u[1], u[2]}}, fm{{m[0], m[1], m[2]}}, fb{{ubar[0], ubar[1], ubar[2]}};
+    k_p2g_vjp<<<nblk(n, 128), 128, 0, s>>>(G.view0(), P, V, n, fu, fm, fb, XB, VB);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+aw_status unsort6(const uint32_t* perm, int64_t n, const float* in, float* out, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    k_unsort6<<<nblk(n), 256, 0, s>>>(perm, n, in, out);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 }  // namespace aw
 
 using namespace aw;

@@ -1684,6 +1684,12 @@ extern "C" aw_status aw_solver_setup(aw_solver* S, const uint8_t* d_fluid, aw_st
     return AW_OK;
 }
 
+extern "C" aw_status aw_solver_precision(const aw_solver* S, int32_t* precision) {
+    AW_CHECK_ARG(S && precision, "null argument");
+    *precision = S->d.precision;
+    return AW_OK;
+}
+
 extern "C" aw_status aw_solver_num_levels(const aw_solver* S, int32_t* n) {
     AW_CHECK_ARG(S && n, "null argument");
     *n = (int32_t)S->lv.size();

@@ -202,6 +202,8 @@ aw_status aw_solver_destroy(aw_solver* sv);
  * coarse flags, and the FP64 factorisation of the coarsest level. */
 aw_status aw_solver_setup(aw_solver* sv, const uint8_t* d_fluid, aw_stream s);
 aw_status aw_solver_num_levels(const aw_solver* sv, int32_t* n);
+/* precision of the solver (AW_PRECISION_FP32 or AW_PRECISION_MIXED) */
+aw_status aw_solver_precision(const aw_solver* sv, int32_t* precision);
 /* level arrays: which 0 = x, 1 = b, 2 = r (float), 3..5 = coefficients x/y/z (float),
  * 6 = fluid (u8), 7 = cell offsets, 8..10 = face offsets (u32; MSBG levels only) */
 aw_status aw_solver_level_array(aw_solver* sv, int32_t level, int32_t which, void** d_ptr, uint32_t* count);
@@ -256,6 +258,59 @@ aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out);
 /* copy particle state to host in the original particle order (AoS) */
 aw_status aw_flip_particles(aw_flip* f, float* h_pos, float* h_vel);
 aw_status aw_flip_solver(aw_flip* f, aw_solver** out);
+
+/* ---- projection and adjoints (no counterpart in the reference) ------------------------------
+ * The vector-Jacobian products differentiate the forward calls with their discrete decisions
+ * held fixed: the block and cell of every particle and sample point, the fluid flags, the P2G
+ * kernel supports and the clamp branches of sampling and advection.  Face-array adjoints
+ * (d_*_bar[3]) have the layout of the VELOCITY_* channels; particle adjoints are float3 AoS.
+ * "+=" marks outputs that are accumulated into, "in/out" adjoints that are replaced. */
+typedef struct aw_rollout aw_rollout;
+
+/* the projection of the FLIP step on VELOCITY_*: divergence, solve (aw_solver_setup with d_fluid
+ * first, done here), pressure-gradient update, T-junction sync, walls.  syncs (aw_solve). */
+aw_status aw_project(aw_msbg* g, aw_solver* sv, const uint8_t* d_fluid, float dt, aw_stream s);
+/* VJP of aw_project: d_u_bar (in/out) from the adjoint of the projected velocity to the adjoint of
+ * its input.  One more solve with the same operator (the finite-volume operator is symmetric).
+ * syncs. */
+aw_status aw_vjp_project(aw_msbg* g, aw_solver* sv, const uint8_t* d_fluid, float dt, float* const d_u_bar[3],
+                         aw_stream s);
+/* VJP of aw_p2g's VELOCITY_* output (P2G with u = P/m): given d_u_bar, d_pos_bar and d_vel_bar +=.
+ * Recomputes the forward mass and velocity of these particles internally (the grid's channels are
+ * not touched).  A G2P-shaped gather: one thread per particle. */
+aw_status aw_vjp_p2g(aw_msbg* g, const float* d_pos, const float* d_vel, int64_t n, const float* const d_u_bar[3],
+                     float* d_pos_bar, float* d_vel_bar, aw_stream s);
+/* VJP of aw_g2p with the current VELOCITY_* / VELOCITY_OLD_* as u_new / u_old: d_vel_bar in/out,
+ * d_pos_bar +=, d_un_bar and d_uo_bar +=.  A P2G-shaped scatter through ghosted adjoint tiles. */
+aw_status aw_vjp_g2p(aw_msbg* g, const float* d_pos, int64_t n, float alpha, float* d_vel_bar, float* d_pos_bar,
+                     float* const d_un_bar[3], float* const d_uo_bar[3], aw_stream s);
+/* VJP of aw_advect through VELOCITY_*: d_pos = positions before advection, d_pos_bar in/out,
+ * d_u_bar +=. */
+aw_status aw_vjp_advect(aw_msbg* g, const float* d_pos, int64_t n, float dt, float* d_pos_bar, float* const d_u_bar[3],
+                        aw_stream s);
+/* VJP of aw_sample_velocity: d_u_bar += I^T d_out_bar; d_points_bar (optional) += (dI/dx)^T d_out_bar */
+aw_status aw_vjp_sample(aw_msbg* g, const float* d_points, int64_t n, int32_t old, const float* d_out_bar,
+                        float* const d_u_bar[3], float* d_points_bar, aw_stream s);
+
+/* Differentiable rollout: particles start at d_pos0 (AoS, copied) with velocities sampled from a
+ * MAC face field u0, take `steps` FLIP steps of desc, and the loss is the mean over particles of
+ * |x_final - target|^2.  The particle state of every checkpoint_every-th step is kept on the
+ * device; aw_vjp_rollout recomputes each segment from its checkpoint and runs the step adjoints
+ * backwards through it. */
+aw_status aw_rollout_create(aw_msbg* g, const aw_flip_desc* desc, const float* d_pos0, int64_t n, int32_t steps,
+                            int32_t checkpoint_every, aw_rollout** out);
+aw_status aw_rollout_destroy(aw_rollout* r);
+/* d_u0: the three face arrays of u0 concatenated (x, y, z; sizes from aw_msbg_totals); d_target:
+ * AoS per particle (copied).  freeze_fluid != 0 reuses the fluid flags of the last forward run
+ * without it, so that finite differences see the same discrete decisions as the adjoint.
+ * syncs; writes *loss. */
+aw_status aw_rollout_forward(aw_rollout* r, const float* d_u0, const float* d_target, int32_t freeze_fluid,
+                             double* loss, aw_stream s);
+/* final positions of the last forward run, AoS in particle order */
+aw_status aw_rollout_final_positions(aw_rollout* r, float* d_pos, aw_stream s);
+/* d loss / d u0 (layout of d_u0) for the last forward run.  The recompute reuses the state
+ * buffers, so run aw_rollout_forward again before another aw_vjp_rollout.  syncs. */
+aw_status aw_vjp_rollout(aw_rollout* r, float* d_u0_bar, aw_stream s);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop

@@ -37,7 +37,10 @@ def main():
     dims = np.array([8, 8, 8], np.int32)
     ms = np.zeros(4, np.float32)
     t0 = time.perf_counter()
-    rc = L.ref_time_kernels(dims, 0, np.ascontiguousarray(S.pos), np.ascontiguousarray(S.vel), S.n, 5, ms)
+    # the reference grid has blockSize 1.0 (8 blocks per axis span [0, 8]); scale the unit-cube
+    # scene by 8 so that its particles cover the same cells as on this library's 128^3 grid
+    rc = L.ref_time_kernels(dims, 0, np.ascontiguousarray(8.0 * S.pos, np.float32),
+                            np.ascontiguousarray(8.0 * S.vel, np.float32), S.n, 5, ms)
     ref_wall = time.perf_counter() - t0
     out = {"grid": "8^3 blocks x 16^3 cells, 1 level (128^3)", "particles": S.n, "ref_status": rc,
            "ref_ms": {"p2g": float(ms[0]), "g2p": float(ms[1]), "advect": float(ms[2]), "vcycle_1thread": float(ms[3])},
