@@ -212,8 +212,9 @@ struct MsbgState {
     DBuf<float> tiles_new, tiles_old;
     DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
+    DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for
     FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
-    DBuf<int> err;  // device error flags: [0] P2G row overflow, [1] TMA wait timeout
+    DBuf<int> err;  // device error flags: [0] non-finite velocity in P2G, [1] TMA wait timeout
     DBuf<uint8_t> occ;
     DBuf<int> flag;
     ParticleWork pw;
@@ -240,6 +241,8 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
 aw_status build_tiles(MsbgState& G, const float* u[3], float* tiles, cudaStream_t s);
 aw_status ensure_tiles(MsbgState& G);
 aw_status advect_tiles(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* tiles, cudaStream_t s);
+// RK3 of cell-sorted SoA particles through G.tiles_new (built for G2P), one CTA per block
+aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, cudaStream_t s);
 aw_status check_device_errors(MsbgState& G, cudaStream_t s);
 aw_status sort_core_soa(MsbgState& G, const float* soa_pos, int64_t n, cudaStream_t s);
 aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_soa, const uint32_t* ids_in,

@@ -28,6 +28,11 @@ struct PArrW {
     __device__ inline float& operator()(int64_t i, int a) const { return p[i * si + a * sa]; }
 };
 
+// ghosted face tile of a block of resolution r: per axis (r+1)(r+2)^2 faces; a block's three axes
+// padded to 16 bytes
+__host__ __device__ inline uint32_t tile_axis(int r) { return (uint32_t)((r + 1) * (r + 2) * (r + 2)); }
+__host__ __device__ inline uint32_t tile_block(int r) { return r ? ((3 * tile_axis(r) + 3u) & ~3u) : 0u; }
+
 // sort key: global level-0 cell index (MSBG offsets + cell index), or `invalid` for particles in
 // inactive blocks.
 __device__ inline uint32_t particle_key(const LevelView& L, const float p[3], uint32_t invalid) {
@@ -247,161 +252,174 @@ struct FaceOut {
     float* mom[3];
 };
 
-// P2G as a block-local scatter.  One CTA per block b accumulates, in shared memory, the weights
-// w = (1 - d^2/h_b^2)^3 of every particle that can reach one of b's faces: b's own particles and
-// the boundary cell layers of its 26 neighbours (rows of cells that are contiguous in the sorted
-// particle array).  Contributions that land outside b are dropped here and accumulated by the
-// owning block's CTA instead, so every face copy is written exactly once (mass and
-// velocity = momentum / mass fused), with no global atomics.  Lanes of a warp walk particles a
-// 32nd of the range apart, so that one warp's shared-memory atomics hit different faces.
-constexpr int P2G_MAXROWS = 2048;
-
-__device__ inline void p2g_nbr_box(const LevelView& L, const int cb[3], int r, int d, int* nblk, int lo[3], int hi[3]) {
-    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-    int nc[3] = {cb[0] + dd[0], cb[1] + dd[1], cb[2] + dd[2]};
-    *nblk = -1;
-    if (!inside(L.g, nc)) return;
-    const int n = bidx(L.g, nc[0], nc[1], nc[2]);
-    const int rn = L.res[n];
-    if (!rn) return;
-    const int k = rn > r ? rn / r : 1;  // neighbour cell layers within one of b's cells
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-        if (dd[q] == 0) { lo[q] = 0; hi[q] = rn - 1; }
-        else if (dd[q] > 0) { lo[q] = 0; hi[q] = k - 1; }
-        else { lo[q] = rn - k; hi[q] = rn - 1; }
-    }
-    *nblk = n;
+__global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, float* out) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < nc) out[c] = (float)(cstart[c + 1] - cstart[c]);
 }
 
-__global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* __restrict__ soa, int64_t n,
-                                                     const uint32_t* __restrict__ cs, FaceOut out, int* err) {
-    extern __shared__ float sm[];
-    __shared__ int dcnt[27];
-    __shared__ int doff[28];
-    __shared__ uint32_t wsum[8];
+// ------------------------------------------------------------------------------------------------
+// P2G, one pass per particle.  One CTA per block b takes only b's own particles (one contiguous
+// range of the cell-sorted array).  Every face within reach of such a particle lies in b's ghosted
+// face tile (faces [0,r] along the axis, [-1,r] across it), so the 2x2x2 candidates per axis need
+// no index checks: the weight is max(0, 1 - d^2/h^2)^3 and the shared-memory atomics of zero
+// weights are predicated off.
+//
+// The tile accumulates in 32-bit fixed point (shared-memory integer atomics are native and about
+// twice the rate of float ones on this part).  The scales are per CTA and safe by construction: a
+// face's support spans 2 x 3 x 3 cells, so its mass from b's particles is at most 18 x (the most
+// particles in one of b's cells), and |momentum| at most that bound x (b's largest |v|); both map
+// to 2^30.  The rounding error is below 1e-7 of those bounds per particle.
+//
+// The flush adds every nonzero tile entry, back in float, into each copy of that physical face held
+// by a block of b's resolution (a face on a block boundary has one copy per side).  Faces of
+// neighbours at another resolution are at other positions: particles within reach of such a
+// neighbour add their weights in the neighbour's own lattice with global float atomics.  A second
+// kernel normalises u = P / m.  The face arrays must start at zero.
+// ------------------------------------------------------------------------------------------------
+__device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
+
+// weights of one particle on the faces of block nb (resolution rn != r), global atomics
+__device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int nc[3], int rn, const float X[3], const float V[3],
+                                 float* const m_out[3], float* const P_out[3]) {
+    const Geo& g = L.g;
+    const float invh = 1.f / fcell(g, rn);
+    float q[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) q[k] = (X[k] - forigin(g, k, nc[k])) * invh;
+    const float rf = (float)rn;
+    if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f) return;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        const int ia = (int)floorf(q[a]);
+        const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
+        const uint32_t ob = L.off[1 + a][nb];
+        for (int da = 0; da < 2; ++da)
+            for (int d1 = 0; d1 < 2; ++d1)
+                for (int d2 = 0; d2 < 2; ++d2) {
+                    int f[3];
+                    f[a] = ia + da;
+                    f[t1] = j1 + d1;
+                    f[t2] = j2 + d2;
+                    if (f[a] < 0 || f[a] > rn || f[t1] < 0 || f[t1] >= rn || f[t2] < 0 || f[t2] >= rn) continue;
+                    const float dA = q[a] - (float)f[a];
+                    const float dB = q[t1] - ((float)f[t1] + 0.5f);
+                    const float dC = q[t2] - ((float)f[t2] + 0.5f);
+                    const float tt = 1.f - ((dA * dA + dB * dB) + dC * dC);
+                    if (tt <= 0.f) continue;
+                    const float w = tt * tt * tt;
+                    const uint32_t fi = ob + fidx(a, f[0], f[1], f[2], rn);
+                    atomicAdd(&m_out[a][fi], w);
+                    atomicAdd(&P_out[a][fi], w * V[a]);
+                }
+    }
+}
+
+struct FaceAcc {
+    float* m[3];
+    float* P[3];
+};
+
+__global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
+                                                 const uint32_t* __restrict__ cs, FaceAcc acc, int* err) {
+    extern __shared__ int smi[];
+    __shared__ int nres[27];
+    __shared__ int cross;
+    __shared__ unsigned red_cnt, red_v;
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
+    const uint32_t c0 = L.off[0][b];
+    const uint32_t ncell = (uint32_t)(r * r * r);
+    const uint32_t p0 = cs[c0], p1 = cs[c0 + ncell];
+    if (p0 == p1) return;
     const Geo& g = L.g;
-    const int nf = (r + 1) * r * r;
-    float* am = sm;
-    float* ap = am + 3 * nf;
-    uint32_t* rstart = (uint32_t*)(ap + 3 * nf);
-    uint32_t* rpre = rstart + P2G_MAXROWS;  // P2G_MAXROWS + 1 entries
     int cb[3];
     bcoord(g, b, cb);
-    for (int i = threadIdx.x; i < 6 * nf; i += blockDim.x) sm[i] = 0.f;
-    if (threadIdx.x < 27) {
-        int nb_, lo[3], hi[3];
-        p2g_nbr_box(L, cb, r, threadIdx.x, &nb_, lo, hi);
-        dcnt[threadIdx.x] = nb_ < 0 ? 0 : (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1);
-    }
-    __syncthreads();
+    const int R1 = r + 1, R2 = r + 2;
+    const int TA = (int)tile_axis(r);
+    int* am = smi;           // 3 TA mass (fixed point)
+    int* ap = smi + 3 * TA;  // 3 TA momentum (fixed point)
+    for (int i = threadIdx.x; i < 6 * TA; i += blockDim.x) smi[i] = 0;
     if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int d = 0; d < 27; ++d) {
-            doff[d] = acc;
-            acc += dcnt[d];
-        }
-        doff[27] = acc;
-        if (acc > P2G_MAXROWS) *err = 1;
+        cross = 0;
+        red_cnt = 0;
+        red_v = 0;
     }
     __syncthreads();
-    const int nrows = min(doff[27], P2G_MAXROWS);
-    for (int k = threadIdx.x; k < nrows; k += blockDim.x) {
-        int d = 0;
-        while (doff[d + 1] <= k) ++d;
-        int nb_, lo[3], hi[3];
-        p2g_nbr_box(L, cb, r, d, &nb_, lo, hi);
-        const int rn = L.res[nb_];
-        const int local = k - doff[d];
-        const int ny = hi[1] - lo[1] + 1;
-        const int y = lo[1] + local % ny, z = lo[2] + local / ny;
-        const uint32_t base = L.off[0][nb_];
-        const uint32_t s0 = cs[base + cidx(lo[0], y, z, rn)];
-        rstart[k] = s0;
-        rpre[k] = cs[base + cidx(hi[0], y, z, rn) + 1] - s0;  // length for now
-    }
-    __syncthreads();
-    // exclusive scan of the row lengths (<= 2048 rows, 8 per thread)
+    // bounds of the fixed-point scales: the most particles in one cell, the largest |v| component
     {
-        const int per = (P2G_MAXROWS + blockDim.x - 1) / blockDim.x;
-        const int r0 = threadIdx.x * per;
-        uint32_t loc = 0;
-        for (int k = r0; k < min(r0 + per, nrows); ++k) loc += rpre[k];
-        // block exclusive scan of loc
-        uint32_t x = loc;
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        unsigned mc = 0, mv = 0;
+        for (uint32_t c = threadIdx.x; c < ncell; c += blockDim.x) mc = max(mc, cs[c0 + c + 1] - cs[c0 + c]);
+        for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x)
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
+            for (int k = 0; k < 3; ++k) mv = max(mv, __float_as_uint(fabsf(soa[(int64_t)(3 + k) * n + i])));
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
+            mv = max(mv, __shfl_xor_sync(0xffffffffu, mv, o));
         }
-        if (lane == 31) wsum[w] = x;
-        __syncthreads();
-        uint32_t wpre = 0;
-        for (int i = 0; i < w; ++i) wpre += wsum[i];
-        uint32_t pre = wpre + x - loc;
-        __syncthreads();
-        for (int k = r0; k < min(r0 + per, nrows); ++k) {
-            uint32_t len = rpre[k];
-            rpre[k] = pre;
-            pre += len;
+        if ((threadIdx.x & 31) == 0) {
+            atomicMax(&red_cnt, mc);
+            atomicMax(&red_v, mv);
         }
-        if (threadIdx.x == blockDim.x - 1) rpre[nrows] = pre;
     }
     __syncthreads();
-    const uint32_t T = rpre[nrows];
+    const float mbound = 18.f * (float)max(red_cnt, 1u);
+    const float vmax = __uint_as_float(red_v);
+    const float Sm = 1073741824.f / mbound;                                  // 2^30 / mass bound
+    if (!isfinite(vmax)) {  // a NaN/Inf velocity: flag it and deposit nothing from this block
+        if (threadIdx.x == 0) atomicExch(err, 1);
+        return;
+    }
+    const float Sp = vmax > 0.f ? 1073741824.f / (mbound * vmax) : Sm;
+    if (threadIdx.x < 27) {
+        const int d = threadIdx.x;
+        const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
+        const int rn = inside(g, nc) ? L.res[bidx(g, nc[0], nc[1], nc[2])] : 0;
+        nres[d] = rn;
+        if (rn && rn != r) atomicOr(&cross, 1 << d);
+    }
+    __syncthreads();
+    const int xmask = cross;
     const float h = fcell(g, r);
     const float invh = 1.f / h;
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
+    // lanes of a warp take particles a 32nd of the range apart, so that they sit in different cells
+    const uint32_t T = p1 - p0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t Ls = (T + 31) / 32;
-    const float rf = (float)r;
-    int row = 0;  // per-lane cursor: v only grows along a lane's walk
     for (uint32_t i = w; i < Ls; i += nw) {
         const uint32_t v = lane * Ls + i;
         if (v >= T) break;
-        while (row + 1 < nrows && rpre[row + 1] <= v) ++row;
-        const uint32_t sidx = rstart[row] + (v - rpre[row]);
-        float q[3], vel[3];
+        const uint32_t sidx = p0 + v;
+        float X[3], V[3], q[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
-            vel[k] = soa[(int64_t)(3 + k) * n + sidx];
+            X[k] = soa[(int64_t)k * n + sidx];
+            V[k] = soa[(int64_t)(3 + k) * n + sidx];
+            q[k] = (X[k] - o[k]) * invh;
         }
-        if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f)
-            continue;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-            const int ia = (int)floorf(q[a]);
-            const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
-            // squared distances per candidate index, 4 (weight 0) where the index is outside the block
+            const int ia = min(max((int)floorf(q[a]), 0), r - 1);
+            const int j1 = min(max((int)floorf(q[t1] - 0.5f), -1), r - 1);
+            const int j2 = min(max((int)floorf(q[t2] - 0.5f), -1), r - 1);
             float dA2[2], dB2[2], dC2[2];
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
                 const float dA = q[a] - (float)(ia + k);
                 const float dB = q[t1] - ((float)(j1 + k) + 0.5f);
                 const float dC = q[t2] - ((float)(j2 + k) + 0.5f);
-                dA2[k] = (ia + k >= 0 && ia + k <= r) ? dA * dA : 4.f;
-                dB2[k] = (j1 + k >= 0 && j1 + k < r) ? dB * dB : 4.f;
-                dC2[k] = (j2 + k >= 0 && j2 + k < r) ? dC * dC : 4.f;
+                dA2[k] = dA * dA;
+                dB2[k] = dB * dB;
+                dC2[k] = dC * dC;
             }
-            // strides of the axis-a face layout (fidx) along x, y, z
-            const int sx = 1, sy = a == 0 ? r + 1 : r, sz = a == 0 ? (r + 1) * r : (a == 1 ? r * (r + 1) : r * r);
-            const int sA = a == 0 ? sx : (a == 1 ? sy : sz);
-            const int s1 = t1 == 0 ? sx : (t1 == 1 ? sy : sz);
-            const int s2 = t2 == 0 ? sx : (t2 == 1 ? sy : sz);
-            const int base = ia * sA + j1 * s1 + j2 * s2;  // index of candidate (0,0,0); may lie outside
-            float* Am = am + a * nf;
-            float* Ap = ap + a * nf;
-            const float va = vel[a];
-            // all 8 candidates, no branches: a candidate with d^2 >= 1 (or outside the block) has
-            // t <= 0 and its two atomics are predicated off
+            const int base = a * TA + ia + R1 * ((j1 + 1) + R2 * (j2 + 1));
+            const float va = V[a];
 #pragma unroll
             for (int da = 0; da < 2; ++da)
 #pragma unroll
@@ -411,53 +429,117 @@ __global__ void __launch_bounds__(256) k_p2g_scatter(LevelView L, const float* _
                     for (int d2 = 0; d2 < 2; ++d2) {
                         const float tt = 1.f - (dAB + dC2[d2]);
                         const float wgt = tt * tt * tt;
-                        const int fi = base + da * sA + d1 * s1 + d2 * s2;
+                        const int e = base + da + d1 * R1 + d2 * R1 * R2;
                         if (tt > 0.f) {
-                            atomicAdd(&Am[fi], wgt);
-                            atomicAdd(&Ap[fi], wgt * va);
+                            atomicAdd(&am[e], __float2int_rn(wgt * Sm));
+                            atomicAdd(&ap[e], __float2int_rn(wgt * va * Sp));
                         }
                     }
                 }
         }
+        if (xmask) {
+            // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
+#pragma unroll 1
+            for (int d = 0; d < 27; ++d) {
+                if (!((xmask >> d) & 1)) continue;
+                const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+                const float reach = nres[d] < r ? 2.f : 1.f;
+                bool near = true;
+#pragma unroll
+                for (int k = 0; k < 3; ++k)
+                    near = near && (dd[k] == 0 || (dd[k] < 0 ? q[k] < reach : q[k] > (float)r - reach));
+                if (!near) continue;
+                const int nc[3] = {cb[0] + dd[0], cb[1] + dd[1], cb[2] + dd[2]};
+                p2g_cross(L, bidx(g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, acc.m, acc.P);
+            }
+        }
     }
     __syncthreads();
+    // flush: every nonzero tile entry into each same-resolution copy of its face
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const uint32_t ob = L.off[1 + a][b];
-        for (int fi = threadIdx.x; fi < nf; fi += blockDim.x) {
-            const float m = am[a * nf + fi], P = ap[a * nf + fi];
-            const uint32_t oi = ob + (uint32_t)fi;
-            out.m[a][oi] = m;
-            if (out.mom[a]) out.mom[a][oi] = P;
-            out.u[a][oi] = m > 1e-6f ? P / m : 0.f;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            const int mi = am[a * TA + rem];
+            if (mi == 0) continue;
+            const float mv = (float)mi / Sm;
+            const float pv = (float)ap[a * TA + rem] / Sp;
+            const int iA = rem % R1;
+            const int i1 = (rem / R1) % R2 - 1;
+            const int i2 = rem / (R1 * R2) - 1;
+            const int B1 = cb[t1] + floordiv(i1, r), B2 = cb[t2] + floordiv(i2, r);
+            const int l1 = i1 - (B1 - cb[t1]) * r, l2 = i2 - (B2 - cb[t2]) * r;
+            const int nA = (iA == 0 || iA == r) ? 2 : 1;
+            for (int k = 0; k < nA; ++k) {
+                int A, lA;
+                if (iA == 0) { A = cb[a] - 1 + k; lA = k == 0 ? r : 0; }
+                else if (iA == r) { A = cb[a] + k; lA = k == 0 ? r : 0; }
+                else { A = cb[a]; lA = iA; }
+                int nc[3];
+                nc[a] = A;
+                nc[t1] = B1;
+                nc[t2] = B2;
+                if (!inside(g, nc)) continue;
+                const int nb = bidx(g, nc[0], nc[1], nc[2]);
+                if (L.res[nb] != r) continue;
+                int f[3];
+                f[a] = lA;
+                f[t1] = l1;
+                f[t2] = l2;
+                const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], r);
+                atomicAdd(&acc.m[a][fi], mv);
+                atomicAdd(&acc.P[a][fi], pv);
+            }
         }
     }
 }
 
-static size_t p2g_smem(int r) {
-    return (size_t)6 * (r + 1) * r * r * sizeof(float) + (size_t)(2 * P2G_MAXROWS + 1) * sizeof(uint32_t);
-}
-
-__global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, float* out) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < nc) out[c] = (float)(cstart[c + 1] - cstart[c]);
+// u = P / m where m > 1e-6, else 0 (normalizeVelocity, P2G.cuh:139-171), over the three axes
+__global__ void k_p2g_normalize(const float* __restrict__ m0, const float* __restrict__ P0, float* u0, uint32_t n0,
+                                const float* __restrict__ m1, const float* __restrict__ P1, float* u1, uint32_t n1,
+                                const float* __restrict__ m2, const float* __restrict__ P2, float* u2, uint32_t n2) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float *m, *P;
+    float* u;
+    if (i < n0) { m = m0; P = P0; u = u0; }
+    else if ((i -= n0) < n1) { m = m1; P = P1; u = u1; }
+    else if ((i -= n1) < n2) { m = m2; P = P2; u = u2; }
+    else return;
+    const float mv = m[i];
+    u[i] = mv > 1e-6f ? P[i] / mv : 0.f;
 }
 
 aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* cstart, float* u[3], float* m[3],
                      float* mom[3], float* cell_count, cudaStream_t s) {
-    FaceOut o;
+    FaceAcc acc;
     for (int a = 0; a < 3; ++a) {
-        o.u[a] = u[a];
-        o.m[a] = m[a];
-        o.mom[a] = mom[a];
+        acc.m[a] = m[a];
+        if (mom[a]) {
+            acc.P[a] = mom[a];
+        } else {
+            AW_TRY(G.p2g_P[a].ensure(std::max<uint32_t>(G.tot[1 + a], 1)));
+            acc.P[a] = G.p2g_P[a].p;
+        }
+        if (G.tot[1 + a]) {
+            AW_CUDA(cudaMemsetAsync(acc.m[a], 0, G.tot[1 + a] * sizeof(float), s));
+            AW_CUDA(cudaMemsetAsync(acc.P[a], 0, G.tot[1 + a] * sizeof(float), s));
+        }
     }
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = p2g_smem(maxres);
-    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    AW_TRY(G.flag.ensure(1));
-    k_p2g_scatter<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, o, G.flag.p);
-    AW_LAUNCH();
+    const size_t smem = (size_t)6 * tile_axis(maxres) * sizeof(float);
+    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_own, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (n > 0) {
+        AW_TRY(ensure_tiles(G));  // allocates the device error flags
+        k_p2g_own<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, acc, G.err.p);
+        AW_LAUNCH();
+    }
+    const uint64_t nf = (uint64_t)G.tot[1] + G.tot[2] + G.tot[3];
+    if (nf) {
+        k_p2g_normalize<<<nblk(nf), 256, 0, s>>>(acc.m[0], acc.P[0], u[0], G.tot[1], acc.m[1], acc.P[1], u[1], G.tot[2],
+                                                 acc.m[2], acc.P[2], u[2], G.tot[3]);
+        AW_LAUNCH();
+    }
     if (cell_count) {
         k_cell_count<<<nblk(G.tot[0]), 256, 0, s>>>(cstart, G.tot[0], cell_count);
         AW_LAUNCH();
@@ -604,8 +686,6 @@ __global__ void k_advect(LevelView L, PArrW pos, int64_t n, float dt, Field3 u) 
 // block: axis-major, entry (iA, i1, i2) at iA + (r+1) ((i1+1) + (r+2) (i2+1)); each block's
 // tiles start on a 16-byte boundary so they can be staged with one TMA bulk copy.
 // ------------------------------------------------------------------------------------------------
-__host__ __device__ inline uint32_t tile_axis(int r) { return (uint32_t)((r + 1) * (r + 2) * (r + 2)); }
-__host__ __device__ inline uint32_t tile_block(int r) { return r ? ((3 * tile_axis(r) + 3u) & ~3u) : 0u; }
 
 __global__ void k_build_tiles(LevelView L, Field3 u, const uint32_t* __restrict__ toff, float* __restrict__ tiles) {
     const int b = blockIdx.x;
@@ -761,16 +841,95 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
-    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
-        float X[3];
+    // four particles per thread in flight: their loads are issued together
+    constexpr int U = 4;
+    const uint32_t st = blockDim.x;
+    for (uint32_t i0 = p0 + threadIdx.x; i0 < p1; i0 += U * st) {
+        float X[U][3], Vv[U][3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) X[k] = soa[(int64_t)k * n + i];
+        for (int k = 0; k < U; ++k) {
+            const uint32_t i = i0 + k * st;
+            if (i < p1)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    X[k][c] = soa[(int64_t)c * n + i];
+                    Vv[k][c] = soa[(int64_t)(3 + c) * n + i];
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const uint32_t i = i0 + k * st;
+            if (i < p1)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    const float vn = tile_interp(tn, a, r, o, h, X[k]);
+                    const float vo = tile_interp(to, a, r, o, h, X[k]);
+                    soa[(int64_t)(3 + a) * n + i] = alpha * (Vv[k][a] + (vn - vo)) + (1.f - alpha) * vn;
+                }
+        }
+    }
+}
+
+// RK3 advection of the sorted particles of one block: the block's u_new tile is staged in shared
+// memory by one bulk copy; stage points that leave the block sample the neighbour's tile in global
+// memory (same arithmetic as sample_tiles).
+__device__ inline float sample_local(const LevelView& L, int b, const int cb[3], int r, const float o[3], float h,
+                                     const float* __restrict__ tl, const uint32_t* __restrict__ toff,
+                                     const float* __restrict__ tg, int a, const float X[3]) {
+    int pc[3];
+    point_block(L.g, X, pc);
+    if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) return tile_interp(tl, a, r, o, h, X);
+    return sample_tiles(L, toff, tg, a, X);
+}
+
+__global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restrict__ soa, int64_t n,
+                                                     const uint32_t* __restrict__ cs, float dt,
+                                                     const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
+                                                     int* err) {
+    extern __shared__ __align__(16) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    const uint32_t p0 = cs[L.off[0][b]], p1 = cs[L.off[0][b] + (uint32_t)(r * r * r)];
+    if (p0 == p1) return;
+    const uint32_t tb = tile_block(r);
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        mbar_expect_tx(&bar, tb * sizeof(float));
+        tma_bulk_load(sm, tn_g + toff[b], tb * sizeof(float), &bar);
+    }
+    const bool ok = mbar_wait_bounded(&bar, 0, err);
+    if (!__syncthreads_and(ok)) return;
+    const Geo& g = L.g;
+    int cb[3];
+    bcoord(g, b, cb);
+    const float h = fcell(g, r);
+    float o[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
+    const float h0 = g.bs / (float)g.R0;
+    for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x) {
+        float x[3], k1[3], k2[3], k3[3], y[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) x[a] = soa[(int64_t)a * n + i];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k1[a] = tile_interp(sm, a, r, o, h, x);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.5f * dt * k1[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k2[a] = sample_local(L, b, cb, r, o, h, sm, toff, tn_g, a, y);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.75f * dt * k2[a];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) k3[a] = sample_local(L, b, cb, r, o, h, sm, toff, tn_g, a, y);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float vn = tile_interp(tn, a, r, o, h, X);
-            const float vo = tile_interp(to, a, r, o, h, X);
-            float* vp = soa + (int64_t)(3 + a) * n + i;
-            *vp = alpha * (*vp + (vn - vo)) + (1.f - alpha) * vn;
+            const float v = (2.f / 9.f) * k1[a] + (3.f / 9.f) * k2[a] + (4.f / 9.f) * k3[a];
+            const float lo = g.dmin[a] + 0.01f * h0;
+            const float hi = g.dmin[a] + (float)g.D[a] * g.bs - 0.01f * h0;
+            soa[(int64_t)a * n + i] = fminf(fmaxf(x[a] + dt * v, lo), hi);
         }
     }
 }
@@ -822,7 +981,10 @@ aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
     int h[4];
     AW_CUDA(cudaMemcpyAsync(h, G.err.p, sizeof h, cudaMemcpyDeviceToHost, s));
     AW_CUDA(cudaStreamSynchronize(s));
-    if (h[0]) return set_error(AW_ERR_STATE, "P2G halo row table overflow");
+    if (h[0]) {
+        AW_CUDA(cudaMemsetAsync(G.err.p, 0, sizeof(int), s));
+        return set_error(AW_ERR_NAN, "P2G met a non-finite particle velocity");
+    }
     if (h[1]) return set_error(AW_ERR_STATE, "TMA bulk-copy wait timed out in G2P");
     return AW_OK;
 }
@@ -895,6 +1057,18 @@ __global__ void k_sample_tiles(LevelView L, PArr pts, int64_t n, const uint32_t*
     float X[3] = {pts(i, 0), pts(i, 1), pts(i, 2)};
 #pragma unroll
     for (int a = 0; a < 3; ++a) out[3 * i + a] = sample_tiles(L, toff, tiles, a, X);
+}
+
+aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, cudaStream_t s) {
+    if (n <= 0) return AW_OK;
+    int maxres = 0;
+    for (int r : G.h_res) maxres = std::max(maxres, r);
+    const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
+    if (smem > 48 * 1024)
+        AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1);
+    AW_LAUNCH();
+    return AW_OK;
 }
 
 aw_status advect_tiles(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* tiles, cudaStream_t s) {

@@ -322,10 +322,16 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-poisson", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--poisson-only", action="store_true",
+                    help="only the poisson_256 projection comparison (for profiling the solver)")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:
-        if args.impl == "reference":
+        if args.poisson_only:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(poisson_bench(args)), flush=True)
+        elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:
             run_ours(args, ws, rank, local)
