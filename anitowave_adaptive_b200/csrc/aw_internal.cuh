@@ -214,7 +214,7 @@ struct MsbgState {
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for
     FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
-    DBuf<int> err;  // device error flags: [0] non-finite velocity in P2G, [1] TMA wait timeout
+    DBuf<int> err;  // device error flags: [1] bulk-copy wait timeout in G2P / advection ([0] unused)
     DBuf<uint8_t> occ;
     DBuf<int> flag;
     ParticleWork pw;

@@ -264,14 +264,11 @@ __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, f
 // no index checks: the weight is max(0, 1 - d^2/h^2)^3 and the shared-memory atomics of zero
 // weights are predicated off.
 //
-// The tile accumulates in 32-bit fixed point (shared-memory integer atomics are native and about
-// twice the rate of float ones on this part).  The scales are per CTA and safe by construction: a
-// face's support spans 2 x 3 x 3 cells, so its mass from b's particles is at most 18 x (the most
-// particles in one of b's cells), and |momentum| at most that bound x (b's largest |v|); both map
-// to 2^30.  The rounding error is below 1e-7 of those bounds per particle.
+// The tile accumulates in FP32.  (A fixed-point tile with integer atomics ran faster, but its
+// absolute rounding error is amplified by u = P/m on the low-mass faces at the fluid's edge.)
 //
-// The flush adds every nonzero tile entry, back in float, into each copy of that physical face held
-// by a block of b's resolution (a face on a block boundary has one copy per side).  Faces of
+// The flush adds every nonzero tile entry into each copy of that physical face held by a block of
+// b's resolution (a face on a block boundary has one copy per side).  Faces of
 // neighbours at another resolution are at other positions: particles within reach of such a
 // neighbour add their weights in the neighbour's own lattice with global float atomics.  A second
 // kernel normalises u = P / m.  The face arrays must start at zero.
@@ -321,58 +318,26 @@ struct FaceAcc {
 };
 
 __global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
-                                                 const uint32_t* __restrict__ cs, FaceAcc acc, int* err) {
-    extern __shared__ int smi[];
+                                                 const uint32_t* __restrict__ cs, FaceAcc acc) {
+    extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ int cross;
-    __shared__ unsigned red_cnt, red_v;
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
     const uint32_t c0 = L.off[0][b];
-    const uint32_t ncell = (uint32_t)(r * r * r);
-    const uint32_t p0 = cs[c0], p1 = cs[c0 + ncell];
+    const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
     if (p0 == p1) return;
     const Geo& g = L.g;
     int cb[3];
     bcoord(g, b, cb);
     const int R1 = r + 1, R2 = r + 2;
     const int TA = (int)tile_axis(r);
-    int* am = smi;           // 3 TA mass (fixed point)
-    int* ap = smi + 3 * TA;  // 3 TA momentum (fixed point)
-    for (int i = threadIdx.x; i < 6 * TA; i += blockDim.x) smi[i] = 0;
-    if (threadIdx.x == 0) {
-        cross = 0;
-        red_cnt = 0;
-        red_v = 0;
-    }
+    float* am = sm;           // 3 TA mass
+    float* ap = sm + 3 * TA;  // 3 TA momentum
+    for (int i = threadIdx.x; i < 6 * TA; i += blockDim.x) sm[i] = 0.f;
+    if (threadIdx.x == 0) cross = 0;
     __syncthreads();
-    // bounds of the fixed-point scales: the most particles in one cell, the largest |v| component
-    {
-        unsigned mc = 0, mv = 0;
-        for (uint32_t c = threadIdx.x; c < ncell; c += blockDim.x) mc = max(mc, cs[c0 + c + 1] - cs[c0 + c]);
-        for (uint32_t i = p0 + threadIdx.x; i < p1; i += blockDim.x)
-#pragma unroll
-            for (int k = 0; k < 3; ++k) mv = max(mv, __float_as_uint(fabsf(soa[(int64_t)(3 + k) * n + i])));
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            mc = max(mc, __shfl_xor_sync(0xffffffffu, mc, o));
-            mv = max(mv, __shfl_xor_sync(0xffffffffu, mv, o));
-        }
-        if ((threadIdx.x & 31) == 0) {
-            atomicMax(&red_cnt, mc);
-            atomicMax(&red_v, mv);
-        }
-    }
-    __syncthreads();
-    const float mbound = 18.f * (float)max(red_cnt, 1u);
-    const float vmax = __uint_as_float(red_v);
-    const float Sm = 1073741824.f / mbound;                                  // 2^30 / mass bound
-    if (!isfinite(vmax)) {  // a NaN/Inf velocity: flag it and deposit nothing from this block
-        if (threadIdx.x == 0) atomicExch(err, 1);
-        return;
-    }
-    const float Sp = vmax > 0.f ? 1073741824.f / (mbound * vmax) : Sm;
     if (threadIdx.x < 27) {
         const int d = threadIdx.x;
         const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
@@ -431,8 +396,8 @@ __global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __res
                         const float wgt = tt * tt * tt;
                         const int e = base + da + d1 * R1 + d2 * R1 * R2;
                         if (tt > 0.f) {
-                            atomicAdd(&am[e], __float2int_rn(wgt * Sm));
-                            atomicAdd(&ap[e], __float2int_rn(wgt * va * Sp));
+                            atomicAdd(&am[e], wgt);
+                            atomicAdd(&ap[e], wgt * va);
                         }
                     }
                 }
@@ -460,10 +425,9 @@ __global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __res
     for (int a = 0; a < 3; ++a) {
         const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
         for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
-            const int mi = am[a * TA + rem];
-            if (mi == 0) continue;
-            const float mv = (float)mi / Sm;
-            const float pv = (float)ap[a * TA + rem] / Sp;
+            const float mv = am[a * TA + rem];
+            if (mv == 0.f) continue;
+            const float pv = ap[a * TA + rem];
             const int iA = rem % R1;
             const int i1 = (rem / R1) % R2 - 1;
             const int i2 = rem / (R1 * R2) - 1;
@@ -530,8 +494,7 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     const size_t smem = (size_t)6 * tile_axis(maxres) * sizeof(float);
     if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_own, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (n > 0) {
-        AW_TRY(ensure_tiles(G));  // allocates the device error flags
-        k_p2g_own<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, acc, G.err.p);
+        k_p2g_own<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, acc);
         AW_LAUNCH();
     }
     const uint64_t nf = (uint64_t)G.tot[1] + G.tot[2] + G.tot[3];
@@ -981,10 +944,6 @@ aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
     int h[4];
     AW_CUDA(cudaMemcpyAsync(h, G.err.p, sizeof h, cudaMemcpyDeviceToHost, s));
     AW_CUDA(cudaStreamSynchronize(s));
-    if (h[0]) {
-        AW_CUDA(cudaMemsetAsync(G.err.p, 0, sizeof(int), s));
-        return set_error(AW_ERR_NAN, "P2G met a non-finite particle velocity");
-    }
     if (h[1]) return set_error(AW_ERR_STATE, "TMA bulk-copy wait timed out in G2P");
     return AW_OK;
 }

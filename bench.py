@@ -11,6 +11,8 @@ Workload (one process per GPU; the path does not shard, so N GPUs run N replicas
              and a device->host copy of the velocities.
   poisson  = poisson_256 (256^3 effective, 4 levels) projection to 1e-6 and 1e-9 relative residual,
              FP32 V-cycle vs mixed precision.
+  flip_256 = dam_drop2_256 (256^3 effective, 4 levels, 34.7M particles) FLIP steps/s with the mixed
+             and the plain FP32 projection.
   --impl reference: the FP64 OpenMP CPU restatement (oracle) of the same P2G+G2P workload, timed on
              the host cores.
 
@@ -247,6 +249,9 @@ def run_ours(args, ws, rank, local):
     poisson = None
     if not args.skip_poisson:
         poisson = poisson_bench(args)
+    flip256 = None
+    if not args.skip_flip256:
+        flip256 = flip256_bench()
 
     if rank != 0:
         return
@@ -279,6 +284,8 @@ def run_ours(args, ws, rank, local):
     }
     if poisson is not None:
         line["poisson"] = poisson
+    if flip256 is not None:
+        line["flip_256"] = flip256
     print(json.dumps(line), flush=True)
 
 
@@ -314,6 +321,58 @@ def poisson_bench(args):
     return out
 
 
+def poisson_solve_once():
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import poisson as pz
+    prob = pz.build_problem(256)
+    sv = aw.Solver(prob.grid, precision=aw.PRECISION_MIXED, tolerance=1e-6, max_cycles=60)
+    sv.setup(None)
+    p = torch.zeros(prob.b.numel(), dtype=torch.float64, device="cuda")
+    sv.solve(prob.b, p, raise_on_error=False)
+    p.zero_()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    cyc, rel, st = sv.solve(prob.b, p, raise_on_error=False)
+    torch.cuda.synchronize()
+    return {"workload": "poisson_256", "ms": 1e3 * (time.perf_counter() - t0), "cycles": cyc, "rel_residual": rel}
+
+
+def flip256_bench(steps=5, warmup=2):
+    """dam_drop2_256 (256^3 effective, 4 levels, 34.7M particles): FLIP steps/s, mixed vs plain FP32
+    projection.  Plain FP32 stalls above 1e-6 relative residual at this size, so it runs to 1e-5."""
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import scenes
+    S = scenes.config("dam_drop2_256")
+    g = aw.build_grid(S)
+    tot = g.totals()
+    out = {"workload": "dam_drop2_256", "particles": S.n, "cells": tot[0], "faces": sum(tot[1:]), "steps": steps}
+    for name, prec, tol in (("mixed", aw.PRECISION_MIXED, 1e-6), ("fp32", aw.PRECISION_FP32, 1e-5)):
+        F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=prec, tolerance=tol, max_cycles=60)
+        for _ in range(warmup):
+            F.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = []
+        for _ in range(steps):
+            F.step()
+            st.append(F.stats())
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"tolerance": tol, "ms_per_step": ms, "steps_per_s": 1e3 / ms,
+                     "cycles": [x["cycles"] for x in st], "residual": st[-1]["residual"],
+                     "div_before": st[-1]["div_before"], "div_after": st[-1]["div_after"],
+                     "ms_solve": float(np.mean([x["ms_solve"] for x in st])),
+                     "ms_p2g": float(np.mean([x["ms_p2g"] for x in st])),
+                     "ms_g2p": float(np.mean([x["ms_g2p"] for x in st]))}
+        F.close()
+    g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -322,8 +381,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-poisson", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--skip-flip256", action="store_true", help="skip the dam_drop2_256 FLIP steps/s section")
     ap.add_argument("--poisson-only", action="store_true",
                     help="only the poisson_256 projection comparison (for profiling the solver)")
+    ap.add_argument("--poisson-solve-once", action="store_true",
+                    help="one mixed-precision poisson_256 solve to 1e-6 after one warm-up solve (small ncu captures)")
     args = ap.parse_args()
     ws, rank, local = dist_init()
     try:
@@ -331,6 +393,10 @@ def main():
             import torch
             torch.cuda.set_device(local)
             print(json.dumps(poisson_bench(args)), flush=True)
+        elif args.poisson_solve_once:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(poisson_solve_once()), flush=True)
         elif args.impl == "reference":
             run_reference(args, ws, rank)
         else:

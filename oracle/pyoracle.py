@@ -463,3 +463,24 @@ def rollout64_grad(O: "Oracle", x0, u0, recs, xN, target, dt, alpha, tol=1e-12):
     ub = O._faces()
     O.sample_vjp(np.ascontiguousarray(x0, np.float64).reshape(-1, 3), u0, vb, ub, None)
     return ub
+
+
+def grad_along_states(O: "Oracle", xs, vs, u0, target, dt, alpha, gravity, tol=1e-12):
+    """d loss / d u0 in FP64 along a given trajectory: xs[k], vs[k] (k = 0..N, particle-id order)
+    are the states another implementation produced.  Each step's adjoint is evaluated at that
+    step's given input state, so the result isolates the adjoint arithmetic from the divergence of
+    two forward trajectories."""
+    recs = []
+    for k in range(len(xs) - 1):
+        _, _, rec = flip_step64(O, np.asarray(xs[k], np.float64), np.asarray(vs[k], np.float64), dt, alpha, gravity, tol)
+        rec.pop("u1_sync", None)
+        recs.append(rec)
+    xN = np.asarray(xs[-1], np.float64)
+    n = xN.shape[0]
+    xb = 2.0 * (xN - target) / n
+    vb = np.zeros_like(xb)
+    for rec in reversed(recs):
+        xb, vb = flip_step64_vjp(O, rec, xb, vb, dt, alpha, tol)
+    ub = O._faces()
+    O.sample_vjp(np.asarray(xs[0], np.float64), u0, vb, ub, None)
+    return ub
