@@ -217,6 +217,14 @@ __device__ inline void rot3(int a, int p0, int p1, int p2, int& x, int& y, int& 
 // that R: every index split is then a shift, a mask or a multiply by a constant, and every loop
 // has a fixed trip count.
 constexpr int NT = 256;
+// CTAs per SM the batched block kernels are compiled for (registers per thread <= 64K / (NT x this))
+#ifndef AW_BLOCK_CTAS_PER_SM
+#define AW_BLOCK_CTAS_PER_SM 6
+#endif
+// loads in flight per thread when staging decoded or averaged halo values
+#ifndef AW_STAGE_BATCH
+#define AW_STAGE_BATCH 2
+#endif
 
 template <int R>
 struct Geom {
@@ -295,7 +303,7 @@ template <int R, class Src, bool HALO>
 __device__ inline void stage_items(SlotImage<typename Src::T, R>& S, const Src& x) {
     using T = typename Src::T;
     using Gm = Geom<R>;
-    constexpr int GM = Gm::GMAX, n3 = Gm::n3, rr = Gm::rr, K = 4;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3, rr = Gm::rr, K = AW_STAGE_BATCH;
     constexpr int NI = HALO ? GM * 6 * rr : GM * n3;
 #pragma unroll
     for (int base = 0; base < NI; base += K * NT) {
@@ -489,12 +497,30 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
         float lmax = 0.f;
 #pragma unroll
         for (int col = 0; col < 2; ++col) {
+            // one slot per CTA (8^3 and 16^3 blocks): each thread visits only cells of this colour;
+            // smaller blocks keep one thread per cell so that a slot's threads stay contiguous
+            constexpr bool HALF = GM == 1 && R >= 2;
+            constexpr int NC = HALF ? n3 / 2 : GM * n3;
 #pragma unroll
-            for (int t0 = 0; t0 < GM * n3; t0 += NT) {
-                const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
+            for (int t0 = 0; t0 < NC; t0 += NT) {
+                const int t = t0 + threadIdx.x;
+                int sl, i, cx, cy, cz;
+                if (HALF) {
+                    if (t >= NC) continue;
+                    sl = 0;
+                    cy = (t / (R / 2)) % R;
+                    cz = t / (R / 2 * R);
+                    cx = 2 * (t % (R / 2)) + ((cy + cz + col) & 1);
+                    i = cx + R * (cy + R * cz);
+                } else {
+                    sl = t / n3;
+                    i = t % n3;
+                    cx = i % R;
+                    cy = (i / R) % R;
+                    cz = i / Gm::rr;
+                }
                 if (sl >= G || sb[sl] < 0 || Z.sdone[sl]) continue;
-                const int cx = i % R, cy = (i / R) % R, cz = i / Gm::rr;
-                if (((cx + cy + cz) & 1) != col) continue;
+                if (!HALF && ((cx + cy + cz) & 1) != col) continue;
                 if (P.check_fluid && !S.fluid(sl, i)) continue;
                 float* xs = S.xs + sl * Gm::X3;
                 const float* bs = S.fs + sl * Gm::FS;
@@ -553,7 +579,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
 
 // smoothActiveBlocks (Smoother.cuh:105-202) for one block colour, batched.  status == nullptr
 // means every block is active (no residual-threshold deactivation) and no activation is written.
-__global__ void __launch_bounds__(NT, 4) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
+__global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_smooth(LevelView L, XStore x, const float* __restrict__ bvec, Coef3 W,
                                                const uint8_t* __restrict__ fluid, Batch B,
                                                const uint8_t* __restrict__ status, uint8_t* __restrict__ status_next,
                                                SmoothParams P) {
@@ -614,7 +640,7 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
 // residual, double for the FP64 residual of the outer defect correction (stored as FP32 into the
 // V-cycle right-hand side).
 template <class Src>
-__global__ void __launch_bounds__(NT, 4) k_residual(Src x, const float* __restrict__ bvec, Coef3 W,
+__global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_residual(Src x, const float* __restrict__ bvec, Coef3 W,
                                                  const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
                                                  float* __restrict__ rout, double* __restrict__ part) {
     extern __shared__ __align__(16) unsigned char smraw[];
