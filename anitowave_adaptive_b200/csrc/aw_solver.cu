@@ -76,8 +76,11 @@ struct aw_solver {
     // level-0 bindings for the current solve
     float* x0 = nullptr;
     const float* b0 = nullptr;
-    // mixed precision
+    // mixed precision: FP64 vectors of the conjugate-gradient outer loop (residual, direction,
+    // -A d), its scalars {rho, rho_old, d.(-A d)} and a zero right-hand side for applying A
     aw::DBuf<double> p64tmp;
+    aw::DBuf<double> cg_r, cg_d, cg_q, cg_sc;
+    aw::DBuf<float> cg_zero;
     aw::DBuf<double> partials, norm;
     size_t smem_max = 0, smem_max64 = 0;
     // the whole V-cycle as a CUDA graph, captured once per (x0, b0) binding
@@ -594,7 +597,7 @@ __global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_smooth(LevelView L
 template <int R, class Src>
 __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred, const Src& x, const float* __restrict__ bvec,
                                      const Coef3& W, const uint8_t* __restrict__ fluid, const Batch& B, int check_fluid,
-                                     float* __restrict__ rout, double* __restrict__ part) {
+                                     float* __restrict__ rout, double* __restrict__ rout64, double* __restrict__ part) {
     using T = typename Src::T;
     using Gm = Geom<R>;
     constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
@@ -626,7 +629,8 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
                          wB * xs[q - sz] + wT * xs[q + sz];
             rv = (T)bs[i] - Ax;
         }
-        rout[S.off(0, sl) + i] = (float)rv;
+        if (rout) rout[S.off(0, sl) + i] = (float)rv;
+        if (rout64) rout64[S.off(0, sl) + i] = (double)rv;
         acc += (double)rv * (double)rv;
     }
     if (part) {
@@ -642,11 +646,12 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
 template <class Src>
 __global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_residual(Src x, const float* __restrict__ bvec, Coef3 W,
                                                  const uint8_t* __restrict__ fluid, Batch B, int check_fluid,
-                                                 float* __restrict__ rout, double* __restrict__ part) {
+                                                 float* __restrict__ rout, double* __restrict__ rout64,
+                                                 double* __restrict__ part) {
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double dred[32];
     const int4 d = B.desc[blockIdx.x];
-#define AW_RESID(R) residual_body<R>(d, smraw, dred, x, bvec, W, fluid, B, check_fluid, rout, part)
+#define AW_RESID(R) residual_body<R>(d, smraw, dred, x, bvec, W, fluid, B, check_fluid, rout, rout64, part)
     AW_SWITCH_RES(d.z, AW_RESID)
 #undef AW_RESID
 }
@@ -771,6 +776,47 @@ __global__ void __launch_bounds__(NT) k_prolong(XStore xf, XStore xc, const uint
     AW_SWITCH_RES(d.z, AW_PROL)
 #undef AW_PROL
 }
+
+// ---- conjugate-gradient outer loop of the mixed-precision solve (FP64 vectors) ----------------
+// dot(a, b) over fluid cells (b is FP64, or FP32 when bf is given), per-CTA partial sums
+__global__ void k_dot64(const double* __restrict__ a, const double* __restrict__ b, const float* __restrict__ bf,
+                        const uint8_t* __restrict__ fluid, size_t n, double* __restrict__ part) {
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (fluid[i]) acc += a[i] * (bf ? (double)bf[i] : b[i]);
+    __shared__ double red[32];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
+}
+// z (FP32 V-cycle output) -> search direction d = z + beta d, beta = rho / rho_old (0 when first)
+__global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__ z, const uint8_t* __restrict__ fluid,
+                               const double* __restrict__ sc, int first, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double beta = first ? 0.0 : sc[0] / sc[1];
+    d[i] = fluid[i] ? (double)z[i] + beta * d[i] : 0.0;
+}
+// qn = -A d (the residual kernel with a zero right-hand side); alpha = rho / (d . A d)
+// p += alpha d; r += alpha qn; and the FP32 copy of r for the next V-cycle
+__global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, float* __restrict__ rf,
+                            const double* __restrict__ d, const double* __restrict__ qn, const double* __restrict__ sc,
+                            size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double dq = -sc[2];
+    const double alpha = dq != 0.0 ? sc[0] / dq : 0.0;
+    p[i] += alpha * d[i];
+    const double rv = r[i] + alpha * qn[i];
+    r[i] = rv;
+    rf[i] = (float)rv;
+}
+__global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1392,7 +1438,7 @@ static aw_status residual_level(aw_solver* S, int m, double* part, cudaStream_t 
     XStore x = xstore(S, m);
     if (L.ndesc[2]) {
         k_residual<SrcX><<<L.ndesc[2], 256, L.smem_smooth, s>>>(SrcX{x}, bptr(S, m), coef(L), L.fluid.p, batch(L, 2), cf,
-                                                                 L.r.p, part);
+                                                                 L.r.p, nullptr, part);
         AW_LAUNCH();
     }
     return AW_OK;
@@ -1668,6 +1714,16 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
     }
     if (S->smem_max64 > 48 * 1024)
         AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
+    if (d->precision == AW_PRECISION_MIXED) {
+        const size_t nc0 = S->lv[0].ncell();
+        AW_TRY(S->cg_r.alloc(nc0));
+        AW_TRY(S->cg_d.alloc(nc0));
+        AW_TRY(S->cg_q.alloc(nc0));
+        AW_TRY(S->cg_sc.alloc(4));
+        AW_TRY(S->cg_zero.alloc(nc0));
+        AW_CUDA(cudaMemset(S->cg_zero.p, 0, nc0 * sizeof(float)));
+        AW_CUDA(cudaMemset(S->cg_d.p, 0, nc0 * sizeof(double)));
+    }
     size_t nparts = (size_t)nb + 1024;
     AW_TRY(S->partials.alloc(nparts));
     AW_TRY(S->norm.alloc(2));
@@ -1866,40 +1922,76 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
         S->x0 = nullptr;
         S->b0 = nullptr;
     } else {
+        // Mixed precision: conjugate gradients preconditioned by the FP32 V-cycle (FP16-stored coarse
+        // corrections), with the residual, the search direction and the pressure accumulation in
+        // FP64 and the FP64 coarsest solve inside the V-cycle.  A stand-alone V-cycle iteration
+        // stalls or diverges on free-surface domains with four levels; as a preconditioner the same
+        // cycle converges on every configuration.  One host read (||r||) per iteration.
         double* p = (double*)d_p;
-        for (;; ++it) {
-            k_residual<SrcD><<<L0.ndesc[2], 256, L0.smem_x64, s>>>(SrcD{p}, d_b, coef(L0), L0.fluid.p, batch(L0, 2), cf,
-                                                                    L0.b.p, S->partials.p);
+        double* sc = S->cg_sc.p;
+        const unsigned ndot = 256;
+        auto launch_err = [&](const char* what) -> aw_status {
             ++g_launches;
             cudaError_t e = cudaGetLastError();
-            if (e != cudaSuccess) {
-                st = set_error(AW_ERR_CUDA, "k_residual64: %s", cudaGetErrorString(e));
-                break;
-            }
-            double rn;
-            st = read_norm(S, nlist, s, &rn);
-            if (st != AW_OK) break;
+            return e == cudaSuccess ? AW_OK : set_error(AW_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+        };
+        auto true_residual = [&]() -> aw_status {
+            k_residual<SrcD><<<L0.ndesc[2], 256, L0.smem_x64, s>>>(SrcD{p}, d_b, coef(L0), L0.fluid.p, batch(L0, 2), cf,
+                                                                    L0.b.p, S->cg_r.p, S->partials.p);
+            return launch_err("k_residual64");
+        };
+        st = true_residual();
+        double rn = 0;
+        if (st == AW_OK) st = read_norm(S, nlist, s, &rn);
+        bool restart = true;
+        while (st == AW_OK) {
             rel = rn / bn;
             if (!(rel == rel)) {
-                st = set_error(AW_ERR_NAN, "residual became NaN after %d cycles", it);
+                st = set_error(AW_ERR_NAN, "residual became NaN after %d iterations", it);
                 break;
             }
-            if (rel < S->d.tolerance) break;
+            if (rel < S->d.tolerance) {
+                if (restart) break;  // rn is a true residual
+                // confirm with the true FP64 residual (the recursive one can drift)
+                st = true_residual();
+                if (st == AW_OK) st = read_norm(S, nlist, s, &rn);
+                restart = true;
+                continue;
+            }
             if (it >= S->d.max_cycles) {
-                st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d cycles", rel, it);
+                st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d iterations", rel, it);
                 break;
             }
+            // z = V(r): one V-cycle on the FP32 copy of r (in L0.b), from zero
             st = zero_x(S, 0, s);
+            if (st == AW_OK) st = run_vcycle(S, s);
             if (st != AW_OK) break;
-            st = run_vcycle(S, s);
-            if (st != AW_OK) break;
-            k_accum64<<<nblk(nc), 256, 0, s>>>(p, L0.x.p, nc);
-            ++g_launches;
-            e = cudaGetLastError();
-            if (e != cudaSuccess) {
-                st = set_error(AW_ERR_CUDA, "k_accum64: %s", cudaGetErrorString(e));
-                break;
-            }
+            // rho = r . z ; d = z + (rho / rho_old) d
+            k_dot64<<<ndot, 256, 0, s>>>(S->cg_r.p, nullptr, L0.x.p, L0.fluid.p, nc, S->partials.p);
+            if ((st = launch_err("k_dot64")) != AW_OK) break;
+            k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, ndot, sc + 0);
+            if ((st = launch_err("k_reduce_sum")) != AW_OK) break;
+            k_cg_direction<<<nblk(nc), 256, 0, s>>>(S->cg_d.p, L0.x.p, L0.fluid.p, sc, restart ? 1 : 0, nc);
+            if ((st = launch_err("k_cg_direction")) != AW_OK) break;
+            // qn = -A d ; sc[2] = d . qn
+            k_residual<SrcD><<<L0.ndesc[2], 256, L0.smem_x64, s>>>(SrcD{S->cg_d.p}, S->cg_zero.p, coef(L0), L0.fluid.p,
+                                                                    batch(L0, 2), cf, nullptr, S->cg_q.p, nullptr);
+            if ((st = launch_err("k_residual64 (A d)")) != AW_OK) break;
+            k_dot64<<<ndot, 256, 0, s>>>(S->cg_d.p, S->cg_q.p, nullptr, L0.fluid.p, nc, S->partials.p);
+            if ((st = launch_err("k_dot64")) != AW_OK) break;
+            k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, ndot, sc + 2);
+            if ((st = launch_err("k_reduce_sum")) != AW_OK) break;
+            // p += alpha d ; r -= alpha A d ; FP32 copy of r for the next V-cycle ; rho_old = rho
+            k_cg_update<<<nblk(nc), 256, 0, s>>>(p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, nc);
+            if ((st = launch_err("k_cg_update")) != AW_OK) break;
+            k_copy_scalar<<<1, 1, 0, s>>>(sc, 1, 0);
+            if ((st = launch_err("k_copy_scalar")) != AW_OK) break;
+            ++it;
+            restart = false;
+            // ||r||
+            k_dot64<<<ndot, 256, 0, s>>>(S->cg_r.p, S->cg_r.p, nullptr, L0.fluid.p, nc, S->partials.p);
+            if ((st = launch_err("k_dot64")) != AW_OK) break;
+            st = read_norm(S, ndot, s, &rn);
         }
     }
     if (cycles) *cycles = it;

@@ -381,19 +381,26 @@ def flip256_bench(steps=5, warmup=2):
     out = {"workload": "dam_drop2_256", "particles": S.n, "cells": tot[0], "faces": sum(tot[1:]), "steps": steps}
     for name, prec, tol in (("mixed", aw.PRECISION_MIXED, 1e-6), ("fp32", aw.PRECISION_FP32, 1e-5)):
         F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=prec, tolerance=tol, max_cycles=60)
-        for _ in range(warmup):
-            F.step()
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        st = []
-        for _ in range(steps):
-            F.step()
-            st.append(F.stats())
-        e1.record()
-        torch.cuda.synchronize()
+        try:
+            for _ in range(warmup):
+                F.step()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            st = []
+            for _ in range(steps):
+                F.step()
+                st.append(F.stats())
+            e1.record()
+            torch.cuda.synchronize()
+        except aw.AWError as err:  # the plain FP32 V-cycle iteration does not converge on this layout
+            torch.cuda.synchronize()
+            out[name] = {"tolerance": tol, "converged": False, "error": str(err), "cycles": F.stats()["cycles"],
+                         "residual": F.stats()["residual"]}
+            F.close()
+            continue
         ms = e0.elapsed_time(e1) / steps
-        out[name] = {"tolerance": tol, "ms_per_step": ms, "steps_per_s": 1e3 / ms,
+        out[name] = {"tolerance": tol, "converged": True, "ms_per_step": ms, "steps_per_s": 1e3 / ms,
                      "cycles": [x["cycles"] for x in st], "residual": st[-1]["residual"],
                      "div_before": st[-1]["div_before"], "div_after": st[-1]["div_after"],
                      "ms_solve": float(np.mean([x["ms_solve"] for x in st])),

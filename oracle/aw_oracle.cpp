@@ -1152,6 +1152,14 @@ OC_API void oc_set_params(void* h, int mode, int pre, int post, int coarsest_ite
     C->built = false;
 }
 
+// FV hierarchy rule for coarse fluid flags: 1 = a coarse cell is fluid iff all its children are,
+// 0 = iff any child is.
+OC_API void oc_set_coarse_all(void* h, int all) {
+    Ctx* C = (Ctx*)h;
+    C->P.coarse_all = all;
+    C->built = false;
+}
+
 // Offsets at MG level m (vanish = reference semantics).  out: 4*nb (cell, fx, fy, fz); tot: 4
 OC_API void oc_offsets(void* h, int m, int vanish, uint32_t* out, uint32_t* tot) {
     Ctx* C = (Ctx*)h;

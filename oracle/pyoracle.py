@@ -92,6 +92,7 @@ def lib():
         L.oc_p2g_vjp.argtypes = [P, f64p, f64p, C.c_int64, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                  C.POINTER(C.c_void_p), f64p, f64p]
         L.oc_face_sync_vjp.argtypes = [P, f64p, f64p, f64p]
+        L.oc_set_coarse_all.argtypes = [P, C.c_int]
         L.oc_divergence_vjp.argtypes = [P, f64p, u8p, C.c_double, f64p, f64p, f64p]
         L.oc_gradient_vjp.argtypes = [P, C.c_double, f64p, f64p, f64p, f64p]
         _lib = L
