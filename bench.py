@@ -59,7 +59,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "50"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
 
@@ -73,7 +73,7 @@ class Clocks:
             self.p.kill()
         self.f.flush()
         self.f.seek(0)
-        sm, mx, reasons = [], [], set()
+        sm, mx, pw, reasons = [], [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.f.read().strip().splitlines():
             parts = [x.strip() for x in line.split(",")]
@@ -82,14 +82,19 @@ class Clocks:
             try:
                 sm.append(float(parts[1]))
                 mx.append(float(parts[2]))
+                pw.append(float(parts[3]))
             except ValueError:
                 continue
             for nm, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
         os.unlink(self.f.name)
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        # "under load": samples drawing well above idle power (host-side scene set-up sits between the
+        # timed regions)
+        load = [c for c, w in zip(sm, pw) if w > 250.0] or sm
+        return {"sm_mhz": float(np.median(load)) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm), "samples_under_load": len(load),
+                "power_w_max": max(pw) if pw else None}
 
 
 def dist_init():
@@ -206,7 +211,6 @@ def run_ours(args, ws, rank, local):
     ev1.record()
     torch.cuda.synchronize()
     launches = aw.launch_count() - l0
-    clocks = clk.stop() if clk else None
     barrier(ws)
     ms_total = max_over_ranks(ws, ev0.elapsed_time(ev1))
     kern_ms = max_over_ranks(ws, ms_p2g + ms_g2p)
@@ -283,6 +287,8 @@ def run_ours(args, ws, rank, local):
     flip256 = None
     if not args.skip_flip256:
         flip256 = flip256_bench()
+    # clocks sampled from the first timed FLIP step through the last timed region of this run
+    clocks = clk.stop() if clk else None
 
     if rank != 0:
         return

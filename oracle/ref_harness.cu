@@ -7,7 +7,7 @@
 //
 // The reference compiles its constants in: BLOCK_BASE_RES 16, MAX_LEVELS 3 (MSBG.cuh:4-5).
 // Calls are restricted to the inputs on which the reference is memory-safe and well defined:
-// single-level (or level-uniform) maps with every block active (SURVEY tier A).  The smoother
+// single-level (or level-uniform) maps with every block active (the reference-exact tier).  The smoother
 // is driven with one thread per CTA: smoothActiveBlocks' early exit is evaluated by thread 0
 // only (Smoother.cuh:183-185), so a 1-thread CTA is the launch shape in which that exit is
 // block-uniform and the kernel is free of the divergent barrier.
