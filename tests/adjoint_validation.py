@@ -1,5 +1,5 @@
 """Full-size validation of the GPU adjoint on the differentiable rollout (the dam_break_64 layout,
-dam_break_64 layout, 505,856 particles, 50 steps, checkpoints every 10).  Needs a GPU and the
+505,856 particles, 50 steps, checkpoints every 10).  Needs a GPU and the
 oracle; prints one JSON object (and writes it to --out when given).
 
   --mode along   GPU VJP (aw_vjp_rollout) against the FP64 adjoint evaluated along the GPU's own
