@@ -115,11 +115,13 @@ def barrier(ws):
 
 
 def max_over_ranks(ws, v):
+    """The largest of the ranks' values (device time of the slowest replica)."""
     if ws == 1:
         return v
     import torch
     import torch.distributed as dist
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
