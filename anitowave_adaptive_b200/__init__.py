@@ -124,6 +124,7 @@ SIGNATURES = {
     "aw_flip_stats_get": (C.c_int, [_VP, C.POINTER(FlipStats)]),
     "aw_flip_particles": (C.c_int, [_VP, _VP, _VP]),
     "aw_flip_solver": (C.c_int, [_VP, _PP]),
+    "aw_flip_rebuild_levels": (C.c_int, [_VP, C.POINTER(_I32), C.POINTER(_I32), _VP]),
     "aw_solver_precision": (C.c_int, [_VP, C.POINTER(_I32)]),
     "aw_project": (C.c_int, [_VP, _VP, _VP, _F, _VP]),
     "aw_vjp_project": (C.c_int, [_VP, _VP, _VP, _F, _PP, _VP]),
@@ -512,6 +513,13 @@ class Flip:
         s = FlipStats()
         check(lib().aw_flip_stats_get(self.h, C.byref(s)))
         return {k: getattr(s, k) for k, _ in FlipStats._fields_}
+
+    def rebuild_levels(self, thresholds, stream=None):
+        """Re-derive the level map from the current particles; True when the layout changed."""
+        th = (C.c_int32 * max(1, len(thresholds)))(*[int(t) for t in thresholds])
+        ch = C.c_int32()
+        check(lib().aw_flip_rebuild_levels(self.h, th, C.byref(ch), _stream(stream)))
+        return bool(ch.value)
 
     def particles(self):
         pos = np.zeros((self.n, 3), np.float32)

@@ -646,6 +646,7 @@ struct aw_flip {
     DBuf<uint32_t> ids[2];
     int cur = 0;
     aw_solver* solver = nullptr;
+    aw_solver_desc sd{};
     FlipBufs B;
     aw_flip_stats stats{};
     cudaEvent_t ev[8] = {};
@@ -689,6 +690,7 @@ extern "C" aw_status aw_flip_create(aw_msbg* g, const aw_flip_desc* d, const flo
     sd.precision = d->precision;
     sd.tolerance = d->tolerance;
     sd.max_cycles = d->max_cycles;
+    F->sd = sd;
     AW_TRY(aw_solver_create(g, &sd, &F->solver));
     AW_TRY(F->B.ensure(G));
     for (auto& e : F->ev) AW_CUDA(cudaEventCreate(&e));
@@ -715,6 +717,35 @@ extern "C" aw_status aw_flip_step(aw_flip* F, aw_stream s_) {
                                  F->ids[c ^ 1].p, F->n, nullptr, nullptr, F->ev, &F->stats, s);
     F->cur ^= 1;  // the sorted state lives in the other buffer from the gather on
     return st;
+}
+
+extern "C" aw_status aw_flip_rebuild_levels(aw_flip* F, const int32_t* h_thresholds, int32_t* changed, aw_stream s_) {
+    AW_CHECK_ARG(F, "null simulation");
+    cudaStream_t s = (cudaStream_t)s_;
+    MsbgState& G = F->g->st;
+    if (changed) *changed = 0;
+    const std::vector<uint32_t> old = G.h_level;
+    const float* soa = F->soa[F->cur].p;
+    AW_TRY(levels_from_positions(G, soa, 1, F->n, F->n, h_thresholds, s));
+    int32_t passes = 0;
+    AW_TRY(aw_msbg_enforce_grading(F->g, &passes, s_));
+    std::vector<uint32_t> now((size_t)G.nb);
+    AW_CUDA(cudaMemcpyAsync(now.data(), G.level.p, G.nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    AW_CUDA(cudaStreamSynchronize(s));
+    if (now == old) {  // same layout: keep the channels and the solver
+        G.allocated = true;
+        return AW_OK;
+    }
+    // a new layout: channels, tiles and the solver hierarchy follow it; the particles carry the state
+    if (F->solver) {
+        aw_solver_destroy(F->solver);
+        F->solver = nullptr;
+    }
+    AW_TRY(aw_msbg_allocate(F->g, s_));
+    AW_TRY(aw_solver_create(F->g, &F->sd, &F->solver));
+    AW_TRY(F->B.ensure(G));
+    if (changed) *changed = 1;
+    return AW_OK;
 }
 
 extern "C" aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out) {

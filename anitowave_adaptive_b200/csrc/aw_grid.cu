@@ -141,7 +141,8 @@ __global__ void k_block_info(Geo g, uint32_t* out) {
 }
 
 // finest-cell occupancy from particles (one byte per finest cell)
-__global__ void k_occupancy(Geo g, const float* __restrict__ pos, int64_t n, uint8_t* occ) {
+// pos: element (i, a) at pos[i * si + a * sa] (AoS: si = 3, sa = 1; SoA: si = 1, sa = n)
+__global__ void k_occupancy(Geo g, const float* __restrict__ pos, int64_t si, int64_t sa, int64_t n, uint8_t* occ) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float h0 = __fdiv_rn(g.bs, (float)g.R0);
@@ -149,7 +150,7 @@ __global__ void k_occupancy(Geo g, const float* __restrict__ pos, int64_t n, uin
     int q[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        float rel = __fsub_rn(pos[3 * i + a], g.dmin[a]);
+        float rel = __fsub_rn(pos[i * si + a * sa], g.dmin[a]);
         int v = (int)floorf(__fdiv_rn(rel, h0));
         q[a] = min(max(v, 0), N[a] - 1);
     }
@@ -429,11 +430,9 @@ extern "C" aw_status aw_msbg_block_info(aw_msbg* g, uint32_t* d_out, aw_stream s
     return AW_OK;
 }
 
-extern "C" aw_status aw_msbg_levels_from_particles(aw_msbg* g, const float* d_pos, int64_t n,
-                                                   const int32_t* thresholds, aw_stream s_) {
-    AW_CHECK_ARG(g && (d_pos || n == 0), "null argument");
-    MsbgState& G = g->st;
-    cudaStream_t s = (cudaStream_t)s_;
+namespace aw {
+aw_status levels_from_positions(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
+                                const int32_t* thresholds, cudaStream_t s) {
     Thresh th{};
     for (int t = 0; t < G.geo.L - 1; ++t) {
         AW_CHECK_ARG(thresholds, "thresholds required when num_levels > 1");
@@ -444,7 +443,7 @@ extern "C" aw_status aw_msbg_levels_from_particles(aw_msbg* g, const float* d_po
     AW_TRY(G.occ.ensure(ncell + G.nb));
     AW_CUDA(cudaMemsetAsync(G.occ.p, 0, ncell + G.nb, s));
     if (n > 0) {
-        k_occupancy<<<nblk(n), 256, 0, s>>>(G.geo, d_pos, n, G.occ.p);
+        k_occupancy<<<nblk(n), 256, 0, s>>>(G.geo, d_pos, si, sa, n, G.occ.p);
         AW_LAUNCH();
     }
     k_block_surface<<<G.nb, 256, 0, s>>>(G.geo, G.occ.p, G.occ.p + ncell);
@@ -453,6 +452,13 @@ extern "C" aw_status aw_msbg_levels_from_particles(aw_msbg* g, const float* d_po
     AW_LAUNCH();
     G.allocated = false;
     return AW_OK;
+}
+}  // namespace aw
+
+extern "C" aw_status aw_msbg_levels_from_particles(aw_msbg* g, const float* d_pos, int64_t n,
+                                                   const int32_t* thresholds, aw_stream s_) {
+    AW_CHECK_ARG(g && (d_pos || n == 0), "null argument");
+    return levels_from_positions(g->st, d_pos, 3, 1, n, thresholds, (cudaStream_t)s_);
 }
 
 extern "C" aw_status aw_msbg_enforce_grading(aw_msbg* g, int32_t* passes, aw_stream s_) {

@@ -227,6 +227,11 @@ struct MsbgState {
     }
 };
 
+// Level map from particle positions (element (i, a) at pos[i * si + a * sa]) into G.level; marks the
+// grid unallocated.
+aw_status levels_from_positions(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
+                                const int32_t* thresholds, cudaStream_t s);
+
 // Exclusive scan of n u32 values into out[0..n] (out[n] = total).  tmp: scan scratch.
 aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<uint32_t>& tmp, cudaStream_t s);
 

@@ -258,6 +258,14 @@ aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out);
 /* copy particle state to host in the original particle order (AoS) */
 aw_status aw_flip_particles(aw_flip* f, float* h_pos, float* h_vel);
 aw_status aw_flip_solver(aw_flip* f, aw_solver** out);
+/* Between steps: rebuild the level map from the simulation's current particle positions (the rule
+ * of aw_msbg_levels_from_particles with these thresholds, then aw_msbg_enforce_grading).  When the
+ * map changed, the grid is laid out again (aw_msbg_allocate) and the solver hierarchy rebuilt;
+ * channel pointers and solver handles obtained before are then stale.  No grid state needs
+ * remapping: P2G regenerates it from the particles every step.  *changed (optional) = 1 when the
+ * layout changed.  syncs.  No counterpart in the reference (markActiveBlocks + grading +
+ * allocateChannels were a one-time setup there, main.cu:154-278). */
+aw_status aw_flip_rebuild_levels(aw_flip* f, const int32_t* h_thresholds, int32_t* changed, aw_stream s);
 
 /* ---- projection and adjoints (no counterpart in the reference) ------------------------------
  * The vector-Jacobian products differentiate the forward calls with their discrete decisions

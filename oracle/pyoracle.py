@@ -238,12 +238,46 @@ class Oracle:
     def coarsest(self):
         lib().oc_coarsest(self.h)
 
-    def solve(self, b, tol=1e-6, max_cycles=100, p0=None):
+    def solve(self, b, tol=1e-6, max_cycles=100, p0=None, method="dc"):
+        """FP64 solve of A p = b on level 0.  method "dc": V-cycle defect correction (oc_solve);
+        "pcg": conjugate gradients preconditioned by the same V-cycle (the library's mixed-precision
+        outer loop)."""
         n = int(self.level_info(0)[4])
         p = np.zeros(n) if p0 is None else np.ascontiguousarray(p0, np.float64).copy()
+        b = np.ascontiguousarray(b, np.float64)
+        if method == "pcg":
+            return self._pcg(b, p, tol, max_cycles)
         hist = np.zeros(max_cycles + 1)
-        it = lib().oc_solve(self.h, p, np.ascontiguousarray(b, np.float64), tol, max_cycles, hist.ctypes.data)
+        it = lib().oc_solve(self.h, p, b, tol, max_cycles, hist.ctypes.data)
         return p, hist[: it + 1]
+
+    def _pcg(self, b, p, tol, max_cycles):
+        fl = self.get(0, 6) != 0
+        n = p.size
+
+        def V(r):
+            self.set(0, 1, r)
+            self.set(0, 0, np.zeros(n))
+            self.vcycle()
+            return self.get(0, 0)
+
+        bn = np.linalg.norm(b * fl) or 1.0
+        r = (b - self.apply(0, p)) * fl
+        hist = [np.linalg.norm(r) / bn]
+        z = V(r) * fl
+        d = z.copy()
+        rho = r @ z
+        while hist[-1] >= tol and len(hist) <= max_cycles:
+            q = self.apply(0, d) * fl
+            alpha = rho / (d @ q)
+            p += alpha * d
+            r -= alpha * q
+            hist.append(np.linalg.norm(r) / bn)
+            z = V(r) * fl
+            rn = r @ z
+            d = z + (rn / rho) * d
+            rho = rn
+        return p, np.array(hist)
 
     def apply(self, m, x):
         y = np.zeros_like(np.ascontiguousarray(x, np.float64))
@@ -374,7 +408,7 @@ class Oracle:
         return out
 
 
-def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=200):
+def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=200, method="dc"):
     """One FLIP step of the FP64 restatement, in the order the GPU step runs: sort -> P2G ->
     T-junction sync -> backup -> gravity -> walls -> divergence -> solve -> gradient -> sync ->
     walls -> G2P -> RK3.  Returns (pos, vel) in sorted order, the sort permutation and details."""
@@ -392,7 +426,7 @@ def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=2
     b = O.divergence(u, fluid, dt)
     O.set_params(mode=0)
     O.build(fluid=fluid)
-    p, hist = O.solve(b, tol=tol, max_cycles=max_cycles)
+    p, hist = O.solve(b, tol=tol, max_cycles=max_cycles, method=method)
     un = O.gradient_update(p, dt, u)
     un = O.wall_bc(O.face_sync(un))
     vnew = O.g2p(ps, un, uo, alpha, vs)
