@@ -233,3 +233,26 @@ def test_closed_box_poisson_converges():
     p, hist = O.solve(b, tol=1e-10, max_cycles=40)
     assert hist[-1] < 1e-10
     assert len(hist) <= 15
+
+
+def test_pcg_and_defect_correction_agree():
+    """The oracle's two FP64 solves (V-cycle defect correction and V-cycle-preconditioned CG) reach
+    the same pressure on a free-surface layout."""
+    from anitowave_adaptive_b200 import scenes
+    from oracle import pyoracle as po
+
+    S = scenes.config("dam_break_16")
+    lv = po.levels_from_particles(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, S.pos, S.thresholds)
+    lv, _ = po.enforce_grading(S.dims, S.num_levels, lv)
+    O = po.Oracle(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, lv)
+    _, _, cnt = O.p2g(S.pos, S.vel)
+    fluid = (cnt > 0).astype(np.uint8)
+    rng = np.random.default_rng(1)
+    b = rng.standard_normal(int(O.tot0[0])) * fluid
+    O.set_params(mode=0)
+    O.build(fluid=fluid)
+    p1, h1 = O.solve(b, tol=1e-12, max_cycles=200)
+    p2, h2 = O.solve(b, tol=1e-12, max_cycles=200, method="pcg")
+    assert h1[-1] < 1e-12 and h2[-1] < 1e-12
+    assert len(h2) <= len(h1)
+    assert np.linalg.norm((p1 - p2) * fluid) <= 1e-9 * np.linalg.norm(p1 * fluid)
