@@ -804,17 +804,29 @@ __global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__
 }
 // qn = -A d (the residual kernel with a zero right-hand side); alpha = rho / (d . A d)
 // p += alpha d; r += alpha qn; and the FP32 copy of r for the next V-cycle
+// ... and the per-CTA partial sums of |r|^2 over fluid cells (grid-stride, part[blockIdx.x])
 __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, float* __restrict__ rf,
                             const double* __restrict__ d, const double* __restrict__ qn, const double* __restrict__ sc,
-                            size_t n) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+                            const uint8_t* __restrict__ fluid, size_t n, double* __restrict__ part) {
     const double dq = -sc[2];
     const double alpha = dq != 0.0 ? sc[0] / dq : 0.0;
-    p[i] += alpha * d[i];
-    const double rv = r[i] + alpha * qn[i];
-    r[i] = rv;
-    rf[i] = (float)rv;
+    double acc = 0.0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        p[i] += alpha * d[i];
+        const double rv = r[i] + alpha * qn[i];
+        r[i] = rv;
+        rf[i] = (float)rv;
+        if (fluid[i]) acc += rv * rv;
+    }
+    __shared__ double red[32];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+        t = warp_sum(t);
+        if (threadIdx.x == 0) part[blockIdx.x] = t;
+    }
 }
 __global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
 
@@ -1929,7 +1941,13 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
         // cycle converges on every configuration.  One host read (||r||) per iteration.
         double* p = (double*)d_p;
         double* sc = S->cg_sc.p;
-        const unsigned ndot = 256;
+        // reductions over the level-0 cells: 8 CTAs per SM, grid-stride
+        int nsm = 148;
+        {
+            int dev = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        }
+        const unsigned ndot = (unsigned)std::min<size_t>((size_t)nsm * 8, S->partials.n);
         auto launch_err = [&](const char* what) -> aw_status {
             ++g_launches;
             cudaError_t e = cudaGetLastError();
@@ -1982,16 +2000,14 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
             k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, ndot, sc + 2);
             if ((st = launch_err("k_reduce_sum")) != AW_OK) break;
             // p += alpha d ; r -= alpha A d ; FP32 copy of r for the next V-cycle ; rho_old = rho
-            k_cg_update<<<nblk(nc), 256, 0, s>>>(p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, nc);
+            k_cg_update<<<ndot, 256, 0, s>>>(p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, L0.fluid.p, nc,
+                                             S->partials.p);
             if ((st = launch_err("k_cg_update")) != AW_OK) break;
             k_copy_scalar<<<1, 1, 0, s>>>(sc, 1, 0);
             if ((st = launch_err("k_copy_scalar")) != AW_OK) break;
             ++it;
             restart = false;
-            // ||r||
-            k_dot64<<<ndot, 256, 0, s>>>(S->cg_r.p, S->cg_r.p, nullptr, L0.fluid.p, nc, S->partials.p);
-            if ((st = launch_err("k_dot64")) != AW_OK) break;
-            st = read_norm(S, ndot, s, &rn);
+            st = read_norm(S, ndot, s, &rn);  // ||r|| from k_cg_update's partial sums
         }
     }
     if (cycles) *cycles = it;
