@@ -270,8 +270,10 @@ __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, f
 // The flush adds every nonzero tile entry into each copy of that physical face held by a block of
 // b's resolution (a face on a block boundary has one copy per side).  Faces of
 // neighbours at another resolution are at other positions: particles within reach of such a
-// neighbour add their weights in the neighbour's own lattice with global float atomics.  A second
-// kernel normalises u = P / m.  The face arrays must start at zero.
+// neighbour add their weights in the neighbour's own lattice with global float atomics.  Those
+// (particle, neighbour) pairs are queued per warp and run one pair per lane, so a warp does not
+// pass over every neighbour direction with most lanes idle.  A second kernel normalises
+// u = P / m.  The face arrays must start at zero.
 // ------------------------------------------------------------------------------------------------
 __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
@@ -317,11 +319,31 @@ struct FaceAcc {
     float* P[3];
 };
 
-__global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
+constexpr int P2G_THREADS = 256;
+constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
+
+// one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
+__device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[3], const int* nres, uint32_t v, int d,
+                                               uint32_t p0, const float* __restrict__ soa, int64_t n,
+                                               const FaceAcc& acc) {
+    const uint32_t sidx = p0 + v;
+    float X[3], V[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        X[k] = soa[(int64_t)k * n + sidx];
+        V[k] = soa[(int64_t)(3 + k) * n + sidx];
+    }
+    const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
+    p2g_cross(L, bidx(L.g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, acc.m, acc.P);
+}
+
+__global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ int cross;
+    __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
+    __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
@@ -356,69 +378,104 @@ __global__ void __launch_bounds__(256) k_p2g_own(LevelView L, const float* __res
     const uint32_t T = p1 - p0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t Ls = (T + 31) / 32;
+    // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32 at
+    // a time, one pair per lane, instead of one divergent pass per neighbour direction
+    uint32_t* qv = xq_v + w * P2G_XQ;
+    uint8_t* qd = xq_d + w * P2G_XQ;
+    int qn = 0;
     for (uint32_t i = w; i < Ls; i += nw) {
         const uint32_t v = lane * Ls + i;
-        if (v >= T) break;
-        const uint32_t sidx = p0 + v;
+        const bool valid = v < T;
         float X[3], V[3], q[3];
+        if (valid) {
+            const uint32_t sidx = p0 + v;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            X[k] = soa[(int64_t)k * n + sidx];
-            V[k] = soa[(int64_t)(3 + k) * n + sidx];
-            q[k] = (X[k] - o[k]) * invh;
-        }
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-            const int ia = min(max((int)floorf(q[a]), 0), r - 1);
-            const int j1 = min(max((int)floorf(q[t1] - 0.5f), -1), r - 1);
-            const int j2 = min(max((int)floorf(q[t2] - 0.5f), -1), r - 1);
-            float dA2[2], dB2[2], dC2[2];
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const float dA = q[a] - (float)(ia + k);
-                const float dB = q[t1] - ((float)(j1 + k) + 0.5f);
-                const float dC = q[t2] - ((float)(j2 + k) + 0.5f);
-                dA2[k] = dA * dA;
-                dB2[k] = dB * dB;
-                dC2[k] = dC * dC;
+            for (int k = 0; k < 3; ++k) {
+                X[k] = soa[(int64_t)k * n + sidx];
+                V[k] = soa[(int64_t)(3 + k) * n + sidx];
+                q[k] = (X[k] - o[k]) * invh;
             }
-            const int base = a * TA + ia + R1 * ((j1 + 1) + R2 * (j2 + 1));
-            const float va = V[a];
 #pragma unroll
-            for (int da = 0; da < 2; ++da)
+            for (int a = 0; a < 3; ++a) {
+                const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+                const int ia = min(max((int)floorf(q[a]), 0), r - 1);
+                const int j1 = min(max((int)floorf(q[t1] - 0.5f), -1), r - 1);
+                const int j2 = min(max((int)floorf(q[t2] - 0.5f), -1), r - 1);
+                float dA2[2], dB2[2], dC2[2];
 #pragma unroll
-                for (int d1 = 0; d1 < 2; ++d1) {
-                    const float dAB = dA2[da] + dB2[d1];
+                for (int k = 0; k < 2; ++k) {
+                    const float dA = q[a] - (float)(ia + k);
+                    const float dB = q[t1] - ((float)(j1 + k) + 0.5f);
+                    const float dC = q[t2] - ((float)(j2 + k) + 0.5f);
+                    dA2[k] = dA * dA;
+                    dB2[k] = dB * dB;
+                    dC2[k] = dC * dC;
+                }
+                const int base = a * TA + ia + R1 * ((j1 + 1) + R2 * (j2 + 1));
+                const float va = V[a];
 #pragma unroll
-                    for (int d2 = 0; d2 < 2; ++d2) {
-                        const float tt = 1.f - (dAB + dC2[d2]);
-                        const float wgt = tt * tt * tt;
-                        const int e = base + da + d1 * R1 + d2 * R1 * R2;
-                        if (tt > 0.f) {
-                            atomicAdd(&am[e], wgt);
-                            atomicAdd(&ap[e], wgt * va);
+                for (int da = 0; da < 2; ++da)
+#pragma unroll
+                    for (int d1 = 0; d1 < 2; ++d1) {
+                        const float dAB = dA2[da] + dB2[d1];
+#pragma unroll
+                        for (int d2 = 0; d2 < 2; ++d2) {
+                            const float tt = 1.f - (dAB + dC2[d2]);
+                            const float wgt = tt * tt * tt;
+                            const int e = base + da + d1 * R1 + d2 * R1 * R2;
+                            if (tt > 0.f) {
+                                atomicAdd(&am[e], wgt);
+                                atomicAdd(&ap[e], wgt * va);
+                            }
                         }
                     }
-                }
+            }
         }
         if (xmask) {
             // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
-#pragma unroll 1
-            for (int d = 0; d < 27; ++d) {
-                if (!((xmask >> d) & 1)) continue;
-                const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                const float reach = nres[d] < r ? 2.f : 1.f;
-                bool near = true;
+            uint32_t near = 0;
+            if (valid) {
+                for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
+                    const int d = __ffs(mm) - 1;
+                    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+                    const float reach = nres[d] < r ? 2.f : 1.f;
+                    bool nr = true;
 #pragma unroll
-                for (int k = 0; k < 3; ++k)
-                    near = near && (dd[k] == 0 || (dd[k] < 0 ? q[k] < reach : q[k] > (float)r - reach));
-                if (!near) continue;
-                const int nc[3] = {cb[0] + dd[0], cb[1] + dd[1], cb[2] + dd[2]};
-                p2g_cross(L, bidx(g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, acc.m, acc.P);
+                    for (int k = 0; k < 3; ++k)
+                        nr = nr && (dd[k] == 0 || (dd[k] < 0 ? q[k] < reach : q[k] > (float)r - reach));
+                    if (nr) near |= 1u << d;
+                }
+            }
+            // at most two pairs per lane per round keeps the queue within 31 + 64 entries
+            while (__any_sync(0xffffffffu, near)) {
+                const uint32_t b1 = near & (0u - near);
+                const uint32_t r1 = near & ~b1;
+                const uint32_t take = b1 | (r1 & (0u - r1));
+                near &= ~take;
+                const int cnt = __popc(take);
+                int incl = cnt;
+#pragma unroll
+                for (int sh = 1; sh < 32; sh <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                    if (lane >= sh) incl += y;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                int slot = qn + incl - cnt;
+                for (uint32_t mm = take; mm; mm &= mm - 1, ++slot) {
+                    qv[slot] = v;
+                    qd[slot] = (uint8_t)(__ffs(mm) - 1);
+                }
+                qn += total;
+                __syncwarp();
+                while (qn >= 32) {
+                    qn -= 32;
+                    p2g_cross_pair(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc);
+                    __syncwarp();
+                }
             }
         }
     }
+    if (qn > 0 && lane < qn) p2g_cross_pair(L, cb, nres, qv[lane], qd[lane], p0, soa, n, acc);
     __syncthreads();
     // flush: every nonzero tile entry into each same-resolution copy of its face
 #pragma unroll
@@ -494,7 +551,7 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     const size_t smem = (size_t)6 * tile_axis(maxres) * sizeof(float);
     if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_own, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (n > 0) {
-        k_p2g_own<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cstart, acc);
+        k_p2g_own<<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc);
         AW_LAUNCH();
     }
     const uint64_t nf = (uint64_t)G.tot[1] + G.tot[2] + G.tot[3];
