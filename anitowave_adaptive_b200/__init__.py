@@ -29,6 +29,7 @@ STATUS = {0: "AW_OK", 1: "AW_ERR_INVALID_ARGUMENT", 2: "AW_ERR_CUDA", 3: "AW_ERR
 
 # channels (MSBG.cuh:12-50)
 VELOCITY_X, VELOCITY_Y, VELOCITY_Z, PRESSURE = 0, 1, 2, 3
+PHASE_FIELD_X, PHASE_FIELD_Y, PHASE_FIELD_Z = 4, 5, 6
 BETA_COEFF_X, BETA_COEFF_Y, BETA_COEFF_Z = 7, 8, 9
 MASS_DENSITY_X, MASS_DENSITY_Y, MASS_DENSITY_Z = 10, 11, 12
 MOMENTUM_X, MOMENTUM_Y, MOMENTUM_Z = 13, 14, 15
@@ -93,6 +94,7 @@ SIGNATURES = {
     "aw_msbg_channel": (C.c_int, [_VP, _I32, _PP, C.POINTER(_U32)]),
     "aw_msbg_run_galerkin": (C.c_int, [_VP, _PP, _PP, _I32, _VP]),
     "aw_p2g": (C.c_int, [_VP, _VP, _VP, _I64, _VP]),
+    "aw_p2g_phase": (C.c_int, [_VP, _VP, _VP, _VP, _I64, _F, _F, _VP]),
     "aw_backup_grid_velocity": (C.c_int, [_VP, _VP]),
     "aw_g2p": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
     "aw_g2p_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
@@ -109,6 +111,7 @@ SIGNATURES = {
     "aw_solver_create": (C.c_int, [_VP, C.POINTER(SolverDesc), _PP]),
     "aw_solver_destroy": (C.c_int, [_VP]),
     "aw_solver_setup": (C.c_int, [_VP, _VP, _VP]),
+    "aw_solver_update_coefficients": (C.c_int, [_VP, _VP]),
     "aw_solver_num_levels": (C.c_int, [_VP, C.POINTER(_I32)]),
     "aw_solver_level_array": (C.c_int, [_VP, _I32, _I32, _PP, C.POINTER(_U32)]),
     "aw_smoother_solve_level": (C.c_int, [_VP, _I32, _I32, _VP]),
@@ -125,6 +128,7 @@ SIGNATURES = {
     "aw_flip_particles": (C.c_int, [_VP, _VP, _VP]),
     "aw_flip_solver": (C.c_int, [_VP, _PP]),
     "aw_flip_rebuild_levels": (C.c_int, [_VP, C.POINTER(_I32), C.POINTER(_I32), _VP]),
+    "aw_flip_set_phase": (C.c_int, [_VP, _VP, _F, _F]),
     "aw_solver_precision": (C.c_int, [_VP, C.POINTER(_I32)]),
     "aw_project": (C.c_int, [_VP, _VP, _VP, _F, _VP]),
     "aw_vjp_project": (C.c_int, [_VP, _VP, _VP, _F, _PP, _VP]),
@@ -311,6 +315,11 @@ class MSBG:
     def p2g(self, pos, vel, stream=None):
         check(lib().aw_p2g(self.h, _ptr(pos), _ptr(vel), int(pos.shape[0]), _stream(stream)))
 
+    def p2g_phase(self, pos, vel, phase, rho0, rho1, stream=None):
+        """p2g plus PHASE_FIELD_* and BETA_COEFF_* = 1/rho from per-particle phases in [0,1]."""
+        check(lib().aw_p2g_phase(self.h, _ptr(pos), _ptr(vel), _ptr(phase), int(pos.shape[0]), float(rho0),
+                                 float(rho1), _stream(stream)))
+
     def backup_grid_velocity(self, stream=None):
         check(lib().aw_backup_grid_velocity(self.h, _stream(stream)))
 
@@ -436,6 +445,10 @@ class Solver:
     def setup(self, fluid=None, stream=None):
         check(lib().aw_solver_setup(self.h, _ptr(fluid), _stream(stream)))
 
+    def update_coefficients(self, stream=None):
+        """Rebuild every level's coefficients from the grid's current BETA_COEFF_*."""
+        check(lib().aw_solver_update_coefficients(self.h, _stream(stream)))
+
     def num_levels(self):
         n = C.c_int32()
         check(lib().aw_solver_num_levels(self.h, C.byref(n)))
@@ -520,6 +533,16 @@ class Flip:
         ch = C.c_int32()
         check(lib().aw_flip_rebuild_levels(self.h, th, C.byref(ch), _stream(stream)))
         return bool(ch.value)
+
+    def set_phase(self, phase=None, rho0=1.0, rho1=1.0):
+        """Two-phase simulation: phase[i] in [0,1] per particle (original order); None = one phase."""
+        if phase is None:
+            check(lib().aw_flip_set_phase(self.h, None, 1.0, 1.0))
+            return
+        ph = np.ascontiguousarray(phase, np.float32).reshape(-1)
+        if ph.shape[0] != self.n:
+            raise ValueError("one phase per particle")
+        check(lib().aw_flip_set_phase(self.h, ph.ctypes.data, float(rho0), float(rho1)))
 
     def particles(self):
         pos = np.zeros((self.n, 3), np.float32)

@@ -53,6 +53,56 @@ __global__ void k_face_sync(LevelView L, float* u0, float* u1, float* u2) {
     }
 }
 
+// Coefficient sync at T-junctions: the coarse face and the 4 fine faces it covers all take the
+// mean of the 4 fine values.  The fine cell's flux uses its own face's coefficient and the coarse
+// cell's flux uses the coarse face's, so equal values on both sides keep A symmetric.  Only the
+// coarse block writes these faces.
+__global__ void k_beta_sync(LevelView L, float* b0, float* b1, float* b2) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    float* B[3] = {b0, b1, b2};
+#pragma unroll 1
+    for (int dir = 0; dir < 6; ++dir) {
+        const int a = dir >> 1, s = (dir & 1) ? 1 : -1;
+        int nc[3] = {cb[0], cb[1], cb[2]};
+        nc[a] += s;
+        if (!inside(L.g, nc)) continue;
+        const int n = bidx(L.g, nc[0], nc[1], nc[2]);
+        const int rn = L.res[n];
+        if (rn != 2 * r) continue;
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int i = threadIdx.x; i < r * r; i += blockDim.x) {
+            const int u1 = i % r, u2 = i / r;
+            uint32_t fine[4];
+            float sum = 0.f;
+            for (int d1 = 0; d1 < 2; ++d1)
+                for (int d2 = 0; d2 < 2; ++d2) {
+                    int q[3];
+                    q[a] = s > 0 ? 0 : rn;
+                    q[t1] = 2 * u1 + d1;
+                    q[t2] = 2 * u2 + d2;
+                    fine[2 * d1 + d2] = L.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn);
+                    sum += B[a][fine[2 * d1 + d2]];
+                }
+            const float v = 0.25f * sum;
+            for (int k = 0; k < 4; ++k) B[a][fine[k]] = v;
+            int f[3];
+            f[a] = s > 0 ? r : 0;
+            f[t1] = u1;
+            f[t2] = u2;
+            B[a][L.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r)] = v;
+        }
+    }
+}
+
+__global__ void k_fill(float* u, size_t n, float v) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) u[i] = v;
+}
+
 __global__ void k_add_const(float* u, size_t n, float v) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) u[i] += v;
@@ -420,6 +470,12 @@ aw_status wall_bc(MsbgState& G, float* u[3], cudaStream_t s) {
     AW_LAUNCH();
     return AW_OK;
 }
+aw_status beta_sync(MsbgState& G, float* beta[3], cudaStream_t s) {
+    k_beta_sync<<<G.nb, 64, 0, s>>>(G.view0(), beta[0], beta[1], beta[2]);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 aw_status face_sync_vjp(MsbgState& G, float* ubar[3], cudaStream_t s) {
     k_face_sync_vjp<<<G.nb, 64, 0, s>>>(G.view0(), ubar[0], ubar[1], ubar[2]);
     AW_LAUNCH();
@@ -520,7 +576,8 @@ static aw_status copy_d2d(void* dst, const void* src, size_t bytes, cudaStream_t
 
 aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
                         const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
-                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s) {
+                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s, const FlipPhase* fp) {
+    if (fp && !ids_out) return set_error(AW_ERR_INVALID_ARGUMENT, "two-phase step needs particle ids");
     float* U[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     float* UO[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
     float* Mm[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
@@ -538,7 +595,18 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
     if (ev) AW_CUDA(cudaEventRecord(ev[1], s));
     // 2. P2G (+ normalise) and fluid flags
     float* nomom[3] = {nullptr, nullptr, nullptr};
-    AW_TRY(p2g_sorted(G, soa_out, n, G.pw.cell_start.p, U, Mm, nomom, nullptr, s));
+    PhaseIn pin{};
+    if (fp) {
+        pin.pid = ids_out;
+        pin.phase = fp->phase;
+        pin.rho0 = fp->rho0;
+        pin.rho1 = fp->rho1;
+        for (int a = 0; a < 3; ++a) {
+            pin.phi[a] = G.ch[AW_PHASE_FIELD_X + a];
+            pin.beta[a] = G.ch[AW_BETA_COEFF_X + a];
+        }
+    }
+    AW_TRY(p2g_sorted(G, soa_out, n, G.pw.cell_start.p, U, Mm, nomom, nullptr, s, fp ? &pin : nullptr));
     if (ev) AW_CUDA(cudaEventRecord(ev[2], s));
     k_fluid_from_count<<<nblk(G.tot[0]), 256, 0, s>>>(G.pw.cell_start.p, G.tot[0], B.fluid.p, G.ch[AW_CELL_TYPE]);
     AW_LAUNCH();
@@ -564,7 +632,11 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
     k_divergence<<<G.nb, 128, 0, s>>>(G.view0(), U[0], U[1], U[2], B.fluid.p, 1.f / d.dt, B.rhs.p, B.divmax.p);
     AW_LAUNCH();
     if (ev) AW_CUDA(cudaEventRecord(ev[3], s));
-    // 5. projection
+    // 5. projection (two-phase: coefficients from this step's beta first)
+    if (fp) {
+        AW_TRY(beta_sync(G, pin.beta, s));
+        AW_TRY(aw_solver_update_coefficients(solver, (aw_stream)s));
+    }
     AW_TRY(aw_solver_setup(solver, B.fluid.p, (aw_stream)s));
     void* p;
     if (d.precision == AW_PRECISION_MIXED) {
@@ -648,6 +720,8 @@ struct aw_flip {
     aw_solver* solver = nullptr;
     aw_solver_desc sd{};
     FlipBufs B;
+    DBuf<float> phase;  // two-phase: phase by particle id (empty = one phase)
+    float rho0 = 1.f, rho1 = 1.f;
     aw_flip_stats stats{};
     cudaEvent_t ev[8] = {};
     ~aw_flip() {
@@ -698,6 +772,31 @@ extern "C" aw_status aw_flip_create(aw_msbg* g, const aw_flip_desc* d, const flo
     return AW_OK;
 }
 
+extern "C" aw_status aw_flip_set_phase(aw_flip* F, const float* h_phase, float rho0, float rho1) {
+    AW_CHECK_ARG(F, "null simulation");
+    if (!h_phase) {
+        F->phase.free();
+        F->rho0 = F->rho1 = 1.f;
+        MsbgState& G = F->g->st;
+        for (int a = 0; a < 3; ++a)
+            if (G.tot[1 + a]) {
+                k_fill<<<nblk(G.tot[1 + a]), 256>>>(G.ch[AW_BETA_COEFF_X + a], G.tot[1 + a], 1.f);
+                AW_LAUNCH();
+            }
+        AW_TRY(aw_solver_update_coefficients(F->solver, 0));
+        AW_CUDA(cudaStreamSynchronize(0));
+        return AW_OK;
+    }
+    AW_CHECK_ARG(std::isfinite(rho0) && std::isfinite(rho1) && rho0 > 0.f && rho1 > 0.f, "densities must be positive");
+    for (int64_t i = 0; i < F->n; ++i)
+        AW_CHECK_ARG(h_phase[i] >= 0.f && h_phase[i] <= 1.f, "phase must lie in [0, 1]");
+    AW_TRY(F->phase.alloc((size_t)std::max<int64_t>(F->n, 1)));
+    if (F->n) AW_CUDA(cudaMemcpy(F->phase.p, h_phase, (size_t)F->n * sizeof(float), cudaMemcpyHostToDevice));
+    F->rho0 = rho0;
+    F->rho1 = rho1;
+    return AW_OK;
+}
+
 extern "C" aw_status aw_flip_destroy(aw_flip* f) {
     delete f;
     return AW_OK;
@@ -713,8 +812,10 @@ extern "C" aw_status aw_flip_step(aw_flip* F, aw_stream s_) {
     AW_CHECK_ARG(F, "null simulation");
     cudaStream_t s = (cudaStream_t)s_;
     const int c = F->cur;
+    const FlipPhase fp{F->phase.p, F->rho0, F->rho1};
     aw_status st = flip_step_soa(F->g->st, F->solver, F->d, F->B, F->soa[c].p, F->ids[c].p, F->soa[c ^ 1].p,
-                                 F->ids[c ^ 1].p, F->n, nullptr, nullptr, F->ev, &F->stats, s);
+                                 F->ids[c ^ 1].p, F->n, nullptr, nullptr, F->ev, &F->stats, s,
+                                 F->phase.p ? &fp : nullptr);
     F->cur ^= 1;  // the sorted state lives in the other buffer from the gather on
     return st;
 }

@@ -213,6 +213,7 @@ struct MsbgState {
     DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for
+    DBuf<float> p2g_Phi[3];                     // P2G phase accumulator (two-phase P2G)
     FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
     DBuf<int> err;  // device error flags: [1] bulk-copy wait timeout in G2P / advection ([0] unused)
     DBuf<uint8_t> occ;
@@ -237,8 +238,20 @@ aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<u
 
 // Particle pipeline (aw_particles.cu)
 aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s);
+// Two-phase input of P2G: sorted particle i has phase phase[pid[i]] in [0,1]; the face phase goes to
+// phi[3] and 1 / ((1 - phi) rho0 + phi rho1) to beta[3].
+struct PhaseIn {
+    const uint32_t* pid;
+    const float* phase;
+    float rho0, rho1;
+    float* phi[3];
+    float* beta[3];
+};
 aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* cell_start, float* u[3], float* m[3],
-                     float* mom[3], float* cell_count, cudaStream_t s);
+                     float* mom[3], float* cell_count, cudaStream_t s, const PhaseIn* ph = nullptr);
+// beta at T-junctions: the coarse face and the 4 fine faces it covers all take the mean of the
+// 4 fine values, which keeps the finite-volume operator symmetric for variable coefficients
+aw_status beta_sync(MsbgState& G, float* beta[3], cudaStream_t s);
 aw_status g2p_launch(MsbgState& G, const float* pos, int pos_stride_soa, float* vel, int vel_soa, int64_t n,
                      float alpha, const float* un[3], const float* uo[3], cudaStream_t s);
 aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float alpha, const float* un[3],
@@ -308,9 +321,17 @@ struct StepRecord {
 // soa_in/ids_in: state in any order; soa_out/ids_out: the stepped state, sorted by cell.
 // fluid_in (optional) replaces the fluid flags derived from the particle counts.  ev (optional,
 // 8 events) and st (optional) receive phase timings and solver statistics; st syncs the stream.
+// Two-phase state of a simulation: phase in [0,1] indexed by particle id, and the two densities.
+struct FlipPhase {
+    const float* phase;
+    float rho0, rho1;
+};
+// fp (optional, needs ids): P2G also writes PHASE_FIELD_* and BETA_COEFF_*, and the solver's
+// coefficients are rebuilt from them before the projection.
 aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
                         const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
-                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s);
+                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s,
+                        const FlipPhase* fp = nullptr);
 
 }  // namespace aw
 

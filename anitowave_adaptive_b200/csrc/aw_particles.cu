@@ -221,37 +221,6 @@ aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_so
     return AW_OK;
 }
 
-// ------------------------------------------------------------------------------------------------
-// P2G — gather form.  One CTA per block; each thread computes whole faces: the face sums
-// w = (1 - d^2/h^2)^3 over every particle within h (h = the face's own cell size), walking the
-// level-0 cells of every block that the support box touches.  No atomics: each face copy is
-// written once, with mass, momentum and velocity (normalizeVelocity fused).
-// ------------------------------------------------------------------------------------------------
-__device__ inline void face_coords(int a, int fi, int r, int f[3]) {
-    if (a == 0) {
-        f[0] = fi % (r + 1);
-        int rem = fi / (r + 1);
-        f[1] = rem % r;
-        f[2] = rem / r;
-    } else if (a == 1) {
-        f[0] = fi % r;
-        int rem = fi / r;
-        f[1] = rem % (r + 1);
-        f[2] = rem / (r + 1);
-    } else {
-        f[0] = fi % r;
-        int rem = fi / r;
-        f[1] = rem % r;
-        f[2] = rem / r;
-    }
-}
-
-struct FaceOut {
-    float* u[3];
-    float* m[3];
-    float* mom[3];
-};
-
 __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, float* out) {
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < nc) out[c] = (float)(cstart[c + 1] - cstart[c]);
@@ -277,9 +246,16 @@ __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, f
 // ------------------------------------------------------------------------------------------------
 __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
+struct FaceAcc {
+    float* m[3];
+    float* P[3];
+    float* Phi[3];  // sum of w * phase (two-phase P2G only)
+};
+
 // weights of one particle on the faces of block nb (resolution rn != r), global atomics
+template <bool PH>
 __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int nc[3], int rn, const float X[3], const float V[3],
-                                 float* const m_out[3], float* const P_out[3]) {
+                                          float ph, const FaceAcc& acc) {
     const Geo& g = L.g;
     const float invh = 1.f / fcell(g, rn);
     float q[3];
@@ -308,24 +284,22 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
                     if (tt <= 0.f) continue;
                     const float w = tt * tt * tt;
                     const uint32_t fi = ob + fidx(a, f[0], f[1], f[2], rn);
-                    atomicAdd(&m_out[a][fi], w);
-                    atomicAdd(&P_out[a][fi], w * V[a]);
+                    atomicAdd(&acc.m[a][fi], w);
+                    atomicAdd(&acc.P[a][fi], w * V[a]);
+                    if (PH) atomicAdd(&acc.Phi[a][fi], w * ph);
                 }
     }
 }
-
-struct FaceAcc {
-    float* m[3];
-    float* P[3];
-};
 
 constexpr int P2G_THREADS = 256;
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
+template <bool PH>
 __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[3], const int* nres, uint32_t v, int d,
                                                uint32_t p0, const float* __restrict__ soa, int64_t n,
-                                               const FaceAcc& acc) {
+                                               const FaceAcc& acc, const uint32_t* __restrict__ pid,
+                                               const float* __restrict__ phase) {
     const uint32_t sidx = p0 + v;
     float X[3], V[3];
 #pragma unroll
@@ -334,11 +308,14 @@ __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[
         V[k] = soa[(int64_t)(3 + k) * n + sidx];
     }
     const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
-    p2g_cross(L, bidx(L.g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, acc.m, acc.P);
+    const float ph = PH ? phase[pid[sidx]] : 0.f;
+    p2g_cross<PH>(L, bidx(L.g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, ph, acc);
 }
 
+template <bool PH>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
-                                                 const uint32_t* __restrict__ cs, FaceAcc acc) {
+                                                 const uint32_t* __restrict__ cs, FaceAcc acc,
+                                                 const uint32_t* __restrict__ pid, const float* __restrict__ phase) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ int cross;
@@ -357,7 +334,8 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     const int TA = (int)tile_axis(r);
     float* am = sm;           // 3 TA mass
     float* ap = sm + 3 * TA;  // 3 TA momentum
-    for (int i = threadIdx.x; i < 6 * TA; i += blockDim.x) sm[i] = 0.f;
+    float* aq = sm + 6 * TA;  // 3 TA phase (PH)
+    for (int i = threadIdx.x; i < (PH ? 9 : 6) * TA; i += blockDim.x) sm[i] = 0.f;
     if (threadIdx.x == 0) cross = 0;
     __syncthreads();
     if (threadIdx.x < 27) {
@@ -389,6 +367,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
         float X[3], V[3], q[3];
         if (valid) {
             const uint32_t sidx = p0 + v;
+            const float ph = PH ? phase[pid[sidx]] : 0.f;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
                 X[k] = soa[(int64_t)k * n + sidx];
@@ -426,6 +405,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                             if (tt > 0.f) {
                                 atomicAdd(&am[e], wgt);
                                 atomicAdd(&ap[e], wgt * va);
+                                if (PH) atomicAdd(&aq[e], wgt * ph);
                             }
                         }
                     }
@@ -469,13 +449,13 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                 __syncwarp();
                 while (qn >= 32) {
                     qn -= 32;
-                    p2g_cross_pair(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc);
+                    p2g_cross_pair<PH>(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc, pid, phase);
                     __syncwarp();
                 }
             }
         }
     }
-    if (qn > 0 && lane < qn) p2g_cross_pair(L, cb, nres, qv[lane], qd[lane], p0, soa, n, acc);
+    if (qn > 0 && lane < qn) p2g_cross_pair<PH>(L, cb, nres, qv[lane], qd[lane], p0, soa, n, acc, pid, phase);
     __syncthreads();
     // flush: every nonzero tile entry into each same-resolution copy of its face
 #pragma unroll
@@ -485,6 +465,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
             const float mv = am[a * TA + rem];
             if (mv == 0.f) continue;
             const float pv = ap[a * TA + rem];
+            const float qv2 = PH ? aq[a * TA + rem] : 0.f;
             const int iA = rem % R1;
             const int i1 = (rem / R1) % R2 - 1;
             const int i2 = rem / (R1 * R2) - 1;
@@ -510,6 +491,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                 const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], r);
                 atomicAdd(&acc.m[a][fi], mv);
                 atomicAdd(&acc.P[a][fi], pv);
+                if (PH) atomicAdd(&acc.Phi[a][fi], qv2);
             }
         }
     }
@@ -530,10 +512,36 @@ __global__ void k_p2g_normalize(const float* __restrict__ m0, const float* __res
     u[i] = mv > 1e-6f ? P[i] / mv : 0.f;
 }
 
+// Two-phase faces: phi = Phi / m where m > 1e-6, else 0; beta = 1 / ((1 - phi) rho0 + phi rho1).
+// PHASE_FIELD_* and BETA_COEFF_* (MSBG.cuh:21-29); the reference leaves this accumulation
+// commented out (P2G.cuh:94-97).
+__global__ void k_p2g_phase(const float* __restrict__ m0, const float* __restrict__ q0, float* phi0, float* beta0,
+                            uint32_t n0, const float* __restrict__ m1, const float* __restrict__ q1, float* phi1,
+                            float* beta1, uint32_t n1, const float* __restrict__ m2, const float* __restrict__ q2,
+                            float* phi2, float* beta2, uint32_t n2, float rho0, float rho1) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float *m, *q;
+    float *phi, *beta;
+    if (i < n0) { m = m0; q = q0; phi = phi0; beta = beta0; }
+    else if ((i -= n0) < n1) { m = m1; q = q1; phi = phi1; beta = beta1; }
+    else if ((i -= n1) < n2) { m = m2; q = q2; phi = phi2; beta = beta2; }
+    else return;
+    const float mv = m[i];
+    const float f = mv > 1e-6f ? fminf(fmaxf(q[i] / mv, 0.f), 1.f) : 0.f;
+    phi[i] = f;
+    beta[i] = 1.f / ((1.f - f) * rho0 + f * rho1);
+}
+
 aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* cstart, float* u[3], float* m[3],
-                     float* mom[3], float* cell_count, cudaStream_t s) {
+                     float* mom[3], float* cell_count, cudaStream_t s, const PhaseIn* ph) {
     FaceAcc acc;
     for (int a = 0; a < 3; ++a) {
+        acc.Phi[a] = nullptr;
+        if (ph) {
+            AW_TRY(G.p2g_Phi[a].ensure(std::max<uint32_t>(G.tot[1 + a], 1)));
+            acc.Phi[a] = G.p2g_Phi[a].p;
+            if (G.tot[1 + a]) AW_CUDA(cudaMemsetAsync(acc.Phi[a], 0, G.tot[1 + a] * sizeof(float), s));
+        }
         acc.m[a] = m[a];
         if (mom[a]) {
             acc.P[a] = mom[a];
@@ -548,10 +556,17 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     }
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = (size_t)6 * tile_axis(maxres) * sizeof(float);
-    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_p2g_own, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = (size_t)(ph ? 9 : 6) * tile_axis(maxres) * sizeof(float);
     if (n > 0) {
-        k_p2g_own<<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc);
+        if (ph) {
+            if (smem > 48 * 1024)
+                AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_p2g_own<true><<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase);
+        } else {
+            if (smem > 48 * 1024)
+                AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_p2g_own<false><<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr);
+        }
         AW_LAUNCH();
     }
     const uint64_t nf = (uint64_t)G.tot[1] + G.tot[2] + G.tot[3];
@@ -559,6 +574,12 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
         k_p2g_normalize<<<nblk(nf), 256, 0, s>>>(acc.m[0], acc.P[0], u[0], G.tot[1], acc.m[1], acc.P[1], u[1], G.tot[2],
                                                  acc.m[2], acc.P[2], u[2], G.tot[3]);
         AW_LAUNCH();
+        if (ph) {
+            k_p2g_phase<<<nblk(nf), 256, 0, s>>>(acc.m[0], acc.Phi[0], ph->phi[0], ph->beta[0], G.tot[1], acc.m[1],
+                                                 acc.Phi[1], ph->phi[1], ph->beta[1], G.tot[2], acc.m[2], acc.Phi[2],
+                                                 ph->phi[2], ph->beta[2], G.tot[3], ph->rho0, ph->rho1);
+            AW_LAUNCH();
+        }
     }
     if (cell_count) {
         k_cell_count<<<nblk(G.tot[0]), 256, 0, s>>>(cstart, G.tot[0], cell_count);
@@ -1545,6 +1566,30 @@ extern "C" aw_status aw_p2g(aw_msbg* g, const float* d_pos, const float* d_vel, 
     float* m[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
     float* mo[3] = {G.ch[AW_MOMENTUM_X], G.ch[AW_MOMENTUM_Y], G.ch[AW_MOMENTUM_Z]};
     return p2g_sorted(G, G.pw.soa.p, n, G.pw.cell_start.p, u, m, mo, G.ch[AW_CELL_TYPE], s);
+}
+
+extern "C" aw_status aw_p2g_phase(aw_msbg* g, const float* d_pos, const float* d_vel, const float* d_phase, int64_t n,
+                                  float rho0, float rho1, aw_stream s_) {
+    AW_CHECK_ARG(g && ((d_pos && d_vel && d_phase) || n == 0) && n >= 0 && n < (int64_t)0xFFFFFFFF, "bad argument");
+    AW_CHECK_ARG(std::isfinite(rho0) && std::isfinite(rho1) && rho0 > 0.f && rho1 > 0.f, "densities must be positive");
+    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
+    cudaStream_t s = (cudaStream_t)s_;
+    MsbgState& G = g->st;
+    AW_TRY(sort_particles_soa(G, d_pos, d_vel, n, s));
+    float* u[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
+    float* m[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
+    float* mo[3] = {G.ch[AW_MOMENTUM_X], G.ch[AW_MOMENTUM_Y], G.ch[AW_MOMENTUM_Z]};
+    PhaseIn ph{};
+    ph.pid = G.pw.sorted;
+    ph.phase = d_phase;
+    ph.rho0 = rho0;
+    ph.rho1 = rho1;
+    for (int a = 0; a < 3; ++a) {
+        ph.phi[a] = G.ch[AW_PHASE_FIELD_X + a];
+        ph.beta[a] = G.ch[AW_BETA_COEFF_X + a];
+    }
+    AW_TRY(p2g_sorted(G, G.pw.soa.p, n, G.pw.cell_start.p, u, m, mo, G.ch[AW_CELL_TYPE], s, &ph));
+    return beta_sync(G, ph.beta, s);
 }
 
 extern "C" aw_status aw_backup_grid_velocity(aw_msbg* g, aw_stream s_) {

@@ -1561,6 +1561,48 @@ static int ilog2(int v) {
     return l;
 }
 
+// Coefficients of the block-structured levels from BETA_COEFF_* (stream-ordered): level 0 takes
+// them as they are, coarser levels average them (k_coarse_bbar); FV mode multiplies by the face
+// geometry (k_conductance), reference mode coarsens with galerkinCoarsen (MSBG.cuh:378-498).
+static aw_status build_coefficients(aw_solver* S, cudaStream_t s) {
+    MsbgState& G = S->g->st;
+    const bool ref = S->d.operator_mode == AW_OPERATOR_REFERENCE;
+    const int nb = G.nb;
+    for (int m = 0; m < S->nmsbg; ++m) {
+        MGLevel& L = S->lv[m];
+        LevelView V = lview(S, m);
+        for (int a = 0; a < 3; ++a) {
+            if (m == 0) {
+                AW_CUDA(cudaMemcpyAsync(L.bbar[a].p, G.ch[AW_BETA_COEFF_X + a], L.nface(a) * sizeof(float),
+                                        cudaMemcpyDeviceToDevice, s));
+            } else {
+                k_coarse_bbar<<<nb, 128, 0, s>>>(lview(S, m - 1), V, a, S->lv[m - 1].bbar[a].p, L.bbar[a].p);
+                AW_LAUNCH();
+            }
+            if (ref) {
+                if (m == 0) {
+                    AW_CUDA(cudaMemcpyAsync(L.W[a].p, L.bbar[a].p, L.nface(a) * sizeof(float),
+                                            cudaMemcpyDeviceToDevice, s));
+                } else {
+                    AW_CUDA(cudaMemsetAsync(L.W[a].p, 0, L.nface(a) * sizeof(float), s));
+                    k_galerkin_ref<<<nb, 256, 0, s>>>(G.geo, G.level.p, a, m, S->lv[m - 1].W[a].p, L.W[a].p,
+                                                      S->lv[m - 1].off[1 + a].p, L.off[1 + a].p);
+                    AW_LAUNCH();
+                }
+            } else {
+                k_conductance<<<nb, 128, 0, s>>>(V, a, L.bbar[a].p, L.W[a].p);
+                AW_LAUNCH();
+            }
+        }
+    }
+    return AW_OK;
+}
+
+extern "C" aw_status aw_solver_update_coefficients(aw_solver* S, aw_stream s) {
+    AW_CHECK_ARG(S, "null solver");
+    return build_coefficients(S, (cudaStream_t)s);
+}
+
 extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_solver** out) {
     AW_CHECK_ARG(g && d && out, "null argument");
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
@@ -1654,32 +1696,7 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         }
     }
     // coefficients of the block-structured levels
-    for (int m = 0; m < S->nmsbg; ++m) {
-        MGLevel& L = S->lv[m];
-        LevelView V = lview(S.get(), m);
-        for (int a = 0; a < 3; ++a) {
-            if (m == 0) {
-                AW_CUDA(cudaMemcpy(L.bbar[a].p, G.ch[AW_BETA_COEFF_X + a], L.nface(a) * sizeof(float),
-                                   cudaMemcpyDeviceToDevice));
-            } else {
-                k_coarse_bbar<<<nb, 128>>>(lview(S.get(), m - 1), V, a, S->lv[m - 1].bbar[a].p, L.bbar[a].p);
-                AW_LAUNCH();
-            }
-            if (ref) {
-                if (m == 0) {
-                    AW_CUDA(cudaMemcpy(L.W[a].p, L.bbar[a].p, L.nface(a) * sizeof(float), cudaMemcpyDeviceToDevice));
-                } else {
-                    AW_CUDA(cudaMemset(L.W[a].p, 0, L.nface(a) * sizeof(float)));
-                    k_galerkin_ref<<<nb, 256>>>(G.geo, G.level.p, a, m, S->lv[m - 1].W[a].p, L.W[a].p,
-                                                S->lv[m - 1].off[1 + a].p, L.off[1 + a].p);
-                    AW_LAUNCH();
-                }
-            } else {
-                k_conductance<<<nb, 128>>>(V, a, L.bbar[a].p, L.W[a].p);
-                AW_LAUNCH();
-            }
-        }
-    }
+    AW_TRY(build_coefficients(S.get(), 0));
     // uniform continuation below one cell per block (FV mode)
     if (!ref && S->nmsbg > 0 && S->lv.back().maxres == 1) {
         int Dd[3] = {G.geo.D[0], G.geo.D[1], G.geo.D[2]};

@@ -137,6 +137,12 @@ def dam_break(N=64, base_res=8, levels=2, thresholds=(8,), seed=0, dt=1.0 / 240,
                  pos=pos, vel=vel)
 
 
+def phase_sphere(pos, center, radius) -> np.ndarray:
+    """Two-phase label per particle: 1 inside the sphere (the second phase), 0 elsewhere."""
+    d2 = ((np.asarray(pos, np.float64) - np.asarray(center, np.float64)) ** 2).sum(-1)
+    return (d2 < radius * radius).astype(np.float32)
+
+
 def config(name: str) -> Scene:
     """The named workloads (see module docstring)."""
     if name == "dam_break_64":

@@ -295,6 +295,9 @@ def run_ours(args, ws, rank, local):
     flip256 = None
     if not args.skip_flip256:
         flip256 = flip256_bench()
+    two_phase = None
+    if not args.skip_two_phase:
+        two_phase = two_phase_bench()
     # clocks sampled from the first timed FLIP step through the last timed region of this run
     clocks = clk.stop() if clk else None
 
@@ -333,6 +336,8 @@ def run_ours(args, ws, rank, local):
         line["poisson"] = poisson
     if flip256 is not None:
         line["flip_256"] = flip256
+    if two_phase is not None:
+        line["two_phase_128"] = two_phase
     print(json.dumps(line), flush=True)
 
 
@@ -427,6 +432,43 @@ def flip256_bench(steps=5, warmup=2):
     return out
 
 
+def two_phase_bench(steps=10, warmup=3, rho=(1.0, 3.0)):
+    """dam_drop_128 with the falling sphere as a second, heavier liquid (rho 3 vs 1): FLIP steps with
+    beta = 1/rho from the P2G phase field (coefficients rebuilt every step), beside the one-phase step
+    on the same layout.  Mixed projection to 1e-6."""
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import scenes
+    S = scenes.config(WORKLOAD)
+    ph = scenes.phase_sphere(S.pos, (0.7, 0.8, 0.5), 0.12)
+    out = {"workload": WORKLOAD, "particles": S.n, "heavy_particles": int(ph.sum()), "rho": list(rho),
+           "steps": steps}
+    for name in ("one_phase", "two_phase"):
+        g = aw.build_grid(S)
+        F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_MIXED, tolerance=1e-6,
+                    max_cycles=100)
+        if name == "two_phase":
+            F.set_phase(ph, *rho)
+        for _ in range(warmup):
+            F.step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        st = []
+        for _ in range(steps):
+            F.step()
+            st.append(F.stats())
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        out[name] = {"ms_per_step": ms, "cycles": [x["cycles"] for x in st], "div_after": st[-1]["div_after"],
+                     "ms_p2g": float(np.mean([x["ms_p2g"] for x in st])),
+                     "ms_solve": float(np.mean([x["ms_solve"] for x in st]))}
+        F.close()
+        g.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,6 +478,7 @@ def main():
     ap.add_argument("--skip-poisson", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-flip256", action="store_true", help="skip the dam_drop2_256 FLIP steps/s section")
+    ap.add_argument("--skip-two-phase", action="store_true", help="skip the two-phase dam_drop_128 section")
     ap.add_argument("--poisson-only", action="store_true",
                     help="only the poisson_256 projection comparison (for profiling the solver)")
     ap.add_argument("--poisson-solve-once", action="store_true",

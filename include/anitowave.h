@@ -131,6 +131,13 @@ aw_status aw_msbg_run_galerkin(aw_msbg* g, const float* d_fine[3], float* d_coar
  * writes MASS_DENSITY_*, MOMENTUM_* and VELOCITY_* = momentum/mass (0 where mass <= 1e-6), and
  * the particle count per cell into CELL_TYPE (as float).  Sorts the particles internally. */
 aw_status aw_p2g(aw_msbg* g, const float* d_pos, const float* d_vel, int64_t n, aw_stream s);
+/* aw_p2g for two phases: particle i also carries a phase d_phase[i] in [0,1].  Adds PHASE_FIELD_* =
+ * sum w phase / sum w (0 where mass <= 1e-6) and BETA_COEFF_* = 1 / ((1 - phi) rho0 + phi rho1),
+ * the face coefficients beta = 1/rho of the Poisson equation, with beta made equal on the coarse
+ * face and the 4 fine faces of each T-junction (their mean).  The reference allocates these
+ * channels (MSBG.cuh:21-29) and leaves their accumulation commented out (P2G.cuh:94-97). */
+aw_status aw_p2g_phase(aw_msbg* g, const float* d_pos, const float* d_vel, const float* d_phase, int64_t n, float rho0,
+                       float rho1, aw_stream s);
 /* G2PManager::backupGridVelocity (G2P.cuh:192-196): VELOCITY_OLD_* = VELOCITY_* */
 aw_status aw_backup_grid_velocity(aw_msbg* g, aw_stream s);
 /* G2PManager::performG2P (G2P.cuh:198-211): v = alpha (v + u_new - u_old) + (1 - alpha) u_new,
@@ -201,6 +208,10 @@ aw_status aw_solver_destroy(aw_solver* sv);
 /* Per-step setup: fluid flags of level 0 (d_fluid: u8 per cell, NULL = every cell fluid),
  * coarse flags, and the FP64 factorisation of the coarsest level. */
 aw_status aw_solver_setup(aw_solver* sv, const uint8_t* d_fluid, aw_stream s);
+/* Rebuild every block-structured level's coefficients from the grid's current BETA_COEFF_*
+ * (after aw_p2g_phase; before aw_solver_setup, whose coarsest factorisation uses them).
+ * Stream-ordered; no counterpart in the reference, whose coefficients are fixed at init. */
+aw_status aw_solver_update_coefficients(aw_solver* sv, aw_stream s);
 aw_status aw_solver_num_levels(const aw_solver* sv, int32_t* n);
 /* precision of the solver (AW_PRECISION_FP32 or AW_PRECISION_MIXED) */
 aw_status aw_solver_precision(const aw_solver* sv, int32_t* precision);
@@ -266,6 +277,12 @@ aw_status aw_flip_solver(aw_flip* f, aw_solver** out);
  * layout changed.  syncs.  No counterpart in the reference (markActiveBlocks + grading +
  * allocateChannels were a one-time setup there, main.cu:154-278). */
 aw_status aw_flip_rebuild_levels(aw_flip* f, const int32_t* h_thresholds, int32_t* changed, aw_stream s);
+/* Two-phase simulation: h_phase[i] in [0,1] is the phase of particle i (original order) and rho0,
+ * rho1 > 0 the densities of phase 0 and 1.  Every later step runs aw_p2g_phase's deposit, rebuilds
+ * the solver's coefficients from BETA_COEFF_* and projects with beta = 1/rho.  The particle
+ * velocity transfer keeps unit particle mass.  h_phase = NULL returns to one phase (beta = 1).
+ * The differentiable rollout does not take a phase.  syncs. */
+aw_status aw_flip_set_phase(aw_flip* f, const float* h_phase, float rho0, float rho1);
 
 /* ---- projection and adjoints (no counterpart in the reference) ------------------------------
  * The vector-Jacobian products differentiate the forward calls with their discrete decisions

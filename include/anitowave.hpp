@@ -130,6 +130,11 @@ public:
     void run(MSBGManager& mg, const float* d_pos, const float* d_vel, uint32_t numParticles, aw_stream s = nullptr) {
         check(aw_p2g(mg.handle(), d_pos, d_vel, numParticles, s));
     }
+    // run() plus the phase field and beta = 1/rho (PHASE_FIELD_*, BETA_COEFF_*; MSBG.cuh:21-29)
+    void runPhase(MSBGManager& mg, const float* d_pos, const float* d_vel, const float* d_phase, uint32_t numParticles,
+                  float rho0, float rho1, aw_stream s = nullptr) {
+        check(aw_p2g_phase(mg.handle(), d_pos, d_vel, d_phase, numParticles, rho0, rho1, s));
+    }
 };
 
 // G2PManager (G2P.cuh:175-228)
@@ -207,6 +212,8 @@ public:
         if (level != 0) throw Error(AW_ERR_UNSUPPORTED, "runCycle runs the whole cycle from level 0");
         check(aw_vcycle_run(sv_, s));
     }
+    // coefficients of every level again from the grid's current BETA_COEFF_* (after runPhase)
+    void updateCoefficients(aw_stream s = nullptr) { check(aw_solver_update_coefficients(sv_, s)); }
     // level array of the hierarchy: which 0 = x, 1 = b, 2 = r (floats)
     float* levelArray(int level, int which, uint32_t* count = nullptr) const {
         void* p = nullptr;

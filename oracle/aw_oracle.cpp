@@ -19,6 +19,7 @@
 //   MSBG.cuh:679-745   computeCoarseOffsets/FaceOffsets -> offsets(mg, vanish=true)
 //   P2G.cuh:6-12,16-135 kernel weight and splat       -> p2g() (gather form, D1/D2 corrected)
 //   P2G.cuh:139-171    normalizeVelocity               -> p2g() (u = P/m if m > 1e-6)
+//   MSBG.cuh:21-29, P2G.cuh:94-97 phase field, beta = 1/rho -> oc_p2g_phase(), oc_beta_sync()
 //   G2P.cuh:11-80      interpolateComponent            -> sample() (D4/D5 corrected staggering)
 //   G2P.cuh:87-128     g2pUpdateKernel (FLIP blend)    -> g2p()
 //   G2P.cuh:131-173    advectParticlesKernel (RK3)     -> advect()
@@ -1342,7 +1343,7 @@ OC_API void oc_particle_keys(void* h, const float* pos, int64_t n, uint32_t* key
 namespace {
 template <class PT>
 void p2g_impl(Ctx* C, const PT* pos, const PT* vel, int64_t n, double* ux, double* uy, double* uz, double* mx,
-              double* my, double* mz, uint32_t* cell_count) {
+              double* my, double* mz, uint32_t* cell_count, const float* phase = nullptr, double* const* phi = nullptr) {
     const Geo& g = C->g;
     PartGrid PG = make_pgrid(*C);
     std::vector<uint32_t> k(n);
@@ -1381,7 +1382,7 @@ void p2g_impl(Ctx* C, const PT* pos, const PT* vel, int64_t n, double* ux, doubl
                         f[a] = fa; f[t1] = u1; f[t2] = u2;
                         double xf[3];
                         for (int q = 0; q < 3; ++q) xf[q] = org[q] + h_ * (f[q] + (q == a ? 0.0 : 0.5));
-                        double msum = 0, psum = 0;
+                        double msum = 0, psum = 0, qsum = 0;
                         // blocks intersecting the support box
                         int blo[3], bhi[3];
                         for (int q = 0; q < 3; ++q) {
@@ -1416,12 +1417,14 @@ void p2g_impl(Ctx* C, const PT* pos, const PT* vel, int64_t n, double* ux, doubl
                                                     double w = kernel_w(d2, R2);
                                                     msum += w;
                                                     psum += w * (double)vel[3 * p + a];
+                                                    if (phase) qsum += w * (double)phase[p];
                                                 }
                                             }
                                 }
                         uint32_t fi = PG.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r);
                         Mm[a][fi] = msum;
                         U[a][fi] = msum > 1e-6 ? psum / msum : 0.0;
+                        if (phase) phi[a][fi] = msum > 1e-6 ? std::min(1.0, std::max(0.0, qsum / msum)) : 0.0;
                     }
         }
     }
@@ -1433,6 +1436,60 @@ OC_API void oc_p2g(void* h, const float* pos, const float* vel, int64_t n, doubl
                    double* mx, double* my, double* mz, uint32_t* cell_count) {
     p2g_impl((Ctx*)h, pos, vel, n, ux, uy, uz, mx, my, mz, cell_count);
 }
+// Two-phase P2G: also the face phase phi = sum w phase / sum w (0 where the mass is <= 1e-6),
+// the channel PHASE_FIELD_* (MSBG.cuh:21-29) whose accumulation P2G.cuh:94-97 leaves commented out.
+OC_API void oc_p2g_phase(void* h, const float* pos, const float* vel, const float* phase, int64_t n, double* ux,
+                         double* uy, double* uz, double* mx, double* my, double* mz, double* px, double* py,
+                         double* pz, uint32_t* cell_count) {
+    double* phi[3] = {px, py, pz};
+    p2g_impl((Ctx*)h, pos, vel, n, ux, uy, uz, mx, my, mz, cell_count, phase, phi);
+}
+
+// Face coefficients at T-junctions: the coarse face and the 4 fine faces it covers all take the
+// mean of the 4 fine values (equal coefficients on both sides keep the FV operator symmetric).
+OC_API void oc_beta_sync(void* h, double* bx, double* by, double* bz) {
+    Ctx* C = (Ctx*)h;
+    const Geo& g = C->g;
+    PartGrid PG = make_pgrid(*C);
+    double* B[3] = {bx, by, bz};
+    for (int b = 0; b < g.nb(); ++b) {
+        int r = PG.res[b];
+        if (!r) continue;
+        int cb[3];
+        bcoord(g, b, cb);
+        for (int a = 0; a < 3; ++a) {
+            int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            for (int s = -1; s <= 1; s += 2) {
+                int nc[3] = {cb[0], cb[1], cb[2]};
+                nc[a] += s;
+                if (!inside(g, nc)) continue;
+                int n = bidx(g, nc[0], nc[1], nc[2]);
+                int rn = PG.res[n];
+                if (rn != 2 * r) continue;
+                for (int u1 = 0; u1 < r; ++u1)
+                    for (int u2 = 0; u2 < r; ++u2) {
+                        uint32_t fine[4];
+                        double sum = 0;
+                        for (int k = 0; k < 4; ++k) {
+                            int q[3];
+                            q[a] = s > 0 ? 0 : rn;
+                            q[t1] = 2 * u1 + k / 2;
+                            q[t2] = 2 * u2 + k % 2;
+                            fine[k] = PG.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn);
+                            sum += B[a][fine[k]];
+                        }
+                        for (int k = 0; k < 4; ++k) B[a][fine[k]] = 0.25 * sum;
+                        int f[3];
+                        f[a] = s > 0 ? r : 0;
+                        f[t1] = u1;
+                        f[t2] = u2;
+                        B[a][PG.off[1 + a][b] + fidx(a, f[0], f[1], f[2], r)] = 0.25 * sum;
+                    }
+            }
+        }
+    }
+}
+
 // P2G on FP64 particle state (the differentiable rollout); cells of particles from float(pos)
 OC_API void oc_p2g64(void* h, const double* pos, const double* vel, int64_t n, double* ux, double* uy, double* uz,
                      double* mx, double* my, double* mz, uint32_t* cell_count) {

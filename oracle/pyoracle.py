@@ -72,6 +72,8 @@ def lib():
         L.oc_apply.argtypes = [P, C.c_int, f64p, f64p]
         L.oc_particle_keys.argtypes = [P, f32p, C.c_int64, u32p, i64p]
         L.oc_p2g.argtypes = [P, f32p, f32p, C.c_int64, f64p, f64p, f64p, f64p, f64p, f64p, u32p]
+        L.oc_p2g_phase.argtypes = [P, f32p, f32p, f32p, C.c_int64] + [f64p] * 9 + [u32p]
+        L.oc_beta_sync.argtypes = [P, f64p, f64p, f64p]
         L.oc_face_sync.argtypes = [P, f64p, f64p, f64p]
         L.oc_wall_bc.argtypes = [P, f64p, f64p, f64p]
         L.oc_divergence.argtypes = [P, f64p, f64p, f64p, u8p, C.c_double, f64p]
@@ -303,6 +305,30 @@ class Oracle:
         lib().oc_p2g(self.h, pos, vel, pos.shape[0], u[0], u[1], u[2], m[0], m[1], m[2], cnt)
         return u, m, cnt
 
+    def p2g_phase(self, pos, vel, phase):
+        """p2g plus the face phase sum w phase / sum w (0 where the mass is <= 1e-6)."""
+        pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+        vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
+        phase = np.ascontiguousarray(phase, np.float32).reshape(-1)
+        t = self.tot0
+        u = [np.zeros(int(t[1 + a])) for a in range(3)]
+        m = [np.zeros(int(t[1 + a])) for a in range(3)]
+        phi = [np.zeros(int(t[1 + a])) for a in range(3)]
+        cnt = np.zeros(int(t[0]), np.uint32)
+        lib().oc_p2g_phase(self.h, pos, vel, phase, pos.shape[0], u[0], u[1], u[2], m[0], m[1], m[2], phi[0], phi[1],
+                           phi[2], cnt)
+        return u, m, cnt, phi
+
+    def beta_sync(self, beta):
+        """T-junction coefficients: the coarse face and its 4 fine faces all take the fine mean."""
+        beta = [np.ascontiguousarray(x, np.float64).copy() for x in beta]
+        lib().oc_beta_sync(self.h, *beta)
+        return beta
+
+    def phase_beta(self, phi, rho0, rho1):
+        """beta = 1 / ((1 - phi) rho0 + phi rho1), then the T-junction sync."""
+        return self.beta_sync([1.0 / ((1.0 - f) * rho0 + f * rho1) for f in phi])
+
     def face_sync(self, u):
         u = [np.ascontiguousarray(x, np.float64).copy() for x in u]
         lib().oc_face_sync(self.h, *u)
@@ -408,15 +434,23 @@ class Oracle:
         return out
 
 
-def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=200, method="dc"):
+def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=200, method="dc", phase=None,
+              rho=(1.0, 1.0)):
     """One FLIP step of the FP64 restatement, in the order the GPU step runs: sort -> P2G ->
     T-junction sync -> backup -> gravity -> walls -> divergence -> solve -> gradient -> sync ->
-    walls -> G2P -> RK3.  Returns (pos, vel) in sorted order, the sort permutation and details."""
+    walls -> G2P -> RK3.  Returns (pos, vel) in sorted order, the sort permutation and details.
+    `phase` (per particle, input order) makes it two-phase: beta = 1/rho from the P2G face phase
+    with densities rho = (rho0, rho1)."""
     pos = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
     vel = np.ascontiguousarray(vel, np.float32).reshape(-1, 3)
     _, perm = O.particle_keys(pos)
     ps, vs = pos[perm], vel[perm]
-    u, m, cnt = O.p2g(ps, vs)
+    beta = None
+    if phase is None:
+        u, m, cnt = O.p2g(ps, vs)
+    else:
+        u, m, cnt, phi = O.p2g_phase(ps, vs, np.asarray(phase, np.float32)[perm])
+        beta = O.phase_beta(phi, rho[0], rho[1])
     u = O.face_sync(u)
     uo = [x.copy() for x in u]
     for a in range(3):
@@ -425,13 +459,14 @@ def flip_step(O: "Oracle", pos, vel, dt, alpha, gravity, tol=1e-12, max_cycles=2
     fluid = (cnt > 0).astype(np.uint8)
     b = O.divergence(u, fluid, dt)
     O.set_params(mode=0)
-    O.build(fluid=fluid)
+    O.build(bbar=beta, fluid=fluid)
     p, hist = O.solve(b, tol=tol, max_cycles=max_cycles, method=method)
     un = O.gradient_update(p, dt, u)
     un = O.wall_bc(O.face_sync(un))
     vnew = O.g2p(ps, un, uo, alpha, vs)
     xnew = O.advect(un, dt, ps.astype(np.float64))
-    return xnew, vnew, perm, dict(u_star=u, u_old=uo, u_new=un, p=p, b=b, fluid=fluid, hist=hist, count=cnt)
+    return xnew, vnew, perm, dict(u_star=u, u_old=uo, u_new=un, p=p, b=b, fluid=fluid, hist=hist, count=cnt,
+                                  beta=beta)
 
 
 # ------------------------------------------------------------------------------------------------
