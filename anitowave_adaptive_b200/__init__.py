@@ -25,7 +25,8 @@ LIB_PATH = os.path.join(_HERE, "libanitowave.so")
 
 AW_OK = 0
 STATUS = {0: "AW_OK", 1: "AW_ERR_INVALID_ARGUMENT", 2: "AW_ERR_CUDA", 3: "AW_ERR_OUT_OF_MEMORY",
-          4: "AW_ERR_NOT_CONVERGED", 5: "AW_ERR_NAN", 6: "AW_ERR_STATE", 7: "AW_ERR_UNSUPPORTED"}
+          4: "AW_ERR_NOT_CONVERGED", 5: "AW_ERR_NAN", 6: "AW_ERR_STATE", 7: "AW_ERR_UNSUPPORTED",
+          8: "AW_ERR_IO"}
 
 # channels (MSBG.cuh:12-50)
 VELOCITY_X, VELOCITY_Y, VELOCITY_Z, PRESSURE = 0, 1, 2, 3
@@ -100,6 +101,13 @@ SIGNATURES = {
     "aw_g2p_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
     "aw_advect": (C.c_int, [_VP, _VP, _I64, _F, _VP]),
     "aw_sample_velocity": (C.c_int, [_VP, _VP, _I64, _I32, _VP, _VP]),
+    "aw_resample_lattice": (C.c_int, [_VP, C.POINTER(_I32), C.POINTER(_F), C.POINTER(_F)]),
+    "aw_resample_cells": (C.c_int, [_VP, _I32, C.POINTER(_I32), _VP, _VP]),
+    "aw_resample_velocity": (C.c_int, [_VP, _I32, C.POINTER(_I32), _VP, _VP]),
+    "aw_vtk_write_structured_points": (C.c_int, [C.c_char_p, C.POINTER(_I32), C.POINTER(_F), C.POINTER(_F),
+                                                 C.c_char_p, _I32, _VP]),
+    "aw_vtk_write_blocks": (C.c_int, [_VP, C.c_char_p]),
+    "aw_vtk_write_particles": (C.c_int, [C.c_char_p, _VP, _I64, C.c_char_p, _VP]),
     "aw_sort_particles": (C.c_int, [_VP, _VP, _I64, _VP, _VP, _VP]),
     "aw_face_positions": (C.c_int, [_VP, _I32, _VP, _VP]),
     "aw_face_sync": (C.c_int, [_VP, _I32, _VP]),
@@ -336,6 +344,33 @@ class MSBG:
                                        _stream(stream)))
         return out
 
+    # inspection ---------------------------------------------------------------------------
+    def resample_lattice(self, dims):
+        """(origin, spacing) of the dense lattice of `dims` points over the domain."""
+        d = (_I32 * 3)(*[int(x) for x in dims])
+        o, s = (_F * 3)(), (_F * 3)()
+        check(lib().aw_resample_lattice(self.h, d, o, s))
+        return tuple(o), tuple(s)
+
+    def resample_cells(self, channel, dims, stream=None):
+        """A cell channel at the dense lattice points: torch tensor (dims[2], dims[1], dims[0])."""
+        import torch
+        d = (_I32 * 3)(*[int(x) for x in dims])
+        out = torch.empty((int(dims[2]), int(dims[1]), int(dims[0])), dtype=torch.float32, device="cuda")
+        check(lib().aw_resample_cells(self.h, int(channel), d, out.data_ptr(), _stream(stream)))
+        return out
+
+    def resample_velocity(self, dims, old=False, stream=None):
+        """The MAC velocity at the dense lattice points: torch tensor (dims[2], dims[1], dims[0], 3)."""
+        import torch
+        d = (_I32 * 3)(*[int(x) for x in dims])
+        out = torch.empty((int(dims[2]), int(dims[1]), int(dims[0]), 3), dtype=torch.float32, device="cuda")
+        check(lib().aw_resample_velocity(self.h, 1 if old else 0, d, out.data_ptr(), _stream(stream)))
+        return out
+
+    def vtk_write_blocks(self, path):
+        check(lib().aw_vtk_write_blocks(self.h, str(path).encode()))
+
     def face_positions(self, axis, stream=None):
         import torch
         n = self.totals()[0 if axis == 3 else 1 + axis]
@@ -409,6 +444,25 @@ class MSBG:
         perm = torch.empty(n, dtype=torch.int32, device="cuda")
         check(lib().aw_sort_particles(self.h, _ptr(pos), n, keys.data_ptr(), perm.data_ptr(), _stream(stream)))
         return keys, perm
+
+
+def vtk_write_structured_points(path, data, origin, spacing, name="field"):
+    """Binary legacy VTK STRUCTURED_POINTS from a host array (nz, ny, nx) or (nz, ny, nx, 3)."""
+    a = np.ascontiguousarray(data, np.float32)
+    ncomp = 3 if a.ndim == 4 else 1
+    dims = (_I32 * 3)(a.shape[2], a.shape[1], a.shape[0])
+    check(lib().aw_vtk_write_structured_points(str(path).encode(), dims, (_F * 3)(*origin), (_F * 3)(*spacing),
+                                               name.encode(), ncomp, a.ctypes.data))
+
+
+def vtk_write_particles(path, pos, scalar=None, name="scalar"):
+    """Binary legacy VTK POLYDATA of host positions (n, 3) with an optional float per particle."""
+    p = np.ascontiguousarray(pos, np.float32).reshape(-1, 3)
+    s = None if scalar is None else np.ascontiguousarray(scalar, np.float32).reshape(-1)
+    if s is not None and s.shape[0] != p.shape[0]:
+        raise ValueError("one scalar per particle")
+    check(lib().aw_vtk_write_particles(str(path).encode(), p.ctypes.data, p.shape[0], name.encode(),
+                                       None if s is None else s.ctypes.data))
 
 
 def solver_default_desc(mode=OPERATOR_FV):

@@ -98,6 +98,13 @@ __global__ void k_beta_sync(LevelView L, float* b0, float* b1, float* b2) {
     }
 }
 
+// the step's pressure into the PRESSURE channel (0 in air cells), for inspection
+template <class PT>
+__global__ void k_store_pressure(const PT* __restrict__ p, const uint8_t* __restrict__ fluid, size_t n, float* out) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = fluid[i] ? (float)p[i] : 0.f;
+}
+
 __global__ void k_fill(float* u, size_t n, float v) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) u[i] = v;
@@ -654,6 +661,13 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
         st->residual = rel;
     }
     if (sst != AW_OK) return sst;
+    if (G.tot[0]) {
+        if (d.precision == AW_PRECISION_MIXED)
+            k_store_pressure<double><<<nblk(G.tot[0]), 256, 0, s>>>(B.p64.p, B.fluid.p, G.tot[0], G.ch[AW_PRESSURE]);
+        else
+            k_store_pressure<float><<<nblk(G.tot[0]), 256, 0, s>>>(B.p32.p, B.fluid.p, G.tot[0], G.ch[AW_PRESSURE]);
+        AW_LAUNCH();
+    }
     if (ev) AW_CUDA(cudaEventRecord(ev[4], s));
     // 6. pressure-gradient update, sync, walls
     void* W[3];

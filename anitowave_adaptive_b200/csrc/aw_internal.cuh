@@ -214,6 +214,7 @@ struct MsbgState {
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for
     DBuf<float> p2g_Phi[3];                     // P2G phase accumulator (two-phase P2G)
+    DBuf<int> lattice_tab;                      // per-axis lookup tables of aw_resample_cells
     FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
     DBuf<int> err;  // device error flags: [1] bulk-copy wait timeout in G2P / advection ([0] unused)
     DBuf<uint8_t> occ;

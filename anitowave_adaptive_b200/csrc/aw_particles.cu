@@ -1628,6 +1628,156 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
     return advect_tiles(G, d_pos, 0, n, dt, G.tiles_new.p, (cudaStream_t)s_);
 }
 
+// ------------------------------------------------------------------------------------------------
+// Dense resampling for inspection (sampleMSBG, vtx_visualization.cuh:8-62).  Lattice point
+// (i, j, k) of an out[0] x out[1] x out[2] lattice over the domain sits at
+// domain_min + (i + 0.5) * spacing (spacing = domain extent / out, rounded to float on the host);
+// x fastest.  Cell channels take the value of the cell holding the point (0 in inactive blocks);
+// the reference's version ignores domain_min.  The velocity takes the MAC trilinear sample.
+// ------------------------------------------------------------------------------------------------
+struct Lattice {
+    int D[3];
+    float sp[3];
+};
+
+__device__ inline float lattice_coord(const Geo& g, const Lattice& T, int a, int i) {
+    return __fadd_rn(g.dmin[a], __fmul_rn(__fadd_rn((float)i, 0.5f), T.sp[a]));
+}
+
+__device__ inline void lattice_point(const Geo& g, const Lattice& T, int64_t idx, float X[3]) {
+    const int64_t nxy = (int64_t)T.D[0] * T.D[1];
+    const int c[3] = {(int)(idx % T.D[0]), (int)((idx / T.D[0]) % T.D[1]), (int)(idx / nxy)};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) X[a] = lattice_coord(g, T, a, c[a]);
+}
+
+// Per-axis lookup of the cell lookup (particle_key's arithmetic split by axis): for lattice
+// coordinate i along axis a, the block coordinate and, for every level l, the cell index in a
+// block of resolution R0 >> l.  Row tab[a] holds D[a] entries of (1 + L) ints.
+__global__ void k_lattice_tables(Geo g, Lattice T, int* tab0, int* tab1, int* tab2) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int a = blockIdx.y;
+    if (i >= T.D[a]) return;
+    int* tab = a == 0 ? tab0 : (a == 1 ? tab1 : tab2);
+    const float p = lattice_coord(g, T, a, i);
+    const int c = min(max((int)floorf(__fdiv_rn(__fsub_rn(p, g.dmin[a]), g.bs)), 0), g.D[a] - 1);
+    const int stride = 1 + g.L;
+    tab[i * stride] = c;
+    const float o = forigin(g, a, c);
+    for (int l = 0; l < g.L; ++l) {
+        const int r = g.R0 >> l;
+        const float h = fcell(g, r);
+        tab[i * stride + 1 + l] = min(max((int)floorf(__fdiv_rn(__fsub_rn(p, o), h)), 0), r - 1);
+    }
+}
+
+// one CTA row = one lattice x-row (fixed y, z): coalesced writes, per-axis tables for the lookup
+__global__ void k_resample_cells(LevelView L, Lattice T, const int* __restrict__ tab0, const int* __restrict__ tab1,
+                                 const int* __restrict__ tab2, const float* __restrict__ ch, float* out) {
+    const int stride = 1 + L.g.L;
+    const int64_t rows = (int64_t)T.D[1] * T.D[2];
+    for (int64_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int y = (int)(row % T.D[1]), z = (int)(row / T.D[1]);
+        const int* ty = tab1 + (size_t)y * stride;
+        const int* tz = tab2 + (size_t)z * stride;
+        float* o = out + row * T.D[0];
+        for (int x = threadIdx.x; x < T.D[0]; x += blockDim.x) {
+            const int* tx = tab0 + (size_t)x * stride;
+            const int b = bidx(L.g, tx[0], ty[0], tz[0]);
+            const int r = L.res[b];
+            float v = 0.f;
+            if (r) {
+                const int l = __ffs(L.g.R0) - __ffs(r);  // r = R0 >> l
+                v = ch[L.off[0][b] + cidx(tx[1 + l], ty[1 + l], tz[1 + l], r)];
+            }
+            o[x] = v;
+        }
+    }
+}
+
+__global__ void k_resample_velocity(LevelView L, Lattice T, const uint32_t* __restrict__ toff,
+                                    const float* __restrict__ tiles, float* out) {
+    const int64_t n = (int64_t)T.D[0] * T.D[1] * T.D[2];
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float X[3];
+        lattice_point(L.g, T, i, X);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) out[3 * i + a] = sample_tiles(L, toff, tiles, a, X);
+    }
+}
+
+static aw_status make_lattice(const MsbgState& G, const int32_t out_dims[3], Lattice& T) {
+    for (int a = 0; a < 3; ++a) {
+        if (out_dims[a] < 1 || out_dims[a] > (1 << 16))
+            return set_error(AW_ERR_INVALID_ARGUMENT, "lattice size %d out of range", out_dims[a]);
+        T.D[a] = out_dims[a];
+        T.sp[a] = (float)G.geo.D[a] * G.geo.bs / (float)out_dims[a];
+    }
+    return AW_OK;
+}
+
+static unsigned resample_grid(int64_t n) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)sms * 8));
+}
+
+extern "C" aw_status aw_resample_lattice(aw_msbg* g, const int32_t out_dims[3], float origin[3], float spacing[3]) {
+    AW_CHECK_ARG(g && out_dims && origin && spacing, "null argument");
+    Lattice T;
+    AW_TRY(make_lattice(g->st, out_dims, T));
+    for (int a = 0; a < 3; ++a) {
+        spacing[a] = T.sp[a];
+        origin[a] = g->st.geo.dmin[a] + 0.5f * T.sp[a];
+    }
+    return AW_OK;
+}
+
+extern "C" aw_status aw_resample_cells(aw_msbg* g, int32_t channel, const int32_t out_dims[3], float* d_out,
+                                       aw_stream s_) {
+    AW_CHECK_ARG(g && out_dims && d_out, "null argument");
+    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
+    if (!(channel == AW_PRESSURE || channel == AW_DIVERGENCE || channel == AW_DISTANCE_FIELD ||
+          channel == AW_VORTICITY || channel == AW_CELL_TYPE))
+        return set_error(AW_ERR_INVALID_ARGUMENT, "channel %d is not a cell channel", channel);
+    MsbgState& G = g->st;
+    Lattice T;
+    AW_TRY(make_lattice(G, out_dims, T));
+    cudaStream_t s = (cudaStream_t)s_;
+    const int stride = 1 + G.geo.L;
+    AW_TRY(G.lattice_tab.ensure((size_t)stride * (T.D[0] + T.D[1] + T.D[2])));
+    int* tab[3] = {G.lattice_tab.p, G.lattice_tab.p + (size_t)stride * T.D[0],
+                   G.lattice_tab.p + (size_t)stride * (T.D[0] + T.D[1])};
+    const int dmax = std::max({T.D[0], T.D[1], T.D[2]});
+    k_lattice_tables<<<dim3((dmax + 127) / 128, 3), 128, 0, s>>>(G.geo, T, tab[0], tab[1], tab[2]);
+    AW_LAUNCH();
+    const int64_t rows = (int64_t)T.D[1] * T.D[2];
+    const int threads = T.D[0] >= 256 ? 256 : (T.D[0] >= 128 ? 128 : 64);
+    k_resample_cells<<<(unsigned)std::min<int64_t>(rows, 148 * 64), threads, 0, s>>>(G.view0(), T, tab[0], tab[1],
+                                                                                   tab[2], G.ch[channel], d_out);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+extern "C" aw_status aw_resample_velocity(aw_msbg* g, int32_t old, const int32_t out_dims[3], float* d_out,
+                                          aw_stream s_) {
+    AW_CHECK_ARG(g && out_dims && d_out, "null argument");
+    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
+    MsbgState& G = g->st;
+    cudaStream_t s = (cudaStream_t)s_;
+    Lattice T;
+    AW_TRY(make_lattice(G, out_dims, T));
+    const int base = old ? AW_VELOCITY_OLD_X : AW_VELOCITY_X;
+    const float* u[3] = {G.ch[base], G.ch[base + 1], G.ch[base + 2]};
+    AW_TRY(ensure_tiles(G));
+    AW_TRY(build_tiles(G, u, G.tiles_old.p, s));
+    const int64_t n = (int64_t)T.D[0] * T.D[1] * T.D[2];
+    k_resample_velocity<<<resample_grid(n), 256, 0, s>>>(G.view0(), T, G.tile_off.p, G.tiles_old.p, d_out);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 extern "C" aw_status aw_sample_velocity(aw_msbg* g, const float* d_points, int64_t n, int32_t old, float* d_out,
                                         aw_stream s_) {
     AW_CHECK_ARG(g && ((d_points && d_out) || n == 0) && n >= 0, "bad argument");

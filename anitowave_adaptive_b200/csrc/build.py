@@ -8,7 +8,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.dirname(HERE)
 ROOT = os.path.dirname(PKG)
-SOURCES = ["aw_grid.cu", "aw_particles.cu", "aw_solver.cu", "aw_flip.cu", "aw_adjoint.cu", "aw_noalloc.cu"]
+SOURCES = ["aw_grid.cu", "aw_particles.cu", "aw_solver.cu", "aw_flip.cu", "aw_adjoint.cu", "aw_noalloc.cu",
+           "aw_output.cu"]
 OUT = os.path.join(PKG, "libanitowave.so")
 NVCC = os.environ.get("NVCC", "nvcc")
 FLAGS = [

@@ -235,6 +235,8 @@ def run_ours(args, ws, rank, local):
     p2g_gbs = p2g_bytes / (p2g_ms / 1e3) / 1e9
     g2p_gbs = g2p_bytes / (g2p_ms / 1e3) / 1e9
 
+    resample = resample_bench(g, aw)
+
     # e2e through the drop-in C ABI with host buffers: every step uploads its positions and
     # velocities from pinned host memory, runs aw_p2g (sort + P2G), the backup and aw_g2p, and reads
     # the velocities back.  Two device buffer sets and two copy streams let step k+1's upload and
@@ -338,6 +340,7 @@ def run_ours(args, ws, rank, local):
         line["flip_256"] = flip256
     if two_phase is not None:
         line["two_phase_128"] = two_phase
+    line["resample_256"] = resample
     print(json.dumps(line), flush=True)
 
 
@@ -429,6 +432,32 @@ def flip256_bench(steps=5, warmup=2):
                      "ms_g2p": float(np.mean([x["ms_g2p"] for x in st]))}
         F.close()
     g.close()
+    return out
+
+
+def resample_bench(g, aw, dims=(256, 256, 256), reps=10, warmup=3):
+    """Dense resampling for inspection on the workload's grid after its FLIP steps: PRESSURE (nearest
+    cell) and the MAC velocity (trilinear) on a 256^3 lattice.  Bytes counted: the lattice written
+    (4 or 12 B per point) plus the grid channel read once (cells 4 B; velocity faces 4 B each)."""
+    import torch
+    tot = g.totals()
+    npts = dims[0] * dims[1] * dims[2]
+    out = {"lattice": list(dims), "points": npts}
+    for name, fn, wbytes, rbytes in (
+            ("pressure", lambda: g.resample_cells(aw.PRESSURE, dims), 4, tot[0] * 4),
+            ("velocity", lambda: g.resample_velocity(dims), 12, sum(tot[1:]) * 4)):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = (npts * wbytes + rbytes) / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "GBps": gbs, "frac_of_hbm": gbs / peaks()[0]}
     return out
 
 

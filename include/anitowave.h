@@ -37,7 +37,8 @@ typedef enum aw_status {
     AW_ERR_NOT_CONVERGED = 4,
     AW_ERR_NAN = 5,
     AW_ERR_STATE = 6,
-    AW_ERR_UNSUPPORTED = 7
+    AW_ERR_UNSUPPORTED = 7,
+    AW_ERR_IO = 8  /* a file could not be written */
 } aw_status;
 
 /* Data channels, numbered as the reference's DataChannel enum (MSBG.cuh:12-50).
@@ -283,6 +284,32 @@ aw_status aw_flip_rebuild_levels(aw_flip* f, const int32_t* h_thresholds, int32_
  * velocity transfer keeps unit particle mass.  h_phase = NULL returns to one phase (beta = 1).
  * The differentiable rollout does not take a phase.  syncs. */
 aw_status aw_flip_set_phase(aw_flip* f, const float* h_phase, float rho0, float rho1);
+
+/* ---- inspection: dense resampling and binary VTK (vtx_visualization.cuh:8-218) ----------------
+ * The lattice has out_dims[0] x out_dims[1] x out_dims[2] points over the domain, x fastest;
+ * point (i, j, k) sits at domain_min + (i + 0.5) * spacing with spacing = domain extent / out_dims
+ * (float).  aw_resample_lattice reports origin (point 0) and spacing for the VTK header. */
+aw_status aw_resample_lattice(aw_msbg* g, const int32_t out_dims[3], float origin[3], float spacing[3]);
+/* sampleMSBG (vtx_visualization.cuh:8-62): a cell channel (PRESSURE, DIVERGENCE, DISTANCE_FIELD,
+ * VORTICITY or CELL_TYPE) at every lattice point: the value of the level-0 cell holding it, 0 in
+ * inactive blocks.  d_out: one float per point.  Corrected: domain_min is honoured.  The FLIP step
+ * leaves its pressure in PRESSURE (0 in air cells). */
+aw_status aw_resample_cells(aw_msbg* g, int32_t channel, const int32_t out_dims[3], float* d_out, aw_stream s);
+/* The MAC velocity (VELOCITY_*, or VELOCITY_OLD_* when old) at every lattice point, with
+ * aw_sample_velocity's trilinear rule; d_out: float3 per point.  No counterpart in the reference. */
+aw_status aw_resample_velocity(aw_msbg* g, int32_t old, const int32_t out_dims[3], float* d_out, aw_stream s);
+/* exportUniformPressure_VTK (vtx_visualization.cuh:64-127) in legacy VTK BINARY encoding (big
+ * endian): STRUCTURED_POINTS with ncomp 1 (SCALARS) or 3 (VECTORS) floats per point, x fastest.
+ * Host data.  AW_ERR_IO if the file cannot be written. */
+aw_status aw_vtk_write_structured_points(const char* path, const int32_t dims[3], const float origin[3],
+                                         const float spacing[3], const char* name, int32_t ncomp, const float* h_data);
+/* exportMultigrid_VTK (vtx_visualization.cuh:129-195), binary: one hexahedron per block with its
+ * level as CELL_DATA refineLevel (-1 for inactive blocks).  syncs. */
+aw_status aw_vtk_write_blocks(aw_msbg* g, const char* path);
+/* exportParticles_VTK (vtx_visualization.cuh:197-218), binary POLYDATA: n float3 host positions as
+ * vertices, with one optional float per particle (h_scalar, may be NULL) named `name`. */
+aw_status aw_vtk_write_particles(const char* path, const float* h_pos, int64_t n, const char* name,
+                                 const float* h_scalar);
 
 /* ---- projection and adjoints (no counterpart in the reference) ------------------------------
  * The vector-Jacobian products differentiate the forward calls with their discrete decisions
