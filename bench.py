@@ -235,7 +235,7 @@ def run_ours(args, ws, rank, local):
     p2g_gbs = p2g_bytes / (p2g_ms / 1e3) / 1e9
     g2p_gbs = g2p_bytes / (g2p_ms / 1e3) / 1e9
 
-    resample = resample_bench(g, aw)
+    resample = None if args.skip_resample else resample_bench(g, aw)
 
     # e2e through the drop-in C ABI with host buffers: every step uploads its positions and
     # velocities from pinned host memory, runs aw_p2g (sort + P2G), the backup and aw_g2p, and reads
@@ -340,7 +340,8 @@ def run_ours(args, ws, rank, local):
         line["flip_256"] = flip256
     if two_phase is not None:
         line["two_phase_128"] = two_phase
-    line["resample_256"] = resample
+    if resample is not None:
+        line["resample_256"] = resample
     print(json.dumps(line), flush=True)
 
 
@@ -508,6 +509,7 @@ def main():
     ap.add_argument("--skip-cpu", action="store_true")
     ap.add_argument("--skip-flip256", action="store_true", help="skip the dam_drop2_256 FLIP steps/s section")
     ap.add_argument("--skip-two-phase", action="store_true", help="skip the two-phase dam_drop_128 section")
+    ap.add_argument("--skip-resample", action="store_true", help="skip the 256^3 resampling section")
     ap.add_argument("--poisson-only", action="store_true",
                     help="only the poisson_256 projection comparison (for profiling the solver)")
     ap.add_argument("--poisson-solve-once", action="store_true",
