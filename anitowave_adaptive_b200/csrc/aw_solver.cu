@@ -496,6 +496,10 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
     stage_data<R>(S, SrcX{x}, bvec, W, P.check_fluid ? fluid : nullptr);
     __syncthreads();
     const int my_slot = GM == 1 ? 0 : min((int)threadIdx.x / n3, G - 1);
+    // The per-slot residual maximum feeds the early exit and the activation of neighbours.  With no
+    // activation output and no exit possible (at most two sweeps and a reduction target below 1:
+    // the first sweep only records the initial residual), it is skipped with its two barriers.
+    const bool track = status_next || (P.target > 0.f && (P.iters > 2 || (P.iters == 2 && P.target >= 1.f)));
     for (int bi = 0; bi < P.iters; ++bi) {
         float lmax = 0.f;
 #pragma unroll
@@ -546,6 +550,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
             }
             __syncthreads();
         }
+        if (!track) continue;
         slot_max(&Z.smr[my_slot], n3, lmax);
         __syncthreads();
         // per-slot early exit (block-uniform); smr keeps the last executed sweep's max
