@@ -102,6 +102,7 @@ struct SmoothParams {
     float omega, target, theta;
     int iters;
     int check_fluid;
+    int reverse;  // visit the cell colours black, red (the adjoint order of red, black)
 };
 
 __host__ __device__ inline int xi3(int x, int y, int z, int R2) { return (x + 1) + R2 * ((y + 1) + R2 * (z + 1)); }
@@ -508,6 +509,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
             // smaller blocks keep one thread per cell so that a slot's threads stay contiguous
             constexpr bool HALF = GM == 1 && R >= 2;
             constexpr int NC = HALF ? n3 / 2 : GM * n3;
+            const int cc = P.reverse ? 1 - col : col;
 #pragma unroll
             for (int t0 = 0; t0 < NC; t0 += NT) {
                 const int t = t0 + threadIdx.x;
@@ -517,7 +519,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
                     sl = 0;
                     cy = (t / (R / 2)) % R;
                     cz = t / (R / 2 * R);
-                    cx = 2 * (t % (R / 2)) + ((cy + cz + col) & 1);
+                    cx = 2 * (t % (R / 2)) + ((cy + cz + cc) & 1);
                     i = cx + R * (cy + R * cz);
                 } else {
                     sl = t / n3;
@@ -527,7 +529,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
                     cz = i / Gm::rr;
                 }
                 if (sl >= G || sb[sl] < 0 || Z.sdone[sl]) continue;
-                if (!HALF && ((cx + cy + cz) & 1) != col) continue;
+                if (!HALF && ((cx + cy + cz) & 1) != cc) continue;
                 if (P.check_fluid && !S.fluid(sl, i)) continue;
                 float* xs = S.xs + sl * Gm::X3;
                 const float* bs = S.fs + sl * Gm::FS;
@@ -1408,15 +1410,19 @@ static aw_status zero_x(aw_solver* S, int m, cudaStream_t s) {
     return AW_OK;
 }
 
-static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t s) {
+// Red-black block Gauss-Seidel on level m.  The post-smoothing of an FV V-cycle (reverse) runs the
+// adjoint order: block colours and cell colours black before red, so that the V-cycle is a
+// symmetric preconditioner for CG.  Reference mode keeps the reference's order (VCycle.cuh:251-304).
+static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t s, bool post = false) {
     MGLevel& L = S->lv[m];
     const int cf = fv(S) ? 1 : 0;
+    const int rev = post && fv(S) ? 1 : 0;
     if (L.dense) {
         DenseArgs A{dview(L), {L.W[0].p, L.W[1].p, L.W[2].p}, L.fluid.p};
         size_t n = L.ncell();
         for (int it = 0; it < iterations; ++it)
-            for (int col = 0; col < 2; ++col) {
-                k_dense_smooth<<<nblk(n), 256, 0, s>>>(A, L.x.p, L.b.p, col, S->d.omega);
+            for (int k = 0; k < 2; ++k) {
+                k_dense_smooth<<<nblk(n), 256, 0, s>>>(A, L.x.p, L.b.p, rev ? 1 - k : k, S->d.omega);
                 AW_LAUNCH();
             }
         return AW_OK;
@@ -1425,13 +1431,14 @@ static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t 
     // a negative activation threshold keeps every block active: no status arrays
     const bool act = S->d.theta >= 0.f;
     if (act) AW_CUDA(cudaMemsetAsync(L.status[0].p, 1, nb, s));
-    SmoothParams P{S->d.omega, S->d.target_reduction, S->d.theta, S->d.block_iterations, cf};
+    SmoothParams P{S->d.omega, S->d.target_reduction, S->d.theta, S->d.block_iterations, cf, rev};
     LevelView V = lview(S, m);
     XStore x = xstore(S, m);
     int cur = 0;
     for (int it = 0; it < iterations; ++it) {
         if (act) AW_CUDA(cudaMemsetAsync(L.status[cur ^ 1].p, 0, nb, s));
-        for (int rb = 0; rb < 2; ++rb) {
+        for (int k = 0; k < 2; ++k) {
+            const int rb = rev ? 1 - k : k;
             if (!L.ndesc[rb]) continue;
             k_smooth<<<L.ndesc[rb], 256, L.smem_smooth, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, rb),
                                                               act ? L.status[cur].p : nullptr,
@@ -1523,7 +1530,7 @@ static aw_status vcycle(aw_solver* S, int m, cudaStream_t s) {
     AW_TRY(zero_x(S, m + 1, s));
     AW_TRY(vcycle(S, m + 1, s));
     AW_TRY(prolong_level(S, m, s));
-    AW_TRY(smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.post_smooth, s));
+    AW_TRY(smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.post_smooth, s, true));
     return AW_OK;
 }
 

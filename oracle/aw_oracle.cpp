@@ -639,15 +639,19 @@ void build_hierarchy(Ctx& C, const double* bbar0[3], const uint8_t* fluid0, cons
 // ----------------------------------------------------------------------------------------------
 // Smoother (Smoother.cuh:105-202, 249-291) — block red-black on block parity, block-local
 // red-black Gauss-Seidel sweeps with early exit, adaptive activation with threshold theta.
+// post (FV mode): the adjoint order, block and cell colours black before red, which makes the
+// V-cycle a symmetric preconditioner; reference mode keeps one order (VCycle.cuh:251-304).
 // ----------------------------------------------------------------------------------------------
-void smooth_level(Ctx& C, int m, int iterations) {
+void smooth_level(Ctx& C, int m, int iterations, bool post = false) {
     const Geo& g = C.g;
     Lvl& L = C.lv[m];
     int nb = g.nb();
     const double w = C.P.omega;
+    const int rev = post && C.P.mode == 0 ? 1 : 0;
     if (L.dense) {
         for (int it = 0; it < iterations; ++it)
-            for (int col = 0; col < 2; ++col) {
+            for (int k2 = 0; k2 < 2; ++k2) {
+                const int col = rev ? 1 - k2 : k2;
 #pragma omp parallel for collapse(2) schedule(static)
                 for (int k = 0; k < L.D[2]; ++k)
                     for (int j = 0; j < L.D[1]; ++j)
@@ -670,7 +674,8 @@ void smooth_level(Ctx& C, int m, int iterations) {
         for (int b = 0; b < nb; ++b) any |= active[b] != 0;
         if (!any) break;
         std::fill(next.begin(), next.end(), 0);
-        for (int rb = 0; rb < 2; ++rb) {
+        for (int k2 = 0; k2 < 2; ++k2) {
+            const int rb = rev ? 1 - k2 : k2;
             std::vector<double> maxres(nb, 0.0);
 #pragma omp parallel for schedule(dynamic, 4)
             for (int b = 0; b < nb; ++b) {
@@ -683,11 +688,11 @@ void smooth_level(Ctx& C, int m, int iterations) {
                 double init = -1.0, mr = 0.0;
                 for (int bi = 0; bi < C.P.block_iters; ++bi) {
                     mr = 0.0;
-                    for (int col = 0; col < 2; ++col)
+                    for (int k3 = 0; k3 < 2; ++k3)
                         for (int z = 0; z < r; ++z)
                             for (int y = 0; y < r; ++y)
                                 for (int x = 0; x < r; ++x) {
-                                    if ((x + y + z) % 2 != col) continue;
+                                    if ((x + y + z) % 2 != (rev ? 1 - k3 : k3)) continue;
                                     uint32_t ci = L.off[0][b] + cidx(x, y, z, r);
                                     if (!ref && !L.fluid[ci]) continue;
                                     int c[3] = {x, y, z};
@@ -873,8 +878,8 @@ void vcycle(Ctx& C, int m) {
     std::fill(C.lv[m + 1].x.begin(), C.lv[m + 1].x.end(), 0.0);
     vcycle(C, m + 1);
     prolong_level(C, m);
-    if (L.dense) smooth_level(C, m, C.P.dense_sweeps);
-    else smooth_level(C, m, C.P.post);
+    if (L.dense) smooth_level(C, m, C.P.dense_sweeps, true);
+    else smooth_level(C, m, C.P.post, true);
 }
 
 double norm2(const std::vector<double>& v) {

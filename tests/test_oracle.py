@@ -256,3 +256,29 @@ def test_pcg_and_defect_correction_agree():
     assert h1[-1] < 1e-12 and h2[-1] < 1e-12
     assert len(h2) <= len(h1)
     assert np.linalg.norm((p1 - p2) * fluid) <= 1e-9 * np.linalg.norm(p1 * fluid)
+
+
+def test_fv_vcycle_is_a_symmetric_preconditioner():
+    """With zero initial guess and no early exit the FV V-cycle is a linear map b -> x.  Post-smoothing
+    in the adjoint order (colours black before red) makes that map symmetric, as conjugate gradients
+    needs of its preconditioner: <V b1, b2> = <b1, V b2>."""
+    S, lv, O = small_scene(64)
+    assert len(np.unique(lv)) == 2
+    rng = np.random.default_rng(7)
+    n = int(O.tot0[0])
+    _, _, cnt = O.p2g(S.pos, S.vel)
+    fluid = (cnt > 0).astype(np.uint8)
+    O.set_params(mode=0, target=0.0)
+    O.build(fluid=fluid)
+
+    def V(b):
+        O.set(0, 0, np.zeros(n))
+        O.set(0, 1, b)
+        O.vcycle()
+        return O.get(0, 0)
+
+    b1 = rng.standard_normal(n) * fluid
+    b2 = rng.standard_normal(n) * fluid
+    x1, x2 = V(b1), V(b2)
+    assert abs(x1 @ b2 - b1 @ x2) < 1e-10 * abs(x1 @ b2)
+    assert x1 @ b1 < 0  # negative definite like A
