@@ -1560,10 +1560,11 @@ extern "C" aw_status aw_solver_default_desc(int32_t mode, aw_solver_desc* d) {
         d->theta = 1e-4f;             // Smoother.cuh:286
     } else {
         d->block_iterations = 2;
-        // Mild over-relaxation: with the V-cycle preconditioning CG, 1.12 reaches 1e-6 on the 4-level
-        // poisson_256 layout in 5 iterations instead of 6 and the dam_drop FLIP projections in fewer
-        // too; much above it the V-cycle loses its smoothing (1.4 needs more iterations than 1.0).
-        d->omega = 1.12f;
+        // Over-relaxed block Gauss-Seidel.  With the symmetric V-cycle preconditioning CG, 1.35
+        // reaches 1e-6 on the 4-level poisson_256 layout in 5 iterations (6 at 1.0) and needs 7
+        // instead of 9 on the 34.7M-particle dam_drop2_256 step; at 1.5 and above the smoothing
+        // degrades and the iteration counts rise again.
+        d->omega = 1.35f;
         d->target_reduction = 0.33f;
         d->theta = -1.0f;  // every block stays active (no residual-threshold deactivation)
     }

@@ -162,12 +162,12 @@ class Oracle:
 
     def set_params(self, mode=0, pre=2, post=2, coarsest_iters=50, block_iters=None, dense_sweeps=2,
                    omega=None, target=0.33, theta=None, lam=1.0):
-        """Defaults follow the library's: FV mode (block_iters 2, omega 1.12 as a float32, every
+        """Defaults follow the library's: FV mode (block_iters 2, omega 1.35 as a float32, every
         block active: theta -1); reference mode (Smoother.cuh:9-11,286: block_iters 10, omega
         0.85714, theta 1e-4)."""
         ref = mode == 1
         block_iters = (10 if ref else 2) if block_iters is None else block_iters
-        omega = (0.85714 if ref else float(np.float32(1.12))) if omega is None else omega
+        omega = (0.85714 if ref else float(np.float32(1.35))) if omega is None else omega
         theta = (1e-4 if ref else -1.0) if theta is None else theta
         lib().oc_set_params(self.h, mode, pre, post, coarsest_iters, block_iters, dense_sweeps, omega, target,
                             theta, lam)
