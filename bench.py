@@ -418,7 +418,7 @@ def flip256_bench(steps=5, warmup=2):
                 st.append(F.stats())
             e1.record()
             torch.cuda.synchronize()
-        except aw.AWError as err:  # the plain FP32 V-cycle iteration does not converge on this layout
+        except aw.AWError as err:  # a form that does not reach its tolerance is reported as such
             torch.cuda.synchronize()
             out[name] = {"tolerance": tol, "converged": False, "error": str(err), "cycles": F.stats()["cycles"],
                          "residual": F.stats()["residual"]}
