@@ -291,7 +291,7 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
     }
 }
 
-constexpr int P2G_THREADS = 256;
+constexpr int P2G_THREADS = 512;
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
