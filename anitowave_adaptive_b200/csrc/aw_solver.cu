@@ -73,6 +73,8 @@ struct aw_solver {
     bool exact = false;
     aw::DBuf<double> M, Minv;
     aw::DBuf<int> ex_idx, ex_n, ex_pos;
+    aw::DBuf<uint8_t> ex_prev;  // coarsest fluid flags of the last factorisation (per position)
+    bool coef_dirty = true;     // coefficients changed since the last factorisation
     // level-0 bindings for the current solve
     float* x0 = nullptr;
     const float* b0 = nullptr;
@@ -1105,9 +1107,27 @@ __device__ inline float uni_W(const Uniform& U, int p, int a, int hi) {
 
 // One CTA: enumerate fluid cells, assemble -A, regularise Neumann components, Cholesky, and
 // write Minv = -( -A + reg )^-1 so that x = Minv b.  ex_n[0] = n (or -1 when n > EXACT_CAP).
+// When the fluid flags match those of the last factorisation (prev) and the coefficients did not
+// change (force == 0), the factorisation in place is still exact and the kernel returns at once.
 __global__ void __launch_bounds__(512) k_coarse_factor(Uniform U, int* pos_of, int* idx, int* ex_n, double* M,
-                                                       double* Minv) {
-    __shared__ int cnt;
+                                                       double* Minv, uint8_t* prev, int force) {
+    __shared__ int cnt, diff;
+    {
+        const int np0 = U.D[0] * U.D[1] * U.D[2];
+        if (threadIdx.x == 0) diff = force;
+        __syncthreads();
+        for (int p = threadIdx.x; p < np0; p += blockDim.x) {
+            const int ci = uni_cell(U, p);
+            const uint8_t f = (ci >= 0 && U.fluid[ci]) ? 1 : 0;
+            if (f != prev[p]) diff = 1;
+        }
+        __syncthreads();
+        if (!diff) return;
+        for (int p = threadIdx.x; p < np0; p += blockDim.x) {
+            const int ci = uni_cell(U, p);
+            prev[p] = (ci >= 0 && U.fluid[ci]) ? 1 : 0;
+        }
+    }
     __shared__ int lab[EXACT_CAP];
     __shared__ int dir[EXACT_CAP];
     __shared__ double dsum[EXACT_CAP];
@@ -1616,6 +1636,7 @@ static aw_status build_coefficients(aw_solver* S, cudaStream_t s) {
 
 extern "C" aw_status aw_solver_update_coefficients(aw_solver* S, aw_stream s) {
     AW_CHECK_ARG(S, "null solver");
+    S->coef_dirty = true;
     return build_coefficients(S, (cudaStream_t)s);
 }
 
@@ -1746,6 +1767,8 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
             AW_TRY(S->Minv.alloc((size_t)EXACT_CAP * EXACT_CAP));
             AW_TRY(S->ex_idx.alloc(EXACT_CAP));
             AW_TRY(S->ex_pos.alloc(npos));
+            AW_TRY(S->ex_prev.alloc(npos));
+            AW_CUDA(cudaMemset(S->ex_prev.p, 0xFF, npos));
             AW_TRY(S->ex_n.alloc(1));
             AW_CUDA(cudaMemset(S->ex_n.p, 0, sizeof(int)));
             S->exact = true;
@@ -1805,7 +1828,9 @@ extern "C" aw_status aw_solver_setup(aw_solver* S, const uint8_t* d_fluid, aw_st
     }
     if (S->exact) {
         Uniform U = uniform_of(S, (int)S->lv.size() - 1);
-        k_coarse_factor<<<1, 512, 0, s>>>(U, S->ex_pos.p, S->ex_idx.p, S->ex_n.p, S->M.p, S->Minv.p);
+        k_coarse_factor<<<1, 512, 0, s>>>(U, S->ex_pos.p, S->ex_idx.p, S->ex_n.p, S->M.p, S->Minv.p, S->ex_prev.p,
+                                          S->coef_dirty ? 1 : 0);
+        S->coef_dirty = false;
         AW_LAUNCH();
     }
     return AW_OK;
