@@ -58,7 +58,9 @@ __global__ void k_keys(LevelView L, PArr pos, int64_t n, uint32_t invalid, uint3
     float p[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
     uint32_t k = particle_key(L, p, invalid);
     keys[i] = k;
-    atomicAdd(&count[k], 1u);
+    // particles arrive mostly in last step's cell order: lanes with the same cell add once
+    const unsigned peers = __match_any_sync(__activemask(), k);
+    if ((__ffs(peers) - 1) == (int)(threadIdx.x & 31)) atomicAdd(&count[k], (uint32_t)__popc(peers));
 }
 
 // ------------------------------------------------------------------------------------------------
