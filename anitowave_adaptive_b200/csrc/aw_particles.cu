@@ -134,7 +134,10 @@ static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* val
         k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, hist.p, ntiles);
         AW_LAUNCH();
         AW_TRY(exclusive_scan_u32(hist.p, scan_out.p, nh, tmp, s));
-        k_radix_scatter<<<(ntiles + wpb - 1) / wpb, 32 * wpb, wpb * RADIX_BINS * sizeof(uint32_t), s>>>(
+        const size_t ssm = (size_t)wpb * RADIX_BINS * sizeof(uint32_t);
+        if (ssm > 48 * 1024)
+            AW_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+        k_radix_scatter<<<(ntiles + wpb - 1) / wpb, 32 * wpb, ssm, s>>>(
             kin, vin, kout, vout, n, shift, scan_out.p, ntiles);
         AW_LAUNCH();
         std::swap(kin, kout);
