@@ -296,7 +296,7 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
     }
 }
 
-constexpr int P2G_THREADS = 512;
+constexpr int P2G_THREADS = 512;  // the most threads a P2G CTA is launched with
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
@@ -559,18 +559,27 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             AW_CUDA(cudaMemsetAsync(acc.P[a], 0, G.tot[1 + a] * sizeof(float), s));
         }
     }
-    int maxres = 0;
-    for (int r : G.h_res) maxres = std::max(maxres, r);
+    int maxres = 0, minres = 1 << 30;
+    for (int r : G.h_res)
+        if (r) {
+            maxres = std::max(maxres, r);
+            minres = std::min(minres, r);
+        }
     const size_t smem = (size_t)(ph ? 9 : 6) * tile_axis(maxres) * sizeof(float);
+    // 512 threads walk a block's particles in half the rounds of 256 (0.64 -> 0.61 ms on the
+    // 3-level dam_drop_128).  A grid with one-cell blocks keeps 256: thousands of particles of such
+    // a block share a tile of 18 faces per axis, and twice the threads on it contend more (the
+    // 4-level dam_drop2_256 P2G takes 6.0 ms with 512 against 5.2 ms with 256).
+    const int nthreads = minres >= 2 ? P2G_THREADS : 256;
     if (n > 0) {
         if (ph) {
             if (smem > 48 * 1024)
                 AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_p2g_own<true><<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase);
+            k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase);
         } else {
             if (smem > 48 * 1024)
                 AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_p2g_own<false><<<G.nb, P2G_THREADS, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr);
+            k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr);
         }
         AW_LAUNCH();
     }
