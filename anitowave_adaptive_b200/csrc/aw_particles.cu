@@ -320,7 +320,8 @@ __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[
 template <bool PH>
 __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
-                                                 const uint32_t* __restrict__ pid, const float* __restrict__ phase) {
+                                                 const uint32_t* __restrict__ pid, const float* __restrict__ phase,
+                                                 int smem_floats) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ int cross;
@@ -340,7 +341,17 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     float* am = sm;           // 3 TA mass
     float* ap = sm + 3 * TA;  // 3 TA momentum
     float* aq = sm + 6 * TA;  // 3 TA phase (PH)
-    for (int i = threadIdx.x; i < (PH ? 9 : 6) * TA; i += blockDim.x) sm[i] = 0.f;
+    // Blocks of one or two cells per edge hold thousands of particles on a tile of 18 or 48 faces
+    // per axis: each warp then deposits into a private copy of the tile, and the copies are summed
+    // before the flush, so that warps do not contend for the same few addresses.
+    const int TW = (PH ? 9 : 6) * TA;
+    const bool priv = r <= 2 && (int)(blockDim.x >> 5) * TW <= smem_floats;
+    const int ntile = priv ? (int)(blockDim.x >> 5) * TW : TW;
+    float* tw = priv ? sm + (threadIdx.x >> 5) * TW : sm;
+    float* amw = tw;
+    float* apw = tw + 3 * TA;
+    float* aqw = tw + 6 * TA;
+    for (int i = threadIdx.x; i < ntile; i += blockDim.x) sm[i] = 0.f;
     if (threadIdx.x == 0) cross = 0;
     __syncthreads();
     if (threadIdx.x < 27) {
@@ -408,9 +419,9 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                             const float wgt = tt * tt * tt;
                             const int e = base + da + d1 * R1 + d2 * R1 * R2;
                             if (tt > 0.f) {
-                                atomicAdd(&am[e], wgt);
-                                atomicAdd(&ap[e], wgt * va);
-                                if (PH) atomicAdd(&aq[e], wgt * ph);
+                                atomicAdd(&amw[e], wgt);
+                                atomicAdd(&apw[e], wgt * va);
+                                if (PH) atomicAdd(&aqw[e], wgt * ph);
                             }
                         }
                     }
@@ -462,6 +473,14 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     }
     if (qn > 0 && lane < qn) p2g_cross_pair<PH>(L, cb, nres, qv[lane], qd[lane], p0, soa, n, acc, pid, phase);
     __syncthreads();
+    if (priv) {
+        for (int i = threadIdx.x; i < TW; i += blockDim.x) {
+            float v = sm[i];
+            for (int c = TW; c < ntile; c += TW) v += sm[c + i];
+            sm[i] = v;
+        }
+        __syncthreads();
+    }
     // flush: every nonzero tile entry into each same-resolution copy of its face
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -565,21 +584,27 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             maxres = std::max(maxres, r);
             minres = std::min(minres, r);
         }
-    const size_t smem = (size_t)(ph ? 9 : 6) * tile_axis(maxres) * sizeof(float);
+    const int NVt = ph ? 9 : 6;
+    // the largest tile, or one private tile per warp for blocks of at most two cells per edge
     // 512 threads walk a block's particles in half the rounds of 256 (0.64 -> 0.61 ms on the
     // 3-level dam_drop_128).  A grid with one-cell blocks keeps 256: thousands of particles of such
     // a block share a tile of 18 faces per axis, and twice the threads on it contend more (the
     // 4-level dam_drop2_256 P2G takes 6.0 ms with 512 against 5.2 ms with 256).
     const int nthreads = minres >= 2 ? P2G_THREADS : 256;
+    const size_t smem_f = std::max((size_t)NVt * tile_axis(maxres),
+                                   minres <= 2 ? (size_t)(nthreads / 32) * NVt * tile_axis(std::min(maxres, 2)) : 0);
+    const size_t smem = smem_f * sizeof(float);
     if (n > 0) {
         if (ph) {
             if (smem > 48 * 1024)
                 AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase);
+            k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase,
+                                                           (int)smem_f);
         } else {
             if (smem > 48 * 1024)
                 AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr);
+            k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr,
+                                                            (int)smem_f);
         }
         AW_LAUNCH();
     }
