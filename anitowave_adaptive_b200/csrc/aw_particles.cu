@@ -818,11 +818,13 @@ __global__ void k_build_tiles2(LevelView L, Field3 un, Field3 uo, const uint32_t
 }
 
 // Trilinear sample of component a at X from the ghosted tiles (same stencil as sample_comp).
-__device__ inline float tile_interp(const float* __restrict__ t, int a, int r, const float o[3], float h, const float X[3]) {
+// invh = 1 / (the block's cell size), computed once per block by the caller
+__device__ inline float tile_interp(const float* __restrict__ t, int a, int r, const float o[3], float invh,
+                                   const float X[3]) {
     const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-    float sA = (X[a] - o[a]) / h;
-    float s1 = (X[t1] - o[t1]) / h - 0.5f;
-    float s2 = (X[t2] - o[t2]) / h - 0.5f;
+    float sA = (X[a] - o[a]) * invh;
+    float s1 = (X[t1] - o[t1]) * invh - 0.5f;
+    float s2 = (X[t2] - o[t2]) * invh - 0.5f;
     sA = fminf(fmaxf(sA, 0.f), (float)r);
     s1 = fminf(fmaxf(s1, -1.f), (float)r);
     s2 = fminf(fmaxf(s2, -1.f), (float)r);
@@ -853,7 +855,7 @@ __device__ inline float sample_tiles(const LevelView& L, const uint32_t* __restr
     float o[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) o[k] = forigin(L.g, k, cb[k]);
-    return tile_interp(tiles + toff[b], a, r, o, h, X);
+    return tile_interp(tiles + toff[b], a, r, o, 1.f / h, X);
 }
 
 // ---- TMA bulk copies (cp.async.bulk, no multicast) and a bounded mbarrier wait ----------------
@@ -918,6 +920,7 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
     int cb[3];
     bcoord(g, b, cb);
     const float h = fcell(g, r);
+    const float invh = 1.f / h;
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
@@ -942,8 +945,8 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
             if (i < p1)
 #pragma unroll
                 for (int a = 0; a < 3; ++a) {
-                    const float vn = tile_interp(tn, a, r, o, h, X[k]);
-                    const float vo = tile_interp(to, a, r, o, h, X[k]);
+                    const float vn = tile_interp(tn, a, r, o, invh, X[k]);
+                    const float vo = tile_interp(to, a, r, o, invh, X[k]);
                     soa[(int64_t)(3 + a) * n + i] = alpha * (Vv[k][a] + (vn - vo)) + (1.f - alpha) * vn;
                 }
         }
@@ -953,12 +956,12 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
 // RK3 advection of the sorted particles of one block: the block's u_new tile is staged in shared
 // memory by one bulk copy; stage points that leave the block sample the neighbour's tile in global
 // memory (same arithmetic as sample_tiles).
-__device__ inline float sample_local(const LevelView& L, int b, const int cb[3], int r, const float o[3], float h,
+__device__ inline float sample_local(const LevelView& L, int b, const int cb[3], int r, const float o[3], float invh,
                                      const float* __restrict__ tl, const uint32_t* __restrict__ toff,
                                      const float* __restrict__ tg, int a, const float X[3]) {
     int pc[3];
     point_block(L.g, X, pc);
-    if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) return tile_interp(tl, a, r, o, h, X);
+    if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) return tile_interp(tl, a, r, o, invh, X);
     return sample_tiles(L, toff, tg, a, X);
 }
 
@@ -986,6 +989,7 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
     int cb[3];
     bcoord(g, b, cb);
     const float h = fcell(g, r);
+    const float invh = 1.f / h;
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
@@ -995,15 +999,15 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
 #pragma unroll
         for (int a = 0; a < 3; ++a) x[a] = soa[(int64_t)a * n + i];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) k1[a] = tile_interp(sm, a, r, o, h, x);
+        for (int a = 0; a < 3; ++a) k1[a] = tile_interp(sm, a, r, o, invh, x);
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.5f * dt * k1[a];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) k2[a] = sample_local(L, b, cb, r, o, h, sm, toff, tn_g, a, y);
+        for (int a = 0; a < 3; ++a) k2[a] = sample_local(L, b, cb, r, o, invh, sm, toff, tn_g, a, y);
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.75f * dt * k2[a];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) k3[a] = sample_local(L, b, cb, r, o, h, sm, toff, tn_g, a, y);
+        for (int a = 0; a < 3; ++a) k3[a] = sample_local(L, b, cb, r, o, invh, sm, toff, tn_g, a, y);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float v = (2.f / 9.f) * k1[a] + (3.f / 9.f) * k2[a] + (4.f / 9.f) * k3[a];
@@ -1231,10 +1235,10 @@ aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t
 __device__ inline void tile_interp_vjp(const float* __restrict__ t, float* tb, int a, int r, const float o[3], float h,
                                        const float X[3], float gbar, float dX[3]) {
     const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-    float sA = (X[a] - o[a]) / h;
-    float s1 = (X[t1] - o[t1]) / h - 0.5f;
-    float s2 = (X[t2] - o[t2]) / h - 0.5f;
     const float rf = (float)r, invh = 1.f / h;
+    float sA = (X[a] - o[a]) * invh;
+    float s1 = (X[t1] - o[t1]) * invh - 0.5f;
+    float s2 = (X[t2] - o[t2]) * invh - 0.5f;
     const float gA = (sA > 0.f && sA < rf) ? invh : 0.f;
     const float g1 = (s1 > -1.f && s1 < rf) ? invh : 0.f;
     const float g2 = (s2 > -1.f && s2 < rf) ? invh : 0.f;
