@@ -549,7 +549,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
                 const float Ax = wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] + wB * xs[q - sz] +
                                  wT * xs[q + sz] + diag * xc;
                 const float res = bs[i] - Ax;
-                xs[q] = xc + P.omega * (res / diag);
+                xs[q] = xc + P.omega * __fdividef(res, diag);  // a smoother tolerates the 2-ulp quotient
                 lmax = fmaxf(lmax, fabsf(res));
             }
             __syncthreads();
@@ -904,7 +904,7 @@ __global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ 
     float diag;
     float ax = dense_Ax(A, x, i, j, k, &diag);
     if (fabsf(diag) < 1e-30f) return;
-    x[t] += omega * (b[t] - ax) / diag;
+    x[t] += omega * __fdividef(b[t] - ax, diag);
 }
 
 __global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const float* __restrict__ b, float* r) {
