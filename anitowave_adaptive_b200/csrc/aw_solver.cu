@@ -92,9 +92,11 @@ struct aw_solver {
     const void* cycle_b0 = nullptr;
     unsigned long long cycle_kernels = 0;
     bool use_graph = true;
+    double* h_norm = nullptr;  // pinned host word for the per-iteration residual norm
     ~aw_solver() {
         if (cycle) cudaGraphExecDestroy(cycle);
         if (cap) cudaStreamDestroy(cap);
+        if (h_norm) cudaFreeHost(h_norm);
     }
 };
 
@@ -1941,10 +1943,10 @@ extern "C" aw_status aw_vcycle_run(aw_solver* S, aw_stream s) {
 static aw_status read_norm(aw_solver* S, int nparts, cudaStream_t s, double* out) {
     k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, nparts, S->norm.p);
     AW_LAUNCH();
-    double h = 0;
-    AW_CUDA(cudaMemcpyAsync(&h, S->norm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (!S->h_norm) AW_CUDA(cudaHostAlloc((void**)&S->h_norm, sizeof(double), cudaHostAllocDefault));
+    AW_CUDA(cudaMemcpyAsync(S->h_norm, S->norm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
     AW_CUDA(cudaStreamSynchronize(s));
-    *out = std::sqrt(h);
+    *out = std::sqrt(*S->h_norm);
     return AW_OK;
 }
 
