@@ -596,13 +596,12 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     const size_t smem = smem_f * sizeof(float);
     if (n > 0) {
         if (ph) {
-            if (smem > 48 * 1024)
-                AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            // always opted in: the pair queues' static shared memory counts against the default 48 KB too
+            AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase,
                                                            (int)smem_f);
         } else {
-            if (smem > 48 * 1024)
-                AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr,
                                                             (int)smem_f);
         }
