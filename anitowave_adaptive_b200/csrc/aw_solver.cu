@@ -1776,14 +1776,13 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
             S->exact = true;
         }
     }
-    if (S->smem_max > 48 * 1024) {
+    {  // always opted in: static shared memory (k_smooth's per-slot state) counts against the default 48 KB too
         AW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_residual<SrcX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_prolong, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
     }
-    if (S->smem_max64 > 48 * 1024)
-        AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
+    AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
     if (d->precision == AW_PRECISION_MIXED) {
         const size_t nc0 = S->lv[0].ncell();
         AW_TRY(S->cg_r.alloc(nc0));
