@@ -816,6 +816,36 @@ __global__ void k_build_tiles2(LevelView L, Field3 un, Field3 uo, const uint32_t
     }
 }
 
+// u_new into tn and the FLIP increment field u_new - alpha u_old into tw, from the same sources.
+// The blend v' = alpha (v + u_new(x) - u_old(x)) + (1 - alpha) u_new(x) (G2P.cuh:11-128) equals
+// alpha v + I(u_new - alpha u_old)(x), since the trilinear interpolation I is linear: G2P then
+// stages and interpolates one tile instead of two.
+__global__ void k_build_tiles_blend(LevelView L, Field3 un, Field3 uo, float alpha, const uint32_t* __restrict__ toff,
+                                    float* __restrict__ tn, float* __restrict__ tw) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    int cb[3];
+    bcoord(L.g, b, cb);
+    const int R1 = r + 1, R2 = r + 2;
+    const int TA = (int)tile_axis(r);
+    const uint32_t o = toff[b];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            int fi[3];
+            fi[a] = rem % R1;
+            fi[t1] = (rem / R1) % R2 - 1;
+            fi[t2] = rem / (R1 * R2) - 1;
+            const uint32_t src = face_source(L, a, b, cb, r, fi);
+            const float vn = un.c[a][src];
+            tn[o + a * TA + rem] = vn;
+            tw[o + a * TA + rem] = vn - alpha * uo.c[a][src];
+        }
+    }
+}
+
 // Trilinear sample of component a at X from the ghosted tiles (same stencil as sample_comp).
 // invh = 1 / (the block's cell size), computed once per block by the caller
 __device__ inline float tile_interp(const float* __restrict__ t, int a, int r, const float o[3], float invh,
@@ -889,13 +919,13 @@ __device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* er
     return false;
 }
 
-// G2P on sorted particles.  One CTA per block: thread 0 issues two TMA bulk copies (u_new and
-// u_old ghosted tiles, 16-byte aligned), every thread waits on the mbarrier, then each particle
-// of the block interpolates both fields from shared memory and applies the FLIP blend.
+// G2P on sorted particles.  One CTA per block: thread 0 issues one TMA bulk copy of the block's
+// ghosted tile of w = u_new - alpha u_old (16-byte aligned), every thread waits on the mbarrier,
+// then each particle of the block takes v' = alpha v + I(w)(x) from shared memory.
 __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict__ soa, int64_t n,
                                                   const uint32_t* __restrict__ cs, float alpha,
-                                                  const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
-                                                  const float* __restrict__ to_g, int* err) {
+                                                  const uint32_t* __restrict__ toff, const float* __restrict__ tw_g,
+                                                  int* err) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
     const int b = blockIdx.x;
@@ -904,22 +934,18 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
     const uint32_t p0 = cs[L.off[0][b]], p1 = cs[L.off[0][b] + (uint32_t)(r * r * r)];
     if (p0 == p1) return;
     const uint32_t tb = tile_block(r);
-    float* tn = sm;
-    float* to = sm + tb;
     if (threadIdx.x == 0) mbar_init(&bar, 1);
     __syncthreads();
     if (threadIdx.x == 0) {
-        mbar_expect_tx(&bar, 2 * tb * sizeof(float));
-        tma_bulk_load(tn, tn_g + toff[b], tb * sizeof(float), &bar);
-        tma_bulk_load(to, to_g + toff[b], tb * sizeof(float), &bar);
+        mbar_expect_tx(&bar, tb * sizeof(float));
+        tma_bulk_load(sm, tw_g + toff[b], tb * sizeof(float), &bar);
     }
     const bool ok = mbar_wait_bounded(&bar, 0, err);
     if (!__syncthreads_and(ok)) return;
     const Geo& g = L.g;
     int cb[3];
     bcoord(g, b, cb);
-    const float h = fcell(g, r);
-    const float invh = 1.f / h;
+    const float invh = 1.f / fcell(g, r);
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
@@ -943,11 +969,8 @@ __global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict
             const uint32_t i = i0 + k * st;
             if (i < p1)
 #pragma unroll
-                for (int a = 0; a < 3; ++a) {
-                    const float vn = tile_interp(tn, a, r, o, invh, X[k]);
-                    const float vo = tile_interp(to, a, r, o, invh, X[k]);
-                    soa[(int64_t)(3 + a) * n + i] = alpha * (Vv[k][a] + (vn - vo)) + (1.f - alpha) * vn;
-                }
+                for (int a = 0; a < 3; ++a)
+                    soa[(int64_t)(3 + a) * n + i] = alpha * Vv[k][a] + tile_interp(sm, a, r, o, invh, X[k]);
         }
     }
 }
@@ -1068,19 +1091,19 @@ aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
     return AW_OK;
 }
 
-static size_t g2p_smem(int r) { return (size_t)2 * tile_block(r) * sizeof(float); }
-
 aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float alpha, const float* un[3],
                      const float* uo[3], cudaStream_t s) {
     if (n <= 0) return AW_OK;
     AW_TRY(ensure_tiles(G));
-    AW_TRY(build_tiles2(G, un, uo, s));
+    // u_new tiles (for the advection that follows) and the blended tiles u_new - alpha u_old
+    Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
+    k_build_tiles_blend<<<G.nb, 128, 0, s>>>(G.view0(), fa, fb, alpha, G.tile_off.p, G.tiles_new.p, G.tiles_old.p);
+    AW_LAUNCH();
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = g2p_smem(maxres);
-    if (smem > 48 * 1024) AW_CUDA(cudaFuncSetAttribute(k_g2p_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_g2p_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, alpha, G.tile_off.p, G.tiles_new.p, G.tiles_old.p,
-                                       G.err.p + 1);
+    const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
+    AW_CUDA(cudaFuncSetAttribute(k_g2p_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_g2p_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, alpha, G.tile_off.p, G.tiles_old.p, G.err.p + 1);
     AW_LAUNCH();
     k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
     AW_LAUNCH();

@@ -323,7 +323,7 @@ def run_ours(args, ws, rank, local):
                      "unit": "GB/s", "frac": p2g_gbs / hbm, "peak_kind": peak_kind,
                      "traffic": traffic.get("k_p2g_own"), "bytes_per_launch": p2g_bytes, "ms_per_launch": p2g_ms,
                      "note": "bound by shared-memory float atomics (about 25 per particle), not HBM"},
-        "roofline_g2p": {"kernel": "k_build_tiles2 + k_g2p_tile", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm,
+        "roofline_g2p": {"kernel": "k_build_tiles_blend + k_g2p_tile", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm,
                          "unit": "GB/s", "frac": g2p_gbs / hbm, "traffic": traffic.get("k_g2p_tile"),
                          "bytes_per_launch": g2p_bytes, "ms_per_launch": g2p_ms},
         "step_breakdown_ms": {k: last[k] for k in ("ms_sort", "ms_p2g", "ms_solve", "ms_g2p", "ms_advect", "ms_other")},
