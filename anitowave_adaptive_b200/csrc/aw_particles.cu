@@ -291,7 +291,7 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
                     const uint32_t fi = ob + fidx(a, f[0], f[1], f[2], rn);
                     atomicAdd(&acc.m[a][fi], w);
                     atomicAdd(&acc.P[a][fi], w * V[a]);
-                    if (PH) atomicAdd(&acc.Phi[a][fi], w * ph);
+                    if (PH && ph != 0.f) atomicAdd(&acc.Phi[a][fi], w * ph);
                 }
     }
 }
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                             if (tt > 0.f) {
                                 atomicAdd(&amw[e], wgt);
                                 atomicAdd(&apw[e], wgt * va);
-                                if (PH) atomicAdd(&aqw[e], wgt * ph);
+                                if (PH && ph != 0.f) atomicAdd(&aqw[e], wgt * ph);  // phase-0 particles add nothing
                             }
                         }
                     }
@@ -515,7 +515,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
                 const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], r);
                 atomicAdd(&acc.m[a][fi], mv);
                 atomicAdd(&acc.P[a][fi], pv);
-                if (PH) atomicAdd(&acc.Phi[a][fi], qv2);
+                if (PH && qv2 != 0.f) atomicAdd(&acc.Phi[a][fi], qv2);
             }
         }
     }
