@@ -986,7 +986,15 @@ __global__ void k_coarse_fluid(LevelView F, LevelView K, const uint8_t* __restri
 }
 
 // coarse 1/rho per face: mean of the 4 fine faces (copy when the block keeps one cell)
-__global__ void k_coarse_bbar(LevelView F, LevelView K, int a, const float* __restrict__ bf, float* __restrict__ bcv) {
+// the three axes in one launch: axis = blockIdx.y
+struct Face3 {
+    float* p[3];
+};
+
+__global__ void k_coarse_bbar(LevelView F, LevelView K, Face3 bfs, Face3 bcvs) {
+    const int a = blockIdx.y;
+    const float* __restrict__ bf = bfs.p[a];
+    float* __restrict__ bcv = bcvs.p[a];
     const int b = blockIdx.x;
     const int rc = K.res[b], rf = F.res[b];
     if (!rc) return;
@@ -1019,7 +1027,10 @@ __global__ void k_coarse_bbar(LevelView F, LevelView K, int a, const float* __re
 
 // finite-volume conductance W = geo * bbar: interior h, wall 0, absent neighbour h (Dirichlet),
 // same level h, coarser neighbour (2/3) h, finer neighbour (4/3) h  (h = the block's cell size)
-__global__ void k_conductance(LevelView L, int a, const float* __restrict__ bbar, float* __restrict__ W) {
+__global__ void k_conductance(LevelView L, Face3 bbars, Face3 Ws) {
+    const int a = blockIdx.y;
+    const float* __restrict__ bbar = bbars.p[a];
+    float* __restrict__ W = Ws.p[a];
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
@@ -1609,26 +1620,30 @@ static aw_status build_coefficients(aw_solver* S, cudaStream_t s) {
     for (int m = 0; m < S->nmsbg; ++m) {
         MGLevel& L = S->lv[m];
         LevelView V = lview(S, m);
-        for (int a = 0; a < 3; ++a) {
-            if (m == 0) {
+        Face3 bb{{L.bbar[0].p, L.bbar[1].p, L.bbar[2].p}};
+        if (m == 0) {
+            for (int a = 0; a < 3; ++a)
                 AW_CUDA(cudaMemcpyAsync(L.bbar[a].p, G.ch[AW_BETA_COEFF_X + a], L.nface(a) * sizeof(float),
                                         cudaMemcpyDeviceToDevice, s));
+        } else {
+            MGLevel& P = S->lv[m - 1];
+            Face3 fb{{P.bbar[0].p, P.bbar[1].p, P.bbar[2].p}};
+            k_coarse_bbar<<<dim3(nb, 3), 128, 0, s>>>(lview(S, m - 1), V, fb, bb);
+            AW_LAUNCH();
+        }
+        if (!ref) {
+            k_conductance<<<dim3(nb, 3), 128, 0, s>>>(V, bb, Face3{{L.W[0].p, L.W[1].p, L.W[2].p}});
+            AW_LAUNCH();
+            continue;
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (m == 0) {
+                AW_CUDA(cudaMemcpyAsync(L.W[a].p, L.bbar[a].p, L.nface(a) * sizeof(float), cudaMemcpyDeviceToDevice,
+                                        s));
             } else {
-                k_coarse_bbar<<<nb, 128, 0, s>>>(lview(S, m - 1), V, a, S->lv[m - 1].bbar[a].p, L.bbar[a].p);
-                AW_LAUNCH();
-            }
-            if (ref) {
-                if (m == 0) {
-                    AW_CUDA(cudaMemcpyAsync(L.W[a].p, L.bbar[a].p, L.nface(a) * sizeof(float),
-                                            cudaMemcpyDeviceToDevice, s));
-                } else {
-                    AW_CUDA(cudaMemsetAsync(L.W[a].p, 0, L.nface(a) * sizeof(float), s));
-                    k_galerkin_ref<<<nb, 256, 0, s>>>(G.geo, G.level.p, a, m, S->lv[m - 1].W[a].p, L.W[a].p,
-                                                      S->lv[m - 1].off[1 + a].p, L.off[1 + a].p);
-                    AW_LAUNCH();
-                }
-            } else {
-                k_conductance<<<nb, 128, 0, s>>>(V, a, L.bbar[a].p, L.W[a].p);
+                AW_CUDA(cudaMemsetAsync(L.W[a].p, 0, L.nface(a) * sizeof(float), s));
+                k_galerkin_ref<<<nb, 256, 0, s>>>(G.geo, G.level.p, a, m, S->lv[m - 1].W[a].p, L.W[a].p,
+                                                  S->lv[m - 1].off[1 + a].p, L.off[1 + a].p);
                 AW_LAUNCH();
             }
         }
