@@ -98,6 +98,12 @@ __global__ void k_beta_sync(LevelView L, float* b0, float* b1, float* b2) {
     }
 }
 
+template <class PT>
+__global__ void k_zero_air(PT* p, const uint8_t* __restrict__ fluid, size_t n) {
+    size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && !fluid[i]) p[i] = PT(0);
+}
+
 // the step's pressure into the PRESSURE channel (0 in air cells), for inspection
 template <class PT>
 __global__ void k_store_pressure(const PT* __restrict__ p, const uint8_t* __restrict__ fluid, size_t n, float* out) {
@@ -583,7 +589,8 @@ static aw_status copy_d2d(void* dst, const void* src, size_t bytes, cudaStream_t
 
 aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
                         const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
-                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s, const FlipPhase* fp) {
+                        StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s, const FlipPhase* fp,
+                        bool warm_start) {
     if (fp && !ids_out) return set_error(AW_ERR_INVALID_ARGUMENT, "two-phase step needs particle ids");
     float* U[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     float* UO[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
@@ -645,14 +652,20 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
         AW_TRY(aw_solver_update_coefficients(solver, (aw_stream)s));
     }
     AW_TRY(aw_solver_setup(solver, B.fluid.p, (aw_stream)s));
+    // initial guess: the previous step's pressure (air cells zeroed: they are Dirichlet p = 0), or 0
     void* p;
+    const bool warm = warm_start && B.p_warm && G.tot[0];
     if (d.precision == AW_PRECISION_MIXED) {
-        AW_CUDA(cudaMemsetAsync(B.p64.p, 0, G.tot[0] * sizeof(double), s));
+        if (warm) k_zero_air<double><<<nblk(G.tot[0]), 256, 0, s>>>(B.p64.p, B.fluid.p, G.tot[0]);
+        else AW_CUDA(cudaMemsetAsync(B.p64.p, 0, G.tot[0] * sizeof(double), s));
         p = B.p64.p;
     } else {
-        AW_CUDA(cudaMemsetAsync(B.p32.p, 0, G.tot[0] * sizeof(float), s));
+        if (warm) k_zero_air<float><<<nblk(G.tot[0]), 256, 0, s>>>(B.p32.p, B.fluid.p, G.tot[0]);
+        else AW_CUDA(cudaMemsetAsync(B.p32.p, 0, G.tot[0] * sizeof(float), s));
         p = B.p32.p;
     }
+    if (warm) AW_LAUNCH();
+    B.p_warm = false;
     int32_t cycles = 0;
     double rel = 0;
     aw_status sst = aw_solve(solver, B.rhs.p, p, &cycles, &rel, (aw_stream)s);
@@ -661,6 +674,7 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
         st->residual = rel;
     }
     if (sst != AW_OK) return sst;
+    B.p_warm = true;
     if (G.tot[0]) {
         if (d.precision == AW_PRECISION_MIXED)
             k_store_pressure<double><<<nblk(G.tot[0]), 256, 0, s>>>(B.p64.p, B.fluid.p, G.tot[0], G.ch[AW_PRESSURE]);
@@ -829,7 +843,7 @@ extern "C" aw_status aw_flip_step(aw_flip* F, aw_stream s_) {
     const FlipPhase fp{F->phase.p, F->rho0, F->rho1};
     aw_status st = flip_step_soa(F->g->st, F->solver, F->d, F->B, F->soa[c].p, F->ids[c].p, F->soa[c ^ 1].p,
                                  F->ids[c ^ 1].p, F->n, nullptr, nullptr, F->ev, &F->stats, s,
-                                 F->phase.p ? &fp : nullptr);
+                                 F->phase.p ? &fp : nullptr, /*warm_start=*/true);
     F->cur ^= 1;  // the sorted state lives in the other buffer from the gather on
     return st;
 }
@@ -859,6 +873,7 @@ extern "C" aw_status aw_flip_rebuild_levels(aw_flip* F, const int32_t* h_thresho
     AW_TRY(aw_msbg_allocate(F->g, s_));
     AW_TRY(aw_solver_create(F->g, &F->sd, &F->solver));
     AW_TRY(F->B.ensure(G));
+    F->B.p_warm = false;  // cell indices changed
     if (changed) *changed = 1;
     return AW_OK;
 }

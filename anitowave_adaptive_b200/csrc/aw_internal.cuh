@@ -186,6 +186,7 @@ struct FlipBufs {
     DBuf<float> p32, rhs, divmax;
     DBuf<double> p64;
     DBuf<uint8_t> fluid;
+    bool p_warm = false;  // p32/p64 hold the last step's pressure on the current layout
     aw_status ensure(const MsbgState& G);
 };
 
@@ -329,10 +330,12 @@ struct FlipPhase {
 };
 // fp (optional, needs ids): P2G also writes PHASE_FIELD_* and BETA_COEFF_*, and the solver's
 // coefficients are rebuilt from them before the projection.
+// warm_start: the projection starts from the previous step's pressure (B.p_warm), with air cells
+// zeroed, instead of from zero.
 aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, FlipBufs& B, const float* soa_in,
                         const uint32_t* ids_in, float* soa_out, uint32_t* ids_out, int64_t n, const uint8_t* fluid_in,
                         StepRecord* rec, cudaEvent_t* ev, aw_flip_stats* st, cudaStream_t s,
-                        const FlipPhase* fp = nullptr);
+                        const FlipPhase* fp = nullptr, bool warm_start = false);
 
 }  // namespace aw
 

@@ -265,6 +265,8 @@ typedef struct aw_flip_stats {
 aw_status aw_flip_create(aw_msbg* g, const aw_flip_desc* desc, const float* h_pos, const float* h_vel, int64_t n,
                          aw_flip** out);
 aw_status aw_flip_destroy(aw_flip* f);
+/* One step.  The pressure solve starts from the previous step's pressure (air cells zeroed) once a
+ * step on the current layout has converged, from zero otherwise. */
 aw_status aw_flip_step(aw_flip* f, aw_stream s);
 aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out);
 /* copy particle state to host in the original particle order (AoS) */
