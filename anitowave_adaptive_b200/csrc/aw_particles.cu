@@ -298,6 +298,8 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
 
 constexpr int P2G_THREADS = 512;  // the most threads a P2G CTA is launched with
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
+constexpr int P2G_SLICE = 16;  // particles of one cell per register-accumulation task
+constexpr int P2G_MAX_SLICES = 1 << 20;  // 3 * 8^3 * this stays below 2^31
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
@@ -325,6 +327,7 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ int cross;
+    __shared__ uint32_t maxcnt;
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
@@ -352,7 +355,10 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     float* apw = tw + 3 * TA;
     float* aqw = tw + 6 * TA;
     for (int i = threadIdx.x; i < ntile; i += blockDim.x) sm[i] = 0.f;
-    if (threadIdx.x == 0) cross = 0;
+    if (threadIdx.x == 0) {
+        cross = 0;
+        maxcnt = 0;
+    }
     __syncthreads();
     if (threadIdx.x < 27) {
         const int d = threadIdx.x;
@@ -368,64 +374,116 @@ __global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const floa
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
-    // lanes of a warp take particles a 32nd of the range apart, so that they sit in different cells
+    // Own particles, cell by cell.  A task is (component a, cell c, slice s): up to `slice` of c's
+    // particles (contiguous in the cell-sorted array).  Its thread sums their weights on the 2x3x3
+    // faces of component a around c in registers, then adds the 18 sums into the tile: one atomic
+    // per face and task instead of one per face and particle.  Slices hold P2G_SLICE particles
+    // unless a crowded cell would push the task count past 3 * 512 * P2G_MAX_SLICES.
+    const int nc3 = r * r * r;
+    for (int c = threadIdx.x; c < nc3; c += blockDim.x) {
+        const uint32_t cnt = cs[c0 + c + 1] - cs[c0 + c];
+        if (cnt > 0) atomicMax(&maxcnt, cnt);
+    }
+    __syncthreads();
+    const uint32_t mc = maxcnt;
+    const int nsl = (int)min((mc + P2G_SLICE - 1) / P2G_SLICE, (uint32_t)P2G_MAX_SLICES);
+    const uint32_t slice = nsl ? (mc + nsl - 1) / nsl : 0;
+    const int ntask = 3 * nc3 * nsl;
+    for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+        const int a = task / (nc3 * nsl);
+        const int rem = task - a * nc3 * nsl;
+        const int c = rem % nc3, sl = rem / nc3;  // neighbouring threads take neighbouring cells
+        const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+        if ((uint32_t)sl * slice >= ce - ca) continue;
+        const uint32_t i0 = ca + (uint32_t)sl * slice;
+        const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
+        const int t1 = a == 2 ? 0 : a + 1, t2 = a == 0 ? 2 : a - 1;
+        const int cx = c % r, cy = (c / r) % r, cz = c / (r * r);
+        const int ka = a == 0 ? cx : (a == 1 ? cy : cz);   // cell index along a
+        const int k1 = a == 0 ? cy : (a == 1 ? cz : cx);   // ... along t1
+        const int k2 = a == 0 ? cz : (a == 1 ? cx : cy);   // ... along t2
+        const float fa0 = (float)ka, f10 = (float)k1 - 0.5f, f20 = (float)k2 - 0.5f;
+        const float oa = a == 0 ? o[0] : (a == 1 ? o[1] : o[2]);
+        const float o1 = t1 == 0 ? o[0] : (t1 == 1 ? o[1] : o[2]);
+        const float o2 = t2 == 0 ? o[0] : (t2 == 1 ? o[1] : o[2]);
+        float sm_m[2][3][3], sm_p[2][3][3], sm_q[2][3][3];
+#pragma unroll
+        for (int da = 0; da < 2; ++da)
+#pragma unroll
+            for (int d1 = 0; d1 < 3; ++d1)
+#pragma unroll
+                for (int d2 = 0; d2 < 3; ++d2) {
+                    sm_m[da][d1][d2] = 0.f;
+                    sm_p[da][d1][d2] = 0.f;
+                    sm_q[da][d1][d2] = 0.f;
+                }
+        for (uint32_t i = i0; i < i1; ++i) {
+            const float qa = (soa[(int64_t)a * n + i] - oa) * invh;
+            const float q1 = (soa[(int64_t)t1 * n + i] - o1) * invh;
+            const float q2 = (soa[(int64_t)t2 * n + i] - o2) * invh;
+            const float va = soa[(int64_t)(3 + a) * n + i];
+            const float ph = PH ? phase[pid[i]] : 0.f;
+            float dA2[2], dB2[3], dC2[3];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const float dA = qa - (fa0 + (float)k);
+                dA2[k] = dA * dA;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float dB = q1 - (f10 + (float)k);
+                const float dC = q2 - (f20 + (float)k);
+                dB2[k] = dB * dB;
+                dC2[k] = dC * dC;
+            }
+#pragma unroll
+            for (int da = 0; da < 2; ++da)
+#pragma unroll
+                for (int d1 = 0; d1 < 3; ++d1) {
+                    const float dAB = dA2[da] + dB2[d1];
+#pragma unroll
+                    for (int d2 = 0; d2 < 3; ++d2) {
+                        const float tt = fmaxf(1.f - (dAB + dC2[d2]), 0.f);
+                        const float wgt = tt * tt * tt;
+                        sm_m[da][d1][d2] += wgt;
+                        sm_p[da][d1][d2] += wgt * va;
+                        if (PH) sm_q[da][d1][d2] += wgt * ph;
+                    }
+                }
+        }
+        // faces fa in {ca, ca+1} along a, f1 in {c1-1, c1, c1+1} and f2 likewise across (tile rows -1..r)
+        const int base = a * TA + ka + R1 * (k1 + R2 * k2);
+#pragma unroll
+        for (int da = 0; da < 2; ++da)
+#pragma unroll
+            for (int d1 = 0; d1 < 3; ++d1)
+#pragma unroll
+                for (int d2 = 0; d2 < 3; ++d2) {
+                    const float mv = sm_m[da][d1][d2];
+                    if (mv == 0.f) continue;
+                    const int e = base + da + d1 * R1 + d2 * R1 * R2;
+                    atomicAdd(&amw[e], mv);
+                    atomicAdd(&apw[e], sm_p[da][d1][d2]);
+                    if (PH && sm_q[da][d1][d2] != 0.f) atomicAdd(&aqw[e], sm_q[da][d1][d2]);
+                }
+    }
+    // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
+    // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
+    // at a time, one pair per lane, instead of one divergent pass per neighbour direction.
     const uint32_t T = p1 - p0;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t Ls = (T + 31) / 32;
-    // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32 at
-    // a time, one pair per lane, instead of one divergent pass per neighbour direction
     uint32_t* qv = xq_v + w * P2G_XQ;
     uint8_t* qd = xq_d + w * P2G_XQ;
     int qn = 0;
-    for (uint32_t i = w; i < Ls; i += nw) {
+    for (uint32_t i = w; xmask && i < Ls; i += nw) {
         const uint32_t v = lane * Ls + i;
         const bool valid = v < T;
-        float X[3], V[3], q[3];
+        float q[3];
         if (valid) {
             const uint32_t sidx = p0 + v;
-            const float ph = PH ? phase[pid[sidx]] : 0.f;
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                X[k] = soa[(int64_t)k * n + sidx];
-                V[k] = soa[(int64_t)(3 + k) * n + sidx];
-                q[k] = (X[k] - o[k]) * invh;
-            }
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-                const int ia = min(max((int)floorf(q[a]), 0), r - 1);
-                const int j1 = min(max((int)floorf(q[t1] - 0.5f), -1), r - 1);
-                const int j2 = min(max((int)floorf(q[t2] - 0.5f), -1), r - 1);
-                float dA2[2], dB2[2], dC2[2];
-#pragma unroll
-                for (int k = 0; k < 2; ++k) {
-                    const float dA = q[a] - (float)(ia + k);
-                    const float dB = q[t1] - ((float)(j1 + k) + 0.5f);
-                    const float dC = q[t2] - ((float)(j2 + k) + 0.5f);
-                    dA2[k] = dA * dA;
-                    dB2[k] = dB * dB;
-                    dC2[k] = dC * dC;
-                }
-                const int base = a * TA + ia + R1 * ((j1 + 1) + R2 * (j2 + 1));
-                const float va = V[a];
-#pragma unroll
-                for (int da = 0; da < 2; ++da)
-#pragma unroll
-                    for (int d1 = 0; d1 < 2; ++d1) {
-                        const float dAB = dA2[da] + dB2[d1];
-#pragma unroll
-                        for (int d2 = 0; d2 < 2; ++d2) {
-                            const float tt = 1.f - (dAB + dC2[d2]);
-                            const float wgt = tt * tt * tt;
-                            const int e = base + da + d1 * R1 + d2 * R1 * R2;
-                            if (tt > 0.f) {
-                                atomicAdd(&amw[e], wgt);
-                                atomicAdd(&apw[e], wgt * va);
-                                if (PH && ph != 0.f) atomicAdd(&aqw[e], wgt * ph);  // phase-0 particles add nothing
-                            }
-                        }
-                    }
-            }
+            for (int k = 0; k < 3; ++k) q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
         }
         if (xmask) {
             // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
