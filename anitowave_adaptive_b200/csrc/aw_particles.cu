@@ -320,7 +320,7 @@ __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[
 }
 
 template <bool PH>
-__global__ void __launch_bounds__(P2G_THREADS) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
+__global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
                                                  const uint32_t* __restrict__ pid, const float* __restrict__ phase,
                                                  int smem_floats) {
