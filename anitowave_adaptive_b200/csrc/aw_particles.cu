@@ -440,10 +440,10 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
             for (int da = 0; da < 2; ++da)
 #pragma unroll
                 for (int d1 = 0; d1 < 3; ++d1) {
-                    const float dAB = dA2[da] + dB2[d1];
+                    const float omAB = 1.f - (dA2[da] + dB2[d1]);  // hoisted: one add per face
 #pragma unroll
                     for (int d2 = 0; d2 < 3; ++d2) {
-                        const float tt = fmaxf(1.f - (dAB + dC2[d2]), 0.f);
+                        const float tt = fmaxf(omAB - dC2[d2], 0.f);
                         const float wgt = tt * tt * tt;
                         sm_m[da][d1][d2] += wgt;
                         sm_p[da][d1][d2] += wgt * va;
