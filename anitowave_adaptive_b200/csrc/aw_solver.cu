@@ -513,6 +513,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
             // smaller blocks keep one thread per cell so that a slot's threads stay contiguous
             constexpr bool HALF = GM == 1 && R >= 2;
             constexpr int NC = HALF ? n3 / 2 : GM * n3;
+            constexpr int RH = R >= 2 ? R / 2 : 1;  // cells of one colour per row (HALF only)
             const int cc = P.reverse ? 1 - col : col;
 #pragma unroll
             for (int t0 = 0; t0 < NC; t0 += NT) {
@@ -521,9 +522,9 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
                 if (HALF) {
                     if (t >= NC) continue;
                     sl = 0;
-                    cy = (t / (R / 2)) % R;
-                    cz = t / (R / 2 * R);
-                    cx = 2 * (t % (R / 2)) + ((cy + cz + cc) & 1);
+                    cy = (t / RH) % R;
+                    cz = t / (RH * R);
+                    cx = 2 * (t % RH) + ((cy + cz + cc) & 1);
                     i = cx + R * (cy + R * cz);
                 } else {
                     sl = t / n3;

@@ -40,7 +40,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc failed")
     with open(os.path.join(PKG, "ptxas_info.txt"), "w") as f:
-        f.write(res.stderr)
+        f.write(res.stderr.replace(ROOT + os.sep, ""))  # paths relative to the repository
     if verbose:
         sys.stderr.write(res.stderr)
     return OUT
