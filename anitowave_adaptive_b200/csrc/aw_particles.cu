@@ -299,7 +299,7 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
 constexpr int P2G_THREADS = 512;  // the most threads a P2G CTA is launched with
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
 constexpr int P2G_SLICE = 16;  // particles of one cell per register-accumulation task
-constexpr int P2G_MAX_SLICES = 1 << 20;  // 3 * 8^3 * this stays below 2^31
+constexpr int P2G_MAX_SLICES = 1 << 19;  // 6 * 8^3 * this stays below 2^31
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
@@ -320,7 +320,7 @@ __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[
 }
 
 template <bool PH>
-__global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
+__global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
                                                  const uint32_t* __restrict__ pid, const float* __restrict__ phase,
                                                  int smem_floats) {
@@ -374,11 +374,13 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
-    // Own particles, cell by cell.  A task is (component a, cell c, slice s): up to `slice` of c's
-    // particles (contiguous in the cell-sorted array).  Its thread sums their weights on the 2x3x3
-    // faces of component a around c in registers, then adds the 18 sums into the tile: one atomic
-    // per face and task instead of one per face and particle.  Slices hold P2G_SLICE particles
-    // unless a crowded cell would push the task count past 3 * 512 * P2G_MAX_SLICES.
+    // Own particles, cell by cell.  A task is (kind, cell c, slice s): up to `slice` of c's particles
+    // (contiguous in the cell-sorted array).  Its thread sums their weights w and w times a value on
+    // the 2x3x3 faces of one component a around c in registers, then adds the sums into the tile:
+    // one atomic per face and task instead of one per face and particle.  Kinds 0-2 sum mass and
+    // momentum of component a = kind; with phases, kinds 3-5 sum w * phase of component kind - 3
+    // over the particles whose phase is not 0 (the others add nothing).  Slices hold P2G_SLICE
+    // particles unless a crowded cell would push the task count past 6 * 512 * P2G_MAX_SLICES.
     const int nc3 = r * r * r;
     for (int c = threadIdx.x; c < nc3; c += blockDim.x) {
         const uint32_t cnt = cs[c0 + c + 1] - cs[c0 + c];
@@ -388,10 +390,13 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
     const uint32_t mc = maxcnt;
     const int nsl = (int)min((mc + P2G_SLICE - 1) / P2G_SLICE, (uint32_t)P2G_MAX_SLICES);
     const uint32_t slice = nsl ? (mc + nsl - 1) / nsl : 0;
-    const int ntask = 3 * nc3 * nsl;
+    constexpr int NK = PH ? 6 : 3;
+    const int ntask = NK * nc3 * nsl;
     for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-        const int a = task / (nc3 * nsl);
-        const int rem = task - a * nc3 * nsl;
+        const int kind = task / (nc3 * nsl);
+        const int rem = task - kind * nc3 * nsl;
+        const bool qpass = PH && kind >= 3;
+        const int a = qpass ? kind - 3 : kind;
         const int c = rem % nc3, sl = rem / nc3;  // neighbouring threads take neighbouring cells
         const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
         if ((uint32_t)sl * slice >= ce - ca) continue;
@@ -406,23 +411,27 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
         const float oa = a == 0 ? o[0] : (a == 1 ? o[1] : o[2]);
         const float o1 = t1 == 0 ? o[0] : (t1 == 1 ? o[1] : o[2]);
         const float o2 = t2 == 0 ? o[0] : (t2 == 1 ? o[1] : o[2]);
-        float sm_m[2][3][3], sm_p[2][3][3], sm_q[2][3][3];
+        float sw[2][3][3], sv[2][3][3];  // sums of w and of w * (velocity component or phase)
 #pragma unroll
         for (int da = 0; da < 2; ++da)
 #pragma unroll
             for (int d1 = 0; d1 < 3; ++d1)
 #pragma unroll
                 for (int d2 = 0; d2 < 3; ++d2) {
-                    sm_m[da][d1][d2] = 0.f;
-                    sm_p[da][d1][d2] = 0.f;
-                    sm_q[da][d1][d2] = 0.f;
+                    sw[da][d1][d2] = 0.f;
+                    sv[da][d1][d2] = 0.f;
                 }
         for (uint32_t i = i0; i < i1; ++i) {
+            float val;
+            if (qpass) {
+                val = phase[pid[i]];
+                if (val == 0.f) continue;
+            } else {
+                val = soa[(int64_t)(3 + a) * n + i];
+            }
             const float qa = (soa[(int64_t)a * n + i] - oa) * invh;
             const float q1 = (soa[(int64_t)t1 * n + i] - o1) * invh;
             const float q2 = (soa[(int64_t)t2 * n + i] - o2) * invh;
-            const float va = soa[(int64_t)(3 + a) * n + i];
-            const float ph = PH ? phase[pid[i]] : 0.f;
             float dA2[2], dB2[3], dC2[3];
 #pragma unroll
             for (int k = 0; k < 2; ++k) {
@@ -445,9 +454,8 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
                     for (int d2 = 0; d2 < 3; ++d2) {
                         const float tt = fmaxf(omAB - dC2[d2], 0.f);
                         const float wgt = tt * tt * tt;
-                        sm_m[da][d1][d2] += wgt;
-                        sm_p[da][d1][d2] += wgt * va;
-                        if (PH) sm_q[da][d1][d2] += wgt * ph;
+                        sw[da][d1][d2] += wgt;
+                        sv[da][d1][d2] += wgt * val;
                     }
                 }
         }
@@ -459,12 +467,15 @@ __global__ void __launch_bounds__(P2G_THREADS, PH ? 1 : 2) k_p2g_own(LevelView L
             for (int d1 = 0; d1 < 3; ++d1)
 #pragma unroll
                 for (int d2 = 0; d2 < 3; ++d2) {
-                    const float mv = sm_m[da][d1][d2];
+                    const float mv = sw[da][d1][d2];
                     if (mv == 0.f) continue;
                     const int e = base + da + d1 * R1 + d2 * R1 * R2;
-                    atomicAdd(&amw[e], mv);
-                    atomicAdd(&apw[e], sm_p[da][d1][d2]);
-                    if (PH && sm_q[da][d1][d2] != 0.f) atomicAdd(&aqw[e], sm_q[da][d1][d2]);
+                    if (qpass) {
+                        atomicAdd(&aqw[e], sv[da][d1][d2]);
+                    } else {
+                        atomicAdd(&amw[e], mv);
+                        atomicAdd(&apw[e], sv[da][d1][d2]);
+                    }
                 }
     }
     // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
