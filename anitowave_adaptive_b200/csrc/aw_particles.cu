@@ -655,10 +655,10 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
         }
     const int NVt = ph ? 9 : 6;
     // the largest tile, or one private tile per warp for blocks of at most two cells per edge
-    // 512 threads walk a block's particles in half the rounds of 256 (0.64 -> 0.61 ms on the
-    // 3-level dam_drop_128).  A grid with one-cell blocks keeps 256: thousands of particles of such
-    // a block share a tile of 18 faces per axis, and twice the threads on it contend more (the
-    // 4-level dam_drop2_256 P2G takes 6.0 ms with 512 against 5.2 ms with 256).
+    // 512-thread CTAs: the aw_p2g call takes 0.43 ms on the 3-level dam_drop_128 against 0.48 ms
+    // with 256.  A grid with one-cell blocks keeps 256: the tasks of such a block all add into one
+    // tile of 18 faces per axis, and more threads on it contend more (the 4-level dam_drop2_256
+    // takes 2.96 ms with 512 against 2.85 ms with 256).
     const int nthreads = minres >= 2 ? P2G_THREADS : 256;
     const size_t smem_f = std::max((size_t)NVt * tile_axis(maxres),
                                    minres <= 2 ? (size_t)(nthreads / 32) * NVt * tile_axis(std::min(maxres, 2)) : 0);
