@@ -90,6 +90,32 @@ def test_crowded_coarse_cell(grid, block):
     check_p2g(g, O, pos, vel)
 
 
+@pytest.mark.parametrize("level", [0, 2])
+def test_cell_beyond_the_slice_cap(level):
+    """9,000,000 particles in one cell: more than 2^19 slices of 16 particles, so P2G lengthens its
+    slices (to 18 particles) to keep the task count below 2^31.  The grid is uniform (8^3-cell blocks,
+    or 2^3-cell blocks with per-warp tiles), so every face is summed by the own-particle pass from
+    per-slice partial sums: each face adds some 10^5 FP32 partial sums, hence 1e-4 relative L2.
+    (With another resolution within reach, each of the millions of particles would add its own weight
+    to the neighbour's faces with a global FP32 atomic, and those sums stagnate once their spacing
+    reaches the size of one weight.)"""
+    g, O, _ = make([level] * 8, (2, 2, 2))
+    rng = np.random.default_rng(12)
+    n = 9_000_000
+    h = 1.0 / (8 >> level)
+    pos = (np.array([1.0, 1.0, 1.0]) + h * (0.1 + 0.8 * rng.random((n, 3)))).astype(np.float32)
+    vel = rng.standard_normal((n, 3)).astype(np.float32)
+    u, m, cnt = O.p2g(pos, vel)
+    g.p2g(dev(pos), dev(vel))
+    torch.cuda.synchronize()
+    for a in range(3):
+        assert rel_l2(g.channel(aw.MASS_DENSITY_X + a).cpu().numpy(), m[a]) < 1e-4
+        assert rel_l2(g.channel(aw.VELOCITY_X + a).cpu().numpy(), u[a]) < 1e-4
+    assert np.array_equal(g.channel(aw.CELL_TYPE).cpu().numpy().astype(np.int64), cnt.astype(np.int64))
+    assert int(cnt.max()) == n
+    g.close()
+
+
 def test_boundary_positions(grid):
     """Particles exactly on cell faces, block faces and the domain's faces (including its far faces,
     which clamp into the last cell), sorted bit-exactly and transferred like the oracle's."""
