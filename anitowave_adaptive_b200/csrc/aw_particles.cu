@@ -496,47 +496,45 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
 #pragma unroll
             for (int k = 0; k < 3; ++k) q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
         }
-        if (xmask) {
-            // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
-            uint32_t near = 0;
-            if (valid) {
-                for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
-                    const int d = __ffs(mm) - 1;
-                    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                    const float reach = nres[d] < r ? 2.f : 1.f;
-                    bool nr = true;
+        // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
+        uint32_t near = 0;
+        if (valid) {
+            for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
+                const int d = __ffs(mm) - 1;
+                const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+                const float reach = nres[d] < r ? 2.f : 1.f;
+                bool nr = true;
 #pragma unroll
-                    for (int k = 0; k < 3; ++k)
-                        nr = nr && (dd[k] == 0 || (dd[k] < 0 ? q[k] < reach : q[k] > (float)r - reach));
-                    if (nr) near |= 1u << d;
-                }
+                for (int k = 0; k < 3; ++k)
+                    nr = nr && (dd[k] == 0 || (dd[k] < 0 ? q[k] < reach : q[k] > (float)r - reach));
+                if (nr) near |= 1u << d;
             }
-            // at most two pairs per lane per round keeps the queue within 31 + 64 entries
-            while (__any_sync(0xffffffffu, near)) {
-                const uint32_t b1 = near & (0u - near);
-                const uint32_t r1 = near & ~b1;
-                const uint32_t take = b1 | (r1 & (0u - r1));
-                near &= ~take;
-                const int cnt = __popc(take);
-                int incl = cnt;
+        }
+        // at most two pairs per lane per round keeps the queue within 31 + 64 entries
+        while (__any_sync(0xffffffffu, near)) {
+            const uint32_t b1 = near & (0u - near);
+            const uint32_t r1 = near & ~b1;
+            const uint32_t take = b1 | (r1 & (0u - r1));
+            near &= ~take;
+            const int cnt = __popc(take);
+            int incl = cnt;
 #pragma unroll
-                for (int sh = 1; sh < 32; sh <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
-                    if (lane >= sh) incl += y;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                int slot = qn + incl - cnt;
-                for (uint32_t mm = take; mm; mm &= mm - 1, ++slot) {
-                    qv[slot] = v;
-                    qd[slot] = (uint8_t)(__ffs(mm) - 1);
-                }
-                qn += total;
+            for (int sh = 1; sh < 32; sh <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                if (lane >= sh) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            int slot = qn + incl - cnt;
+            for (uint32_t mm = take; mm; mm &= mm - 1, ++slot) {
+                qv[slot] = v;
+                qd[slot] = (uint8_t)(__ffs(mm) - 1);
+            }
+            qn += total;
+            __syncwarp();
+            while (qn >= 32) {
+                qn -= 32;
+                p2g_cross_pair<PH>(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc, pid, phase);
                 __syncwarp();
-                while (qn >= 32) {
-                    qn -= 32;
-                    p2g_cross_pair<PH>(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc, pid, phase);
-                    __syncwarp();
-                }
             }
         }
     }
