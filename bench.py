@@ -97,14 +97,14 @@ class Clocks:
                 "power_w_max": max(pw) if pw else None}
 
 
-def dist_init():
+def dist_init(backend="nccl"):
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if ws > 1:
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        dist.init_process_group(backend, timeout=timedelta(seconds=120))
     return ws, rank, local
 
 
@@ -515,7 +515,8 @@ def main():
     ap.add_argument("--poisson-solve-once", action="store_true",
                     help="one mixed-precision poisson_256 solve to 1e-6 after one warm-up solve (small ncu captures)")
     args = ap.parse_args()
-    ws, rank, local = dist_init()
+    # the reference arm runs on the host cores only and takes no collective: a gloo group suffices
+    ws, rank, local = dist_init("gloo" if args.impl == "reference" else "nccl")
     try:
         if args.poisson_only:
             import torch
