@@ -3,6 +3,7 @@ prints one JSON line with the metric, the `cpu_baseline` and `e2e` objects and t
 the other rank exits 0 and prints nothing."""
 import json
 import os
+import socket
 import subprocess
 import sys
 
@@ -40,8 +41,11 @@ def test_reference_arm_prints_one_line():
 @pytest.mark.slow
 def test_reference_arm_under_torchrun_prints_once():
     """Two ranks as the multi-GPU launch starts them: rank 0 alone runs and prints."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2", "--master-addr",
-           "127.0.0.1", "--master-port", "29513", os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus",
+           "127.0.0.1", "--master-port", str(port), os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus",
            "2", "--steps", "1", "--warmup", "1"]
     res = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert res.returncode == 0, res.stderr[-2000:]
