@@ -38,7 +38,7 @@ DIVERGENCE, CELL_TYPE = 16, 19
 VELOCITY_OLD_X, VELOCITY_OLD_Y, VELOCITY_OLD_Z = 20, 21, 22
 
 OPERATOR_FV, OPERATOR_REFERENCE = 0, 1
-PRECISION_FP32, PRECISION_MIXED = 0, 1
+PRECISION_FP32, PRECISION_MIXED, PRECISION_FP32_PCG = 0, 1, 2
 
 
 class AWError(RuntimeError):
@@ -99,6 +99,7 @@ SIGNATURES = {
     "aw_backup_grid_velocity": (C.c_int, [_VP, _VP]),
     "aw_g2p": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
     "aw_g2p_noalloc": (C.c_int, [_VP, _VP, _VP, _I64, _F, _VP]),
+    "aw_test_arm_copy_timeout": (C.c_int, [_VP]),
     "aw_advect": (C.c_int, [_VP, _VP, _I64, _F, _VP]),
     "aw_sample_velocity": (C.c_int, [_VP, _VP, _I64, _I32, _VP, _VP]),
     "aw_resample_lattice": (C.c_int, [_VP, C.POINTER(_I32), C.POINTER(_F), C.POINTER(_F)]),
@@ -114,6 +115,7 @@ SIGNATURES = {
     "aw_wall_bc": (C.c_int, [_VP, _I32, _VP]),
     "aw_add_gravity": (C.c_int, [_VP, C.POINTER(_F), _F, _VP]),
     "aw_velocity_divergence": (C.c_int, [_VP, _VP, _F, _VP, _VP, _VP]),
+    "aw_velocity_divergence_max64": (C.c_int, [_VP, _VP, _VP, _VP]),
     "aw_pressure_gradient": (C.c_int, [_VP, _VP, _VP, _I32, _VP, _F, _VP]),
     "aw_solver_default_desc": (C.c_int, [_I32, C.POINTER(SolverDesc)]),
     "aw_solver_create": (C.c_int, [_VP, C.POINTER(SolverDesc), _PP]),
@@ -396,6 +398,13 @@ class MSBG:
         check(lib().aw_velocity_divergence(self.h, _ptr(fluid), 1.0 / float(dt), out.data_ptr(), mx.data_ptr(),
                                            _stream(stream)))
         return out, mx
+
+    def divergence_max64(self, fluid=None, stream=None):
+        """max |div u| per unit volume of VELOCITY_* over fluid cells, face sums in FP64"""
+        import torch
+        out = torch.zeros(1, dtype=torch.float64, device="cuda")
+        check(lib().aw_velocity_divergence_max64(self.h, _ptr(fluid), out.data_ptr(), _stream(stream)))
+        return float(out.item())
 
     def pressure_gradient(self, solver, p, fluid, dt, stream=None):
         import torch

@@ -172,7 +172,7 @@ extern "C" aw_status aw_rollout_create(aw_msbg* g, const aw_flip_desc* desc, con
     R->every = checkpoint_every;
     const size_t np = (size_t)std::max<int64_t>(n, 1);
     for (int k = 0; k < 2; ++k) {
-        AW_TRY(R->state[k].alloc(6 * np));
+        AW_TRY(R->state[k].alloc(6 * np + kSoaPad));
         AW_TRY(R->ids[k].alloc(np));
         AW_TRY(R->bar[k].alloc(6 * np));
     }

@@ -184,6 +184,32 @@ __global__ void k_divergence(LevelView L, const float* __restrict__ u0, const fl
     if ((threadIdx.x & 31) == 0 && divmax) atomic_max_pos(divmax, lmax);
 }
 
+// max over fluid cells of |div u| per unit volume, the face sums taken in FP64 (for reporting the
+// divergence an FP32 velocity field really has, free of the FP32 rounding of the sum itself)
+__global__ void k_divergence_max64(LevelView L, const float* __restrict__ u0, const float* __restrict__ u1,
+                                   const float* __restrict__ u2, const uint8_t* __restrict__ fluid,
+                                   unsigned long long* divmax) {
+    const int b = blockIdx.x;
+    const int r = L.res[b];
+    if (!r) return;
+    const double invH = (double)r / (double)L.g.bs;
+    const uint32_t oc = L.off[0][b], ox = L.off[1][b], oy = L.off[2][b], oz = L.off[3][b];
+    double lmax = 0.0;
+    for (int i = threadIdx.x; i < r * r * r; i += blockDim.x) {
+        const int x = i % r, y = (i / r) % r, z = i / (r * r);
+        if (!fluid || fluid[oc + i]) {
+            const double d = ((double)u0[ox + fidx(0, x + 1, y, z, r)] - (double)u0[ox + fidx(0, x, y, z, r)]) +
+                             ((double)u1[oy + fidx(1, x, y + 1, z, r)] - (double)u1[oy + fidx(1, x, y, z, r)]) +
+                             ((double)u2[oz + fidx(2, x, y, z + 1, r)] - (double)u2[oz + fidx(2, x, y, z, r)]);
+            lmax = fmax(lmax, fabs(d) * invH);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    // non-negative doubles order like their bit patterns
+    if ((threadIdx.x & 31) == 0) atomicMax(divmax, (unsigned long long)__double_as_longlong(lmax));
+}
+
 // pressure of the cell across face (a, s) of cell c, plus whether that cell is fluid; kind 0 =
 // outside the domain (wall)
 template <class PT>
@@ -570,7 +596,7 @@ aw_status FlipBufs::ensure(const MsbgState& G) {
 aw_status StepRecord::ensure(const MsbgState& G, int64_t n) {
     const size_t np = (size_t)std::max<int64_t>(n, 1);
     AW_TRY(perm.ensure(np));
-    AW_TRY(soa.ensure(6 * np));
+    AW_TRY(soa.ensure(6 * np + kSoaPad));
     for (int a = 0; a < 3; ++a) {
         const size_t nf = std::max<uint32_t>(G.tot[1 + a], 1);
         AW_TRY(u1[a].ensure(nf));
@@ -770,7 +796,7 @@ extern "C" aw_status aw_flip_create(aw_msbg* g, const aw_flip_desc* d, const flo
     F->n = n;
     MsbgState& G = g->st;
     for (int k = 0; k < 2; ++k) {
-        AW_TRY(F->soa[k].alloc((size_t)std::max<int64_t>(n, 1) * 6));
+        AW_TRY(F->soa[k].alloc((size_t)std::max<int64_t>(n, 1) * 6 + kSoaPad));
         AW_TRY(F->ids[k].alloc((size_t)std::max<int64_t>(n, 1)));
     }
     // host AoS -> device SoA
@@ -952,6 +978,16 @@ extern "C" aw_status aw_velocity_divergence(aw_msbg* g, const uint8_t* d_fluid, 
     MsbgState& G = g->st;
     k_divergence<<<G.nb, 128, 0, (cudaStream_t)s>>>(G.view0(), G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y],
                                                     G.ch[AW_VELOCITY_Z], d_fluid, inv_dt, d_out, d_max);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+extern "C" aw_status aw_velocity_divergence_max64(aw_msbg* g, const uint8_t* d_fluid, double* d_max, aw_stream s) {
+    AW_CHECK_ARG(g && d_max && g->st.allocated, "bad argument");
+    MsbgState& G = g->st;
+    AW_CUDA(cudaMemsetAsync(d_max, 0, sizeof(double), (cudaStream_t)s));
+    k_divergence_max64<<<G.nb, 128, 0, (cudaStream_t)s>>>(G.view0(), G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y],
+                                                          G.ch[AW_VELOCITY_Z], d_fluid, (unsigned long long*)d_max);
     AW_LAUNCH();
     return AW_OK;
 }

@@ -539,6 +539,7 @@ extern "C" aw_status aw_msbg_allocate(aw_msbg* g, aw_stream s_) {
     AW_CUDA(cudaStreamSynchronize(s));
     G.h_tile_off.clear();  // tiles follow the new resolutions
     G.allocated = true;
+    G.pw.src_valid = false;  // a sorted particle order refers to the previous layout
     return AW_OK;
 }
 

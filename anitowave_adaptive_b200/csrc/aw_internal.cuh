@@ -171,11 +171,23 @@ __device__ inline double warp_sum(double v) {
 // ------------------------------------------------------------------------------------------------
 // Host-side objects
 // ------------------------------------------------------------------------------------------------
+// Floats allocated past the six arrays of every SoA particle buffer: G2P's bulk copies round each
+// array segment up to 16 bytes and may read up to 3 floats past the last array's end.
+constexpr size_t kSoaPad = 16;
+
 struct ParticleWork {
     DBuf<uint32_t> keys, keys2, keys3, perm, perm2, cell_start, cell_fill, tmp, hist, hscan;
     uint32_t* sorted = nullptr;  // sorted slot -> input index (perm or perm2)
     DBuf<float> soa, soa2;  // 6 SoA arrays: px py pz vx vy vz
     int64_t n = 0;
+    // The particle arrays the last aw_p2g sorted (caller pointers and count) and 64-bit hashes of
+    // their contents then: hash[0] positions, hash[1] velocities; hash[2..3] receive the hashes of
+    // the arrays at a later drop-in G2P or advection, which reuses this sort when they match.
+    const float* src_pos = nullptr;
+    const float* src_vel = nullptr;
+    int64_t src_n = -1;
+    bool src_valid = false;
+    DBuf<unsigned long long> hash;
     aw_status ensure(int64_t np, uint32_t ncell);
 };
 
@@ -218,6 +230,7 @@ struct MsbgState {
     DBuf<int> lattice_tab;                      // per-axis lookup tables of aw_resample_cells
     FlipBufs proj;                              // aw_project / aw_vjp_project work buffers
     DBuf<int> err;  // device error flags: [1] bulk-copy wait timeout in G2P / advection ([0] unused)
+    bool test_copy_timeout = false;  // next G2P arms its first copy barrier without issuing the copy
     DBuf<uint8_t> occ;
     DBuf<int> flag;
     ParticleWork pw;
@@ -239,7 +252,9 @@ aw_status levels_from_positions(MsbgState& G, const float* d_pos, int64_t si, in
 aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<uint32_t>& tmp, cudaStream_t s);
 
 // Particle pipeline (aw_particles.cu)
-aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s);
+// record: remember the arrays and their hashes for the drop-in G2P / advection (aw_p2g)
+aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s,
+                             bool record = false);
 // Two-phase input of P2G: sorted particle i has phase phase[pid[i]] in [0,1]; the face phase goes to
 // phi[3] and 1 / ((1 - phi) rho0 + phi rho1) to beta[3].
 struct PhaseIn {

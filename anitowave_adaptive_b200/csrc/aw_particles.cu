@@ -148,23 +148,80 @@ static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* val
     return AW_OK;
 }
 
-// gather pos/vel into SoA sorted order, carry the original ids
+// 64-bit content hash of a particle array: the sum over particles of a mixed hash of (index, x, y, z),
+// so that it does not depend on the order the particles are visited in.  mix64 is the splitmix64
+// finaliser (S. Vigna).
+__device__ inline unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ inline unsigned long long hash3(uint32_t i, float x, float y, float z) {
+    const unsigned long long a = ((unsigned long long)__float_as_uint(x) << 32) | __float_as_uint(y);
+    const unsigned long long b = ((unsigned long long)__float_as_uint(z) << 32) | i;
+    return mix64(mix64(a) ^ b);
+}
+__device__ inline unsigned long long warp_sum_u64(unsigned long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// gather pos/vel into SoA sorted order, carry the original ids; with hash, add the content hashes
+// of the input positions (hash[0]) and velocities (hash[1])
 __global__ void k_gather(const uint32_t* __restrict__ src, int64_t n, PArr pos, PArr vel, float* __restrict__ soa,
                          const uint32_t* __restrict__ ids_in, uint32_t* __restrict__ ids_out,
-                         const uint32_t* __restrict__ keys, uint32_t* __restrict__ keys_sorted) {
-    int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    uint32_t i = src[j];
-    soa[j] = pos(i, 0);
-    soa[n + j] = pos(i, 1);
-    soa[2 * n + j] = pos(i, 2);
-    if (vel.p) {
-        soa[3 * n + j] = vel(i, 0);
-        soa[4 * n + j] = vel(i, 1);
-        soa[5 * n + j] = vel(i, 2);
+                         const uint32_t* __restrict__ keys, uint32_t* __restrict__ keys_sorted,
+                         unsigned long long* hash = nullptr) {
+    const int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long hp = 0, hv = 0;
+    if (j < n) {
+        const uint32_t i = src[j];
+        const float x = pos(i, 0), y = pos(i, 1), z = pos(i, 2);
+        soa[j] = x;
+        soa[n + j] = y;
+        soa[2 * n + j] = z;
+        if (hash) hp = hash3(i, x, y, z);
+        if (vel.p) {
+            const float u = vel(i, 0), v = vel(i, 1), w = vel(i, 2);
+            soa[3 * n + j] = u;
+            soa[4 * n + j] = v;
+            soa[5 * n + j] = w;
+            if (hash) hv = hash3(i, u, v, w);
+        }
+        if (ids_out) ids_out[j] = ids_in ? ids_in[i] : i;
+        if (keys_sorted) keys_sorted[j] = keys[i];
     }
-    if (ids_out) ids_out[j] = ids_in ? ids_in[i] : i;
-    if (keys_sorted) keys_sorted[j] = keys[i];
+    if (hash) {  // uniform across the CTA
+        hp = warp_sum_u64(hp);
+        hv = warp_sum_u64(hv);
+        if ((threadIdx.x & 31) == 0) {
+            atomicAdd(hash, hp);
+            atomicAdd(hash + 1, hv);
+        }
+    }
+}
+
+// content hashes of AoS positions (out[0]) and, when given, velocities (out[1]); out must start at 0
+__global__ void k_hash_aos(const float* __restrict__ pos, const float* __restrict__ vel, int64_t n,
+                           unsigned long long* out) {
+    unsigned long long hp = 0, hv = 0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        hp += hash3((uint32_t)i, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        if (vel) hv += hash3((uint32_t)i, vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+    }
+    hp = warp_sum_u64(hp);
+    hv = warp_sum_u64(hv);
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(out, hp);
+        if (vel) atomicAdd(out + 1, hv);
+    }
+}
+
+// the caller's arrays still hold what the last aw_p2g sorted (positions; velocities too if asked)
+__device__ inline bool sort_reusable(const unsigned long long* h, bool need_vel) {
+    return h[0] == h[2] && (!need_vel || h[1] == h[3]);
 }
 
 aw_status ParticleWork::ensure(int64_t np, uint32_t ncell) {
@@ -173,8 +230,8 @@ aw_status ParticleWork::ensure(int64_t np, uint32_t ncell) {
     AW_TRY(perm2.ensure((size_t)np));
     AW_TRY(cell_start.ensure((size_t)ncell + 2));
     AW_TRY(cell_fill.ensure((size_t)ncell + 2));
-    AW_TRY(soa.ensure((size_t)np * 6));
-    AW_TRY(soa2.ensure((size_t)np * 6));
+    AW_TRY(soa.ensure((size_t)np * 6 + kSoaPad));
+    AW_TRY(soa2.ensure((size_t)np * 6 + kSoaPad));
     n = np;
     return AW_OK;
 }
@@ -193,6 +250,7 @@ aw_status sort_core(MsbgState& G, PArr pos, int64_t n, cudaStream_t s) {
     }
     AW_TRY(exclusive_scan_u32(W.cell_fill.p, W.cell_start.p, (size_t)nc + 1, W.tmp, s));
     W.sorted = W.perm.p;
+    W.src_valid = false;  // the recorded order of aw_p2g is replaced
     if (n > 0) {
         // keys are consumed by the sort: keep a copy for aw_sort_particles' key output
         AW_TRY(W.keys2.ensure((size_t)n));
@@ -203,12 +261,26 @@ aw_status sort_core(MsbgState& G, PArr pos, int64_t n, cudaStream_t s) {
     return AW_OK;
 }
 
-aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s) {
+aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* vel_aos, int64_t n, cudaStream_t s,
+                             bool record) {
     PArr pos{pos_aos, 3, 1}, vel{vel_aos, 3, 1};
     AW_TRY(sort_core(G, pos, n, s));
+    ParticleWork& W = G.pw;
+    unsigned long long* hash = nullptr;
+    if (record) {
+        AW_TRY(W.hash.ensure(4));
+        AW_CUDA(cudaMemsetAsync(W.hash.p, 0, 2 * sizeof(unsigned long long), s));
+        hash = W.hash.p;
+    }
     if (n > 0) {
-        k_gather<<<nblk(n), 256, 0, s>>>(G.pw.sorted, n, pos, vel, G.pw.soa.p, nullptr, nullptr, nullptr, nullptr);
+        k_gather<<<nblk(n), 256, 0, s>>>(W.sorted, n, pos, vel, W.soa.p, nullptr, nullptr, nullptr, nullptr, hash);
         AW_LAUNCH();
+    }
+    if (record) {
+        W.src_pos = pos_aos;
+        W.src_vel = vel_aos;
+        W.src_n = n;
+        W.src_valid = true;
     }
     return AW_OK;
 }
@@ -257,15 +329,20 @@ struct FaceAcc {
     float* Phi[3];  // sum of w * phase (two-phase P2G only)
 };
 
-// weights of one particle on the faces of block nb (resolution rn != r), global atomics
+// weights of one particle on the faces of a neighbouring block of resolution rn != r, global atomics.
+// N holds that block's origin, 1 / cell size and face offsets (computed once per CTA).
+struct CrossNb {
+    float o[3];
+    float invh;
+    uint32_t off[3];
+};
+
 template <bool PH>
-__device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int nc[3], int rn, const float X[3], const float V[3],
-                                          float ph, const FaceAcc& acc) {
-    const Geo& g = L.g;
-    const float invh = 1.f / fcell(g, rn);
+__device__ __forceinline__ void p2g_cross(const CrossNb& N, int rn, const float X[3], const float V[3], float ph,
+                                          const FaceAcc& acc) {
     float q[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) q[k] = (X[k] - forigin(g, k, nc[k])) * invh;
+    for (int k = 0; k < 3; ++k) q[k] = (X[k] - N.o[k]) * N.invh;
     const float rf = (float)rn;
     if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f) return;
 #pragma unroll
@@ -273,7 +350,7 @@ __device__ __forceinline__ void p2g_cross(const LevelView& L, int nb, const int 
         const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
         const int ia = (int)floorf(q[a]);
         const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
-        const uint32_t ob = L.off[1 + a][nb];
+        const uint32_t ob = N.off[a];
         for (int da = 0; da < 2; ++da)
             for (int d1 = 0; d1 < 2; ++d1)
                 for (int d2 = 0; d2 < 2; ++d2) {
@@ -300,13 +377,13 @@ constexpr int P2G_THREADS = 512;  // the most threads a P2G CTA is launched with
 constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 waiting + 2 per lane
 constexpr int P2G_SLICE = 16;  // particles of one cell per register-accumulation task
 constexpr int P2G_MAX_SLICES = 1 << 19;  // 6 * 8^3 * this stays below 2^31
+constexpr int P2G_MAX_CELLS = 16 * 16 * 16;  // cells of the largest block (base resolution <= 16)
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
-__device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[3], const int* nres, uint32_t v, int d,
-                                               uint32_t p0, const float* __restrict__ soa, int64_t n,
-                                               const FaceAcc& acc, const uint32_t* __restrict__ pid,
-                                               const float* __restrict__ phase) {
+__device__ __forceinline__ void p2g_cross_pair(const CrossNb* xn, const int* nres, uint32_t v, int d, uint32_t p0,
+                                               const float* __restrict__ soa, int64_t n, const FaceAcc& acc,
+                                               const uint32_t* __restrict__ pid, const float* __restrict__ phase) {
     const uint32_t sidx = p0 + v;
     float X[3], V[3];
 #pragma unroll
@@ -314,9 +391,8 @@ __device__ __forceinline__ void p2g_cross_pair(const LevelView& L, const int cb[
         X[k] = soa[(int64_t)k * n + sidx];
         V[k] = soa[(int64_t)(3 + k) * n + sidx];
     }
-    const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
     const float ph = PH ? phase[pid[sidx]] : 0.f;
-    p2g_cross<PH>(L, bidx(L.g, nc[0], nc[1], nc[2]), nc, nres[d], X, V, ph, acc);
+    p2g_cross<PH>(xn[d], nres[d], X, V, ph, acc);
 }
 
 template <bool PH>
@@ -326,8 +402,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                                                  int smem_floats) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
+    __shared__ CrossNb xn[27];
     __shared__ int cross;
     __shared__ uint32_t maxcnt;
+    __shared__ int ccount[P2G_MAX_CELLS / 32];
+    __shared__ uint16_t clist[P2G_MAX_CELLS];
+    __shared__ int nonempty;
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
@@ -363,9 +443,18 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     if (threadIdx.x < 27) {
         const int d = threadIdx.x;
         const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
-        const int rn = inside(g, nc) ? L.res[bidx(g, nc[0], nc[1], nc[2])] : 0;
+        const int nb = inside(g, nc) ? bidx(g, nc[0], nc[1], nc[2]) : -1;
+        const int rn = nb >= 0 ? L.res[nb] : 0;
         nres[d] = rn;
-        if (rn && rn != r) atomicOr(&cross, 1 << d);
+        if (rn && rn != r) {
+            atomicOr(&cross, 1 << d);
+            xn[d].invh = 1.f / fcell(g, rn);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                xn[d].o[k] = forigin(g, k, nc[k]);
+                xn[d].off[k] = L.off[1 + k][nb];
+            }
+        }
     }
     __syncthreads();
     const int xmask = cross;
@@ -382,22 +471,54 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // over the particles whose phase is not 0 (the others add nothing).  Slices hold P2G_SLICE
     // particles unless a crowded cell would push the task count past 6 * 512 * P2G_MAX_SLICES.
     const int nc3 = r * r * r;
-    for (int c = threadIdx.x; c < nc3; c += blockDim.x) {
-        const uint32_t cnt = cs[c0 + c + 1] - cs[c0 + c];
+    // The block's non-empty cells, in cell order: tasks run over these only, so that lanes do not
+    // idle on the air cells of a surface block.
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int nchunk = (nc3 + 31) / 32;
+    for (int ch = wid; ch < nchunk; ch += nwarp) {
+        const int c = ch * 32 + lane;
+        const uint32_t cnt = c < nc3 ? cs[c0 + c + 1] - cs[c0 + c] : 0u;
         if (cnt > 0) atomicMax(&maxcnt, cnt);
+        const unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
+        if (lane == 0) ccount[ch] = __popc(m);
     }
     __syncthreads();
+    if (wid == 0) {  // exclusive scan of the per-chunk counts
+        int carry = 0;
+        for (int base = 0; base < nchunk; base += 32) {
+            const int ch = base + lane;
+            const int v = ch < nchunk ? ccount[ch] : 0;
+            int incl = v;
+#pragma unroll
+            for (int sh = 1; sh < 32; sh <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                if (lane >= sh) incl += y;
+            }
+            if (ch < nchunk) ccount[ch] = carry + incl - v;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) nonempty = carry;
+    }
+    __syncthreads();
+    for (int ch = wid; ch < nchunk; ch += nwarp) {
+        const int c = ch * 32 + lane;
+        const bool ne = c < nc3 && cs[c0 + c + 1] > cs[c0 + c];
+        const unsigned m = __ballot_sync(0xffffffffu, ne);
+        if (ne) clist[ccount[ch] + __popc(m & ((1u << lane) - 1u))] = (uint16_t)c;
+    }
+    __syncthreads();
+    const int ncell = nonempty;
     const uint32_t mc = maxcnt;
     const int nsl = (int)min((mc + P2G_SLICE - 1) / P2G_SLICE, (uint32_t)P2G_MAX_SLICES);
     const uint32_t slice = nsl ? (mc + nsl - 1) / nsl : 0;
     constexpr int NK = PH ? 6 : 3;
-    const int ntask = NK * nc3 * nsl;
+    const int ntask = NK * ncell * nsl;
     for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-        const int kind = task / (nc3 * nsl);
-        const int rem = task - kind * nc3 * nsl;
+        const int kind = task / (ncell * nsl);
+        const int rem = task - kind * ncell * nsl;
         const bool qpass = PH && kind >= 3;
         const int a = qpass ? kind - 3 : kind;
-        const int c = rem % nc3, sl = rem / nc3;  // neighbouring threads take neighbouring cells
+        const int c = clist[rem % ncell], sl = rem / ncell;  // neighbouring threads take neighbouring cells
         const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
         if ((uint32_t)sl * slice >= ce - ca) continue;
         const uint32_t i0 = ca + (uint32_t)sl * slice;
@@ -432,32 +553,55 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
             const float qa = (soa[(int64_t)a * n + i] - oa) * invh;
             const float q1 = (soa[(int64_t)t1 * n + i] - o1) * invh;
             const float q2 = (soa[(int64_t)t2 * n + i] - o2) * invh;
-            float dA2[2], dB2[3], dC2[3];
+            // Along a: faces ka and ka + 1.  Across: of the three face rows k - 1, k, k + 1 (centres at
+            // k - 0.5, k + 0.5, k + 1.5 in cell units) a particle reaches the centre row k and the side
+            // row on its own side of the cell centre; the third is more than one cell away, so its
+            // weight is zero and it is skipped.  c is the offset from the centre row, 1 - |c| the
+            // distance to the side row.
+            const float dA = qa - fa0;
+            const float A0 = dA * dA, A1 = (dA - 1.f) * (dA - 1.f);
+            const float c1 = q1 - (f10 + 1.f), c2 = q2 - (f20 + 1.f);
+            const float s1 = 1.f - fabsf(c1), s2 = 1.f - fabsf(c2);
+            const float Bc = c1 * c1, Bs = s1 * s1, Cc = c2 * c2, Cs = s2 * s2;
+            const bool lo1 = c1 < 0.f, lo2 = c2 < 0.f;
 #pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const float dA = qa - (fa0 + (float)k);
-                dA2[k] = dA * dA;
-            }
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float dB = q1 - (f10 + (float)k);
-                const float dC = q2 - (f20 + (float)k);
-                dB2[k] = dB * dB;
-                dC2[k] = dC * dC;
-            }
-#pragma unroll
-            for (int da = 0; da < 2; ++da)
-#pragma unroll
-                for (int d1 = 0; d1 < 3; ++d1) {
-                    const float omAB = 1.f - (dA2[da] + dB2[d1]);  // hoisted: one add per face
-#pragma unroll
-                    for (int d2 = 0; d2 < 3; ++d2) {
-                        const float tt = fmaxf(omAB - dC2[d2], 0.f);
-                        const float wgt = tt * tt * tt;
-                        sw[da][d1][d2] += wgt;
-                        sv[da][d1][d2] += wgt * val;
-                    }
+            for (int da = 0; da < 2; ++da) {
+                const float A = da ? A1 : A0;
+                const float omc = 1.f - (A + Bc), oms = 1.f - (A + Bs);
+                float t = fmaxf(omc - Cc, 0.f);
+                t = t * t * t;
+                sw[da][1][1] += t;
+                sv[da][1][1] += t * val;
+                t = fmaxf(oms - Cc, 0.f);
+                t = t * t * t;
+                if (lo1) {
+                    sw[da][0][1] += t;
+                    sv[da][0][1] += t * val;
+                } else {
+                    sw[da][2][1] += t;
+                    sv[da][2][1] += t * val;
                 }
+                t = fmaxf(omc - Cs, 0.f);
+                t = t * t * t;
+                if (lo2) {
+                    sw[da][1][0] += t;
+                    sv[da][1][0] += t * val;
+                } else {
+                    sw[da][1][2] += t;
+                    sv[da][1][2] += t * val;
+                }
+                t = fmaxf(oms - Cs, 0.f);
+                t = t * t * t;
+                const int j1 = lo1 ? 0 : 2, j2 = lo2 ? 0 : 2;
+#pragma unroll
+                for (int e1 = 0; e1 < 3; e1 += 2)
+#pragma unroll
+                    for (int e2 = 0; e2 < 3; e2 += 2)
+                        if (e1 == j1 && e2 == j2) {
+                            sw[da][e1][e2] += t;
+                            sv[da][e1][e2] += t * val;
+                        }
+            }
         }
         // faces fa in {ca, ca+1} along a, f1 in {c1-1, c1, c1+1} and f2 likewise across (tile rows -1..r)
         const int base = a * TA + ka + R1 * (k1 + R2 * k2);
@@ -482,7 +626,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
     // at a time, one pair per lane, instead of one divergent pass per neighbour direction.
     const uint32_t T = p1 - p0;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int w = wid, nw = nwarp;
     const uint32_t Ls = (T + 31) / 32;
     uint32_t* qv = xq_v + w * P2G_XQ;
     uint8_t* qd = xq_d + w * P2G_XQ;
@@ -533,12 +677,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
             __syncwarp();
             while (qn >= 32) {
                 qn -= 32;
-                p2g_cross_pair<PH>(L, cb, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc, pid, phase);
+                p2g_cross_pair<PH>(xn, nres, qv[qn + lane], qd[qn + lane], p0, soa, n, acc, pid, phase);
                 __syncwarp();
             }
         }
     }
-    if (qn > 0 && lane < qn) p2g_cross_pair<PH>(L, cb, nres, qv[lane], qd[lane], p0, soa, n, acc, pid, phase);
+    if (qn > 0 && lane < qn) p2g_cross_pair<PH>(xn, nres, qv[lane], qd[lane], p0, soa, n, acc, pid, phase);
     __syncthreads();
     if (priv) {
         for (int i = threadIdx.x; i < TW; i += blockDim.x) {
@@ -859,7 +1003,9 @@ __global__ void k_build_tiles(LevelView L, Field3 u, const uint32_t* __restrict_
 // Both ghosted tiles of G2P (u_new and u_old) in one pass: every entry's source face is located
 // once and read from the two fields.
 __global__ void k_build_tiles2(LevelView L, Field3 un, Field3 uo, const uint32_t* __restrict__ toff,
-                               float* __restrict__ tn, float* __restrict__ to) {
+                               float* __restrict__ tn, float* __restrict__ to,
+                               const unsigned long long* __restrict__ skip = nullptr) {
+    if (skip && sort_reusable(skip, true)) return;  // the drop-in G2P took the sorted path
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
@@ -879,36 +1025,6 @@ __global__ void k_build_tiles2(LevelView L, Field3 un, Field3 uo, const uint32_t
             const uint32_t src = face_source(L, a, b, cb, r, fi);
             tn[o + a * TA + rem] = un.c[a][src];
             to[o + a * TA + rem] = uo.c[a][src];
-        }
-    }
-}
-
-// u_new into tn and the FLIP increment field u_new - alpha u_old into tw, from the same sources.
-// The blend v' = alpha (v + u_new(x) - u_old(x)) + (1 - alpha) u_new(x) (G2P.cuh:11-128) equals
-// alpha v + I(u_new - alpha u_old)(x), since the trilinear interpolation I is linear: G2P then
-// stages and interpolates one tile instead of two.
-__global__ void k_build_tiles_blend(LevelView L, Field3 un, Field3 uo, float alpha, const uint32_t* __restrict__ toff,
-                                    float* __restrict__ tn, float* __restrict__ tw) {
-    const int b = blockIdx.x;
-    const int r = L.res[b];
-    if (!r) return;
-    int cb[3];
-    bcoord(L.g, b, cb);
-    const int R1 = r + 1, R2 = r + 2;
-    const int TA = (int)tile_axis(r);
-    const uint32_t o = toff[b];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
-            int fi[3];
-            fi[a] = rem % R1;
-            fi[t1] = (rem / R1) % R2 - 1;
-            fi[t2] = rem / (R1 * R2) - 1;
-            const uint32_t src = face_source(L, a, b, cb, r, fi);
-            const float vn = un.c[a][src];
-            tn[o + a * TA + rem] = vn;
-            tw[o + a * TA + rem] = vn - alpha * uo.c[a][src];
         }
     }
 }
@@ -978,91 +1094,199 @@ __device__ inline bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// true when phase `parity` completed; false (and the error flag set) after ~1 s of polling
-__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err) {
-    for (int it = 0; it < (1 << 20); ++it)
+// true when phase `parity` completed; false (and the error flag set) after `polls` polls (2^20 polls,
+// about a second, in production)
+__device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* err, int polls = 1 << 20) {
+    for (int it = 0; it < polls; ++it)
         if (mbar_try_wait(bar, parity)) return true;
     atomicExch(err, 1);
     return false;
 }
 
-// G2P on sorted particles.  One CTA per block: thread 0 issues one TMA bulk copy of the block's
-// ghosted tile of w = u_new - alpha u_old (16-byte aligned), every thread waits on the mbarrier,
-// then each particle of the block takes v' = alpha v + I(w)(x) from shared memory.
-__global__ void __launch_bounds__(256) k_g2p_tile(LevelView L, float* __restrict__ soa, int64_t n,
-                                                  const uint32_t* __restrict__ cs, float alpha,
-                                                  const uint32_t* __restrict__ toff, const float* __restrict__ tw_g,
-                                                  int* err) {
+// G2P on sorted particles, one CTA per block.
+// - The ghosted tile of w = u_new - alpha u_old is built in shared memory from the face arrays (the
+//   FLIP blend alpha (v + u_new - u_old) + (1 - alpha) u_new equals alpha v + I(w) because the
+//   trilinear interpolation I is linear), and the u_new tile is written to `tn` for the advection
+//   that follows.  Every active block writes its u_new tile, with particles or not.
+// - The block's particles (a contiguous range of each SoA array) are staged in chunks of G2P_CHUNK
+//   by TMA bulk copies (cp.async.bulk, no multicast), two chunks in flight, each behind an mbarrier
+//   with a bounded wait.  A copy starts at the 16-byte boundary at or below the chunk's first
+//   element and its size is rounded up to 16 bytes, so up to 3 floats past the end of the last array
+//   are read: SoA buffers are allocated kSoaPad floats longer.
+// - On a wait that runs out, the CTA waits (again bounded) for every copy it issued before it
+//   returns, so that no copy lands in shared memory that another CTA may then own.
+// arm_only (tests of the timeout path): chunk 0's barrier is armed but its copy is not issued, and
+// the waits poll `polls` times.
+// Drop-in mode (D.perm set): the particles are the sorted copy that aw_p2g made of the caller's AoS
+// arrays; the new velocities go to the caller's array through the sort permutation, no u_new tile is
+// written, and the kernel does nothing unless the caller's arrays still hash as they did then.
+struct DropIn {
+    const uint32_t* perm;            // sorted slot -> caller index (nullptr: FLIP-step SoA state)
+    float* aos;                      // caller's AoS array, written through perm
+    const unsigned long long* hash;  // {pos, vel} at sort time, {pos, vel} now
+};
+constexpr int G2P_THREADS = 256;
+constexpr int G2P_CHUNK = 512;
+constexpr int G2P_SLOT = G2P_CHUNK + 8;  // floats per staged array: chunk + alignment head and tail
+
+__device__ inline void g2p_stage_chunk(const float* soa, int64_t n, uint32_t q0, uint32_t q1, float* slot,
+                                       uint64_t* bar, bool issue) {
+    uint32_t bytes[6];
+    const float* src[6];
+    uint32_t total = 0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float* g = soa + (int64_t)k * n + q0;
+        const uint32_t head = (uint32_t)(((uintptr_t)g >> 2) & 3u);
+        src[k] = g - head;
+        bytes[k] = ((q1 - q0 + head) * 4u + 15u) & ~15u;
+        total += bytes[k];
+    }
+    mbar_expect_tx(bar, total);
+    if (issue)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) tma_bulk_load(slot + k * G2P_SLOT, src[k], bytes[k], bar);
+}
+
+__global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* __restrict__ soa, int64_t n,
+                                                           const uint32_t* __restrict__ cs, float alpha, Field3 un,
+                                                           Field3 uo, const uint32_t* __restrict__ toff,
+                                                           float* __restrict__ tn, int* err, int polls, int arm_only,
+                                                           DropIn D) {
     extern __shared__ __align__(16) float sm[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[2];
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
-    const uint32_t p0 = cs[L.off[0][b]], p1 = cs[L.off[0][b] + (uint32_t)(r * r * r)];
-    if (p0 == p1) return;
+    if (D.perm && !sort_reusable(D.hash, true)) return;
+    const uint32_t c0 = L.off[0][b];
+    const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
+    const uint32_t nchunk = (p1 - p0 + G2P_CHUNK - 1) / G2P_CHUNK;
     const uint32_t tb = tile_block(r);
-    if (threadIdx.x == 0) mbar_init(&bar, 1);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        mbar_expect_tx(&bar, tb * sizeof(float));
-        tma_bulk_load(sm, tw_g + toff[b], tb * sizeof(float), &bar);
+    float* tw = sm;
+    float* stage = sm + tb;  // tb is a multiple of 4 floats
+    if (nchunk) {
+        if (threadIdx.x == 0) {
+            mbar_init(&bar[0], 1);
+            mbar_init(&bar[1], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint32_t c = 0; c < 2 && c < nchunk; ++c) {
+                const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
+                g2p_stage_chunk(soa, n, q0, q1, stage + c * 6 * G2P_SLOT, &bar[c], !(arm_only && c == 0));
+            }
     }
-    const bool ok = mbar_wait_bounded(&bar, 0, err);
-    if (!__syncthreads_and(ok)) return;
-    const Geo& g = L.g;
+    // ghosted tiles (the copies above are in flight meanwhile)
     int cb[3];
-    bcoord(g, b, cb);
-    const float invh = 1.f / fcell(g, r);
+    bcoord(L.g, b, cb);
+    {
+        const int R1 = r + 1, R2 = r + 2;
+        const int TA = (int)tile_axis(r);
+        float* tno = tn ? tn + toff[b] : nullptr;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+            for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+                int fi[3];
+                fi[a] = rem % R1;
+                fi[t1] = (rem / R1) % R2 - 1;
+                fi[t2] = rem / (R1 * R2) - 1;
+                const uint32_t src = face_source(L, a, b, cb, r, fi);
+                const float vn = un.c[a][src];
+                if (tno) tno[a * TA + rem] = vn;
+                tw[a * TA + rem] = vn - alpha * uo.c[a][src];
+            }
+        }
+    }
+    __syncthreads();
+    if (!nchunk) return;
+    const float invh = 1.f / fcell(L.g, r);
     float o[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) o[a] = forigin(g, a, cb[a]);
-    // four particles per thread in flight: their loads are issued together
-    constexpr int U = 4;
-    const uint32_t st = blockDim.x;
-    for (uint32_t i0 = p0 + threadIdx.x; i0 < p1; i0 += U * st) {
-        float X[U][3], Vv[U][3];
-#pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const uint32_t i = i0 + k * st;
-            if (i < p1)
-#pragma unroll
-                for (int c = 0; c < 3; ++c) {
-                    X[k][c] = soa[(int64_t)c * n + i];
-                    Vv[k][c] = soa[(int64_t)(3 + c) * n + i];
-                }
+    for (int a = 0; a < 3; ++a) o[a] = forigin(L.g, a, cb[a]);
+    for (uint32_t c = 0; c < nchunk; ++c) {
+        const int sl = c & 1;
+        const bool ok = mbar_wait_bounded(&bar[sl], (c >> 1) & 1u, err, polls);
+        if (!__syncthreads_and(ok)) {
+            // drain: the copies of chunks c and c + 1 may still be in flight
+            if (threadIdx.x == 0)
+                for (uint32_t k = c; k < c + 2 && k < nchunk; ++k)
+                    if (!(arm_only && k == 0)) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1u, err, polls);
+            __syncthreads();
+            return;
         }
+        const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
+        const float* slot = stage + sl * 6 * G2P_SLOT;
+        uint32_t head[6];
 #pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const uint32_t i = i0 + k * st;
-            if (i < p1)
+        for (int k = 0; k < 6; ++k) head[k] = (uint32_t)(((uintptr_t)(soa + (int64_t)k * n + q0) >> 2) & 3u);
+        for (uint32_t j = threadIdx.x; j < q1 - q0; j += blockDim.x) {
+            const float X[3] = {slot[head[0] + j], slot[G2P_SLOT + head[1] + j], slot[2 * G2P_SLOT + head[2] + j]};
+            float vout[3];
 #pragma unroll
-                for (int a = 0; a < 3; ++a)
-                    soa[(int64_t)(3 + a) * n + i] = alpha * Vv[k][a] + tile_interp(sm, a, r, o, invh, X[k]);
+            for (int a = 0; a < 3; ++a)
+                vout[a] = alpha * slot[(3 + a) * G2P_SLOT + head[3 + a] + j] + tile_interp(tw, a, r, o, invh, X);
+            if (D.perm) {
+                float* dst = D.aos + 3 * (size_t)D.perm[q0 + j];
+#pragma unroll
+                for (int a = 0; a < 3; ++a) dst[a] = vout[a];
+            } else {
+#pragma unroll
+                for (int a = 0; a < 3; ++a) soa[(int64_t)(3 + a) * n + q0 + j] = vout[a];
+            }
+        }
+        __syncthreads();  // slot sl is free again
+        if (threadIdx.x == 0 && c + 2 < nchunk) {
+            const uint32_t n0 = p0 + (c + 2) * G2P_CHUNK, n1 = min(p1, n0 + G2P_CHUNK);
+            g2p_stage_chunk(soa, n, n0, n1, stage + sl * 6 * G2P_SLOT, &bar[sl], true);
         }
     }
 }
 
 // RK3 advection of the sorted particles of one block: the block's u_new tile is staged in shared
 // memory by one bulk copy; stage points that leave the block sample the neighbour's tile in global
-// memory (same arithmetic as sample_tiles).
-__device__ inline float sample_local(const LevelView& L, int b, const int cb[3], int r, const float o[3], float invh,
-                                     const float* __restrict__ tl, const uint32_t* __restrict__ toff,
-                                     const float* __restrict__ tg, int a, const float X[3]) {
+// memory (same arithmetic as sample_tiles).  The block holding a stage point is located once per
+// point, not once per component.
+struct PointTile {
+    const float* t;  // tile of the block holding the point (nullptr: inactive block, velocity 0)
+    int r;
+    float o[3];
+    float invh;
+};
+__device__ inline PointTile point_tile(const LevelView& L, const int cb[3], int r, const float o[3], float invh,
+                                       const float* __restrict__ tl, const uint32_t* __restrict__ toff,
+                                       const float* __restrict__ tg, const float X[3]) {
     int pc[3];
     point_block(L.g, X, pc);
-    if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) return tile_interp(tl, a, r, o, invh, X);
-    return sample_tiles(L, toff, tg, a, X);
+    PointTile T;
+    if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) {
+        T.t = tl;
+        T.r = r;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) T.o[k] = o[k];
+        T.invh = invh;
+        return T;
+    }
+    const int b2 = bidx(L.g, pc[0], pc[1], pc[2]);
+    T.r = L.res[b2];
+    T.t = T.r ? tg + toff[b2] : nullptr;
+    T.invh = T.r ? 1.f / fcell(L.g, T.r) : 0.f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) T.o[k] = forigin(L.g, k, pc[k]);
+    return T;
 }
 
 __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restrict__ soa, int64_t n,
                                                      const uint32_t* __restrict__ cs, float dt,
                                                      const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
-                                                     int* err) {
+                                                     int* err, DropIn D) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
+    if (D.perm && !sort_reusable(D.hash, false)) return;
     const uint32_t p0 = cs[L.off[0][b]], p1 = cs[L.off[0][b] + (uint32_t)(r * r * r)];
     if (p0 == p1) return;
     const uint32_t tb = tile_block(r);
@@ -1073,7 +1297,12 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
         tma_bulk_load(sm, tn_g + toff[b], tb * sizeof(float), &bar);
     }
     const bool ok = mbar_wait_bounded(&bar, 0, err);
-    if (!__syncthreads_and(ok)) return;
+    if (!__syncthreads_and(ok)) {
+        // the copy may still be in flight: wait for it (bounded) before the CTA gives up its memory
+        if (threadIdx.x == 0) mbar_wait_bounded(&bar, 0, err);
+        __syncthreads();
+        return;
+    }
     const Geo& g = L.g;
     int cb[3];
     bcoord(g, b, cb);
@@ -1091,18 +1320,50 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
         for (int a = 0; a < 3; ++a) k1[a] = tile_interp(sm, a, r, o, invh, x);
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.5f * dt * k1[a];
+        {
+            const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) k2[a] = sample_local(L, b, cb, r, o, invh, sm, toff, tn_g, a, y);
+            for (int a = 0; a < 3; ++a)  // shared-memory loads when the point stays in the block
+                k2[a] = T.t == sm ? tile_interp(sm, a, r, o, invh, y) : (T.t ? tile_interp(T.t, a, T.r, T.o, T.invh, y) : 0.f);
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.75f * dt * k2[a];
+        {
+            const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
 #pragma unroll
-        for (int a = 0; a < 3; ++a) k3[a] = sample_local(L, b, cb, r, o, invh, sm, toff, tn_g, a, y);
+            for (int a = 0; a < 3; ++a)  // shared-memory loads when the point stays in the block
+                k3[a] = T.t == sm ? tile_interp(sm, a, r, o, invh, y) : (T.t ? tile_interp(T.t, a, T.r, T.o, T.invh, y) : 0.f);
+        }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const float v = (2.f / 9.f) * k1[a] + (3.f / 9.f) * k2[a] + (4.f / 9.f) * k3[a];
             const float lo = g.dmin[a] + 0.01f * h0;
             const float hi = g.dmin[a] + (float)g.D[a] * g.bs - 0.01f * h0;
-            soa[(int64_t)a * n + i] = fminf(fmaxf(x[a] + dt * v, lo), hi);
+            const float xn = fminf(fmaxf(x[a] + dt * v, lo), hi);
+            if (D.perm) D.aos[3 * (size_t)D.perm[i] + a] = xn;
+            else soa[(int64_t)a * n + i] = xn;
+        }
+    }
+}
+
+// Drop-in mode, particles of inactive blocks (the last bucket of the sort): G2P samples zero velocity
+// there (v = alpha v), RK3 leaves them in place up to the domain clamp.  Caller arrays, through the
+// sort permutation; nothing is done unless the arrays still hash as when sorted.
+__global__ void k_inactive_aos(Geo g, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ bucket,
+                               float* aos, const unsigned long long* __restrict__ hash, int advect, float alpha) {
+    if (!sort_reusable(hash, !advect)) return;
+    const uint32_t p0 = bucket[0], p1 = bucket[1];
+    const float h0 = g.bs / (float)g.R0;
+    for (uint32_t j = p0 + blockIdx.x * blockDim.x + threadIdx.x; j < p1; j += gridDim.x * blockDim.x) {
+        float* p = aos + 3 * (size_t)perm[j];
+        for (int a = 0; a < 3; ++a) {
+            if (advect) {
+                const float lo = g.dmin[a] + 0.01f * h0;
+                const float hi = g.dmin[a] + (float)g.D[a] * g.bs - 0.01f * h0;
+                p[a] = fminf(fmaxf(p[a], lo), hi);
+            } else {
+                p[a] *= alpha;
+            }
         }
     }
 }
@@ -1154,7 +1415,12 @@ aw_status check_device_errors(MsbgState& G, cudaStream_t s) {
     int h[4];
     AW_CUDA(cudaMemcpyAsync(h, G.err.p, sizeof h, cudaMemcpyDeviceToHost, s));
     AW_CUDA(cudaStreamSynchronize(s));
-    if (h[1]) return set_error(AW_ERR_STATE, "TMA bulk-copy wait timed out in G2P");
+    if (h[1]) {
+        // reported once: the flag is cleared so that the next call starts clean
+        AW_CUDA(cudaMemsetAsync(G.err.p, 0, 4 * sizeof(int), s));
+        AW_CUDA(cudaStreamSynchronize(s));
+        return set_error(AW_ERR_STATE, "TMA bulk-copy wait timed out in G2P / advection");
+    }
     return AW_OK;
 }
 
@@ -1162,15 +1428,16 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
                      const float* uo[3], cudaStream_t s) {
     if (n <= 0) return AW_OK;
     AW_TRY(ensure_tiles(G));
-    // u_new tiles (for the advection that follows) and the blended tiles u_new - alpha u_old
-    Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
-    k_build_tiles_blend<<<G.nb, 128, 0, s>>>(G.view0(), fa, fb, alpha, G.tile_off.p, G.tiles_new.p, G.tiles_old.p);
-    AW_LAUNCH();
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
-    AW_CUDA(cudaFuncSetAttribute(k_g2p_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_g2p_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, alpha, G.tile_off.p, G.tiles_old.p, G.err.p + 1);
+    const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
+    AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
+    const int arm_only = G.test_copy_timeout ? 1 : 0;
+    const int polls = arm_only ? 1 << 10 : 1 << 20;
+    G.test_copy_timeout = false;
+    k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), soa, n, cs, alpha, fa, fb, G.tile_off.p, G.tiles_new.p,
+                                                 G.err.p + 1, polls, arm_only, DropIn{nullptr, nullptr, nullptr});
     AW_LAUNCH();
     k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
     AW_LAUNCH();
@@ -1178,7 +1445,9 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
 }
 
 __global__ void k_advect_tiles(LevelView L, PArrW pos, int64_t n, float dt, const uint32_t* __restrict__ toff,
-                               const float* __restrict__ tiles) {
+                               const float* __restrict__ tiles,
+                               const unsigned long long* __restrict__ skip = nullptr) {
+    if (skip && sort_reusable(skip, false)) return;  // the drop-in advection took the sorted path
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const Geo& g = L.g;
@@ -1206,7 +1475,9 @@ __global__ void k_advect_tiles(LevelView L, PArrW pos, int64_t n, float dt, cons
 
 // G2P / sampling on arbitrary (unsorted, AoS) particles through the ghosted tiles
 __global__ void k_g2p_tiles(LevelView L, PArr pos, PArrW vel, int64_t n, float alpha, const uint32_t* __restrict__ toff,
-                            const float* __restrict__ tn, const float* __restrict__ to) {
+                            const float* __restrict__ tn, const float* __restrict__ to,
+                            const unsigned long long* __restrict__ skip = nullptr) {
+    if (skip && sort_reusable(skip, true)) return;  // the drop-in G2P took the sorted path
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float X[3] = {pos(i, 0), pos(i, 1), pos(i, 2)};
@@ -1235,7 +1506,8 @@ aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs,
     const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
     if (smem > 48 * 1024)
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1);
+    k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1,
+                                          DropIn{nullptr, nullptr, nullptr});
     AW_LAUNCH();
     return AW_OK;
 }
@@ -1693,7 +1965,7 @@ extern "C" aw_status aw_p2g(aw_msbg* g, const float* d_pos, const float* d_vel, 
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     cudaStream_t s = (cudaStream_t)s_;
     MsbgState& G = g->st;
-    AW_TRY(sort_particles_soa(G, d_pos, d_vel, n, s));
+    AW_TRY(sort_particles_soa(G, d_pos, d_vel, n, s, /*record=*/true));
     float* u[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     float* m[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
     float* mo[3] = {G.ch[AW_MOMENTUM_X], G.ch[AW_MOMENTUM_Y], G.ch[AW_MOMENTUM_Z]};
@@ -1707,7 +1979,7 @@ extern "C" aw_status aw_p2g_phase(aw_msbg* g, const float* d_pos, const float* d
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     cudaStream_t s = (cudaStream_t)s_;
     MsbgState& G = g->st;
-    AW_TRY(sort_particles_soa(G, d_pos, d_vel, n, s));
+    AW_TRY(sort_particles_soa(G, d_pos, d_vel, n, s, /*record=*/true));
     float* u[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     float* m[3] = {G.ch[AW_MASS_DENSITY_X], G.ch[AW_MASS_DENSITY_Y], G.ch[AW_MASS_DENSITY_Z]};
     float* mo[3] = {G.ch[AW_MOMENTUM_X], G.ch[AW_MOMENTUM_Y], G.ch[AW_MOMENTUM_Z]};
@@ -1724,6 +1996,12 @@ extern "C" aw_status aw_p2g_phase(aw_msbg* g, const float* d_pos, const float* d
     return beta_sync(G, ph.beta, s);
 }
 
+extern "C" aw_status aw_test_arm_copy_timeout(aw_msbg* g) {
+    AW_CHECK_ARG(g, "null grid");
+    g->st.test_copy_timeout = true;
+    return AW_OK;
+}
+
 extern "C" aw_status aw_backup_grid_velocity(aw_msbg* g, aw_stream s_) {
     AW_CHECK_ARG(g && g->st.allocated, "grid not allocated");
     MsbgState& G = g->st;
@@ -1733,18 +2011,45 @@ extern "C" aw_status aw_backup_grid_velocity(aw_msbg* g, aw_stream s_) {
     return AW_OK;
 }
 
+// Drop-in G2P and RK3 on the caller's AoS arrays (G2PManager::performG2P / advect,
+// G2P.cuh:198-227).  When the arrays are the ones the last aw_p2g sorted and still hold the same
+// contents (64-bit content hashes compared on the device), the block-sorted kernels run on the
+// sorted copy aw_p2g made and write the caller's arrays through the sort permutation: G2P builds
+// its tile in shared memory and stages the particles by TMA bulk copies.  Otherwise, or for any other
+// arrays, the general path samples ghosted tiles in global memory particle by particle.  Both paths
+// are launched; the device picks one, so no host synchronisation is needed.
 extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_t n, float alpha, aw_stream s_) {
     AW_CHECK_ARG(g && ((d_pos && d_vel) || n == 0) && n >= 0, "bad argument");
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     MsbgState& G = g->st;
+    ParticleWork& W = G.pw;
     const float* un[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     const float* uo[3] = {G.ch[AW_VELOCITY_OLD_X], G.ch[AW_VELOCITY_OLD_Y], G.ch[AW_VELOCITY_OLD_Z]};
     if (n == 0) return AW_OK;
     cudaStream_t s = (cudaStream_t)s_;
     AW_TRY(ensure_tiles(G));
-    AW_TRY(build_tiles2(G, un, uo, s));
+    const unsigned long long* skip = nullptr;
+    if (W.src_valid && W.src_pos == d_pos && W.src_vel == d_vel && W.src_n == n) {
+        AW_CUDA(cudaMemsetAsync(W.hash.p + 2, 0, 2 * sizeof(unsigned long long), s));
+        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, d_vel, n, W.hash.p + 2);
+        AW_LAUNCH();
+        int maxres = 0;
+        for (int r : G.h_res) maxres = std::max(maxres, r);
+        const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
+        AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
+        k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,
+                                                     nullptr, G.err.p + 1, 1 << 20, 0, DropIn{W.sorted, d_vel, W.hash.p});
+        AW_LAUNCH();
+        k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_vel, W.hash.p, 0, alpha);
+        AW_LAUNCH();
+        skip = W.hash.p;
+    }
+    Field3 a{{un[0], un[1], un[2]}}, b{{uo[0], uo[1], uo[2]}};
+    k_build_tiles2<<<G.nb, 128, 0, s>>>(G.view0(), a, b, G.tile_off.p, G.tiles_new.p, G.tiles_old.p, skip);
+    AW_LAUNCH();
     k_g2p_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), PArr{d_pos, 3, 1}, PArrW{d_vel, 3, 1}, n, alpha, G.tile_off.p,
-                                        G.tiles_new.p, G.tiles_old.p);
+                                        G.tiles_new.p, G.tiles_old.p, skip);
     AW_LAUNCH();
     return AW_OK;
 }
@@ -1753,11 +2058,32 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
     AW_CHECK_ARG(g && (d_pos || n == 0) && n >= 0, "bad argument");
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     MsbgState& G = g->st;
+    ParticleWork& W = G.pw;
     const float* u[3] = {G.ch[AW_VELOCITY_X], G.ch[AW_VELOCITY_Y], G.ch[AW_VELOCITY_Z]};
     if (n == 0) return AW_OK;
+    cudaStream_t s = (cudaStream_t)s_;
     AW_TRY(ensure_tiles(G));
-    AW_TRY(build_tiles(G, u, G.tiles_new.p, (cudaStream_t)s_));
-    return advect_tiles(G, d_pos, 0, n, dt, G.tiles_new.p, (cudaStream_t)s_);
+    AW_TRY(build_tiles(G, u, G.tiles_new.p, s));  // both paths sample neighbouring blocks' u_new tiles
+    const unsigned long long* skip = nullptr;
+    if (W.src_valid && W.src_pos == d_pos && W.src_n == n) {
+        AW_CUDA(cudaMemsetAsync(W.hash.p + 2, 0, 2 * sizeof(unsigned long long), s));
+        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, nullptr, n, W.hash.p + 2);
+        AW_LAUNCH();
+        int maxres = 0;
+        for (int r : G.h_res) maxres = std::max(maxres, r);
+        const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
+        AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, dt, G.tile_off.p, G.tiles_new.p,
+                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p});
+        AW_LAUNCH();
+        k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_pos, W.hash.p, 1, 0.f);
+        AW_LAUNCH();
+        skip = W.hash.p;
+    }
+    k_advect_tiles<<<nblk(n), 256, 0, s>>>(G.view0(), PArrW{d_pos, 3, 1}, n, dt, G.tile_off.p, G.tiles_new.p, skip);
+    AW_LAUNCH();
+    W.src_valid = false;  // the positions have moved
+    return AW_OK;
 }
 
 // ------------------------------------------------------------------------------------------------

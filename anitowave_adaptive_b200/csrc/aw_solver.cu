@@ -83,6 +83,8 @@ struct aw_solver {
     aw::DBuf<double> p64tmp;
     aw::DBuf<double> cg_r, cg_d, cg_q, cg_sc;
     aw::DBuf<float> cg_zero;
+    // FP32 conjugate gradients: direction, -A d, scalars {rho, rho_old, d.(-A d)}, partial sums
+    aw::DBuf<float> cg32_d, cg32_q, cg32_sc, partials32;
     aw::DBuf<double> partials, norm;
     size_t smem_max = 0, smem_max64 = 0;
     // the whole V-cycle as a CUDA graph, captured once per (x0, b0) binding
@@ -841,6 +843,66 @@ __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, floa
     }
 }
 __global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
+
+// ---- conjugate gradients with every vector and scalar in FP32 (AW_PRECISION_FP32_PCG) ----------
+// The same V-cycle preconditioner as the mixed form, without its FP64 residual, direction and
+// accumulation: the like-for-like baseline of the mixed precision.  Partial sums and scalars are
+// FP32 as well.
+__device__ inline float block_sum_f(float v, float* red) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    float t = 0.f;
+    if (w == 0) {
+        t = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.f;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    }
+    return t;  // valid in thread 0
+}
+__global__ void k_dot32(const float* __restrict__ a, const float* __restrict__ b, const uint8_t* __restrict__ fluid,
+                        size_t n, float* __restrict__ part) {
+    __shared__ float red[32];
+    float acc = 0.f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        if (fluid[i]) acc += a[i] * b[i];
+    const float t = block_sum_f(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+__global__ void k_reduce_sum32(const float* __restrict__ part, int n, float* out) {
+    __shared__ float red[32];
+    float acc = 0.f;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
+    const float t = block_sum_f(acc, red);
+    if (threadIdx.x == 0) *out = t;
+}
+__global__ void k_cg_direction32(float* __restrict__ d, const float* __restrict__ z, const uint8_t* __restrict__ fluid,
+                                 const float* __restrict__ sc, int first, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float beta = first ? 0.f : sc[0] / sc[1];
+    d[i] = fluid[i] ? z[i] + beta * d[i] : 0.f;
+}
+// p += alpha d; r += alpha qn (qn = -A d, alpha = rho / (d . A d)); per-CTA partial sums of |r|^2
+__global__ void k_cg_update32(float* __restrict__ p, float* __restrict__ r, const float* __restrict__ d,
+                              const float* __restrict__ qn, const float* __restrict__ sc,
+                              const uint8_t* __restrict__ fluid, size_t n, float* __restrict__ part) {
+    __shared__ float red[32];
+    const float dq = -sc[2];
+    const float alpha = dq != 0.f ? sc[0] / dq : 0.f;
+    float acc = 0.f;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        p[i] += alpha * d[i];
+        const float rv = r[i] + alpha * qn[i];
+        r[i] = rv;
+        if (fluid[i]) acc += rv * rv;
+    }
+    const float t = block_sum_f(acc, red);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+__global__ void k_copy_scalar32(float* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1662,7 +1724,9 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
     AW_CHECK_ARG(g && d && out, "null argument");
     AW_CHECK_ARG(g->st.allocated, "grid not allocated");
     AW_CHECK_ARG(d->operator_mode == AW_OPERATOR_FV || d->operator_mode == AW_OPERATOR_REFERENCE, "bad operator mode");
-    AW_CHECK_ARG(d->precision == AW_PRECISION_FP32 || d->precision == AW_PRECISION_MIXED, "bad precision");
+    AW_CHECK_ARG(d->precision == AW_PRECISION_FP32 || d->precision == AW_PRECISION_MIXED ||
+                     d->precision == AW_PRECISION_FP32_PCG,
+                 "bad precision");
     AW_CHECK_ARG(d->block_iterations >= 1 && d->pre_smooth >= 0 && d->post_smooth >= 0, "bad smoother settings");
     *out = nullptr;
     MsbgState& G = g->st;
@@ -1808,6 +1872,16 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         AW_TRY(S->cg_zero.alloc(nc0));
         AW_CUDA(cudaMemset(S->cg_zero.p, 0, nc0 * sizeof(float)));
         AW_CUDA(cudaMemset(S->cg_d.p, 0, nc0 * sizeof(double)));
+    }
+    if (d->precision == AW_PRECISION_FP32_PCG) {
+        const size_t nc0 = S->lv[0].ncell();
+        AW_TRY(S->cg32_d.alloc(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->cg32_q.alloc(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->cg32_sc.alloc(4));
+        AW_TRY(S->cg_zero.alloc(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->partials32.alloc(4096));
+        AW_CUDA(cudaMemset(S->cg_zero.p, 0, std::max<size_t>(nc0, 1) * sizeof(float)));
+        AW_CUDA(cudaMemset(S->cg32_d.p, 0, std::max<size_t>(nc0, 1) * sizeof(float)));
     }
     size_t nparts = (size_t)nb + 1024;
     AW_TRY(S->partials.alloc(nparts));
@@ -2008,6 +2082,89 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
         }
         S->x0 = nullptr;
         S->b0 = nullptr;
+    } else if (S->d.precision == AW_PRECISION_FP32_PCG) {
+        // Conjugate gradients preconditioned by the same V-cycle as the mixed form, with the pressure,
+        // residual, direction and every scalar in FP32 (the like-for-like FP32 baseline of the mixed
+        // precision).  r lives in the level-0 right-hand side array, the V-cycle's input.
+        float* p = (float*)d_p;
+        float* sc = S->cg32_sc.p;
+        int nsm = 148;
+        {
+            int dev = 0;
+            if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        }
+        const unsigned ndot = (unsigned)std::min<size_t>((size_t)nsm * 8, S->partials32.n);
+        XStore xp, xd;
+        xp.f = p;
+        xd.f = S->cg32_d.p;
+        auto launch_err = [&](const char* what) -> aw_status {
+            ++g_launches;
+            cudaError_t e = cudaGetLastError();
+            return e == cudaSuccess ? AW_OK : set_error(AW_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+        };
+        auto read_norm32 = [&](double* out) -> aw_status {
+            k_reduce_sum32<<<1, 256, 0, s>>>(S->partials32.p, (int)ndot, sc + 3);
+            AW_TRY(launch_err("k_reduce_sum32"));
+            if (!S->h_norm) AW_CUDA(cudaHostAlloc((void**)&S->h_norm, sizeof(double), cudaHostAllocDefault));
+            AW_CUDA(cudaMemcpyAsync(S->h_norm, sc + 3, sizeof(float), cudaMemcpyDeviceToHost, s));
+            AW_CUDA(cudaStreamSynchronize(s));
+            float f;
+            memcpy(&f, S->h_norm, sizeof f);
+            *out = std::sqrt((double)f);
+            return AW_OK;
+        };
+        // r = b - A p into the V-cycle's input; its norm (FP64 partial sums) for the stopping test
+        auto true_residual = [&]() -> aw_status {
+            k_residual<SrcX><<<L0.ndesc[2], 256, L0.smem_smooth, s>>>(SrcX{xp}, d_b, coef(L0), L0.fluid.p, batch(L0, 2),
+                                                                       cf, L0.b.p, nullptr, S->partials.p);
+            return launch_err("k_residual");
+        };
+        st = L0.ndesc[2] ? true_residual() : AW_OK;
+        double rn = 0;
+        if (st == AW_OK) st = read_norm(S, nlist, s, &rn);
+        bool restart = true;
+        while (st == AW_OK) {
+            rel = rn / bn;
+            if (!(rel == rel)) {
+                st = set_error(AW_ERR_NAN, "residual became NaN after %d iterations", it);
+                break;
+            }
+            if (rel < S->d.tolerance) {
+                if (restart) break;
+                st = true_residual();
+                if (st == AW_OK) st = read_norm(S, nlist, s, &rn);
+                restart = true;
+                continue;
+            }
+            if (it >= S->d.max_cycles) {
+                st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d iterations", rel, it);
+                break;
+            }
+            st = zero_x(S, 0, s);
+            if (st == AW_OK) st = run_vcycle(S, s);
+            if (st != AW_OK) break;
+            k_dot32<<<ndot, 256, 0, s>>>(L0.b.p, L0.x.p, L0.fluid.p, nc, S->partials32.p);
+            if ((st = launch_err("k_dot32")) != AW_OK) break;
+            k_reduce_sum32<<<1, 256, 0, s>>>(S->partials32.p, (int)ndot, sc + 0);
+            if ((st = launch_err("k_reduce_sum32")) != AW_OK) break;
+            k_cg_direction32<<<nblk(nc), 256, 0, s>>>(S->cg32_d.p, L0.x.p, L0.fluid.p, sc, restart ? 1 : 0, nc);
+            if ((st = launch_err("k_cg_direction32")) != AW_OK) break;
+            k_residual<SrcX><<<L0.ndesc[2], 256, L0.smem_smooth, s>>>(SrcX{xd}, S->cg_zero.p, coef(L0), L0.fluid.p,
+                                                                       batch(L0, 2), cf, S->cg32_q.p, nullptr, nullptr);
+            if ((st = launch_err("k_residual (A d)")) != AW_OK) break;
+            k_dot32<<<ndot, 256, 0, s>>>(S->cg32_d.p, S->cg32_q.p, L0.fluid.p, nc, S->partials32.p);
+            if ((st = launch_err("k_dot32")) != AW_OK) break;
+            k_reduce_sum32<<<1, 256, 0, s>>>(S->partials32.p, (int)ndot, sc + 2);
+            if ((st = launch_err("k_reduce_sum32")) != AW_OK) break;
+            k_cg_update32<<<ndot, 256, 0, s>>>(p, L0.b.p, S->cg32_d.p, S->cg32_q.p, sc, L0.fluid.p, nc,
+                                               S->partials32.p);
+            if ((st = launch_err("k_cg_update32")) != AW_OK) break;
+            k_copy_scalar32<<<1, 1, 0, s>>>(sc, 1, 0);
+            if ((st = launch_err("k_copy_scalar32")) != AW_OK) break;
+            ++it;
+            restart = false;
+            st = read_norm32(&rn);
+        }
     } else {
         // Mixed precision: conjugate gradients preconditioned by the FP32 V-cycle (FP16-stored coarse
         // corrections), with the residual, the search direction and the pressure accumulation in

@@ -39,7 +39,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if res.returncode != 0:
         sys.stderr.write(res.stdout + res.stderr)
         raise RuntimeError("nvcc failed")
-    with open(os.path.join(PKG, "ptxas_info.txt"), "w") as f:
+    # register / spill / shared-memory report of every kernel, kept out of the tracked tree
+    os.makedirs(os.path.join(PKG, "_build"), exist_ok=True)
+    with open(os.path.join(PKG, "_build", "ptxas_info.txt"), "w") as f:
         f.write(res.stderr.replace(ROOT + os.sep, ""))  # paths relative to the repository
     if verbose:
         sys.stderr.write(res.stderr)

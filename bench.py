@@ -290,6 +290,7 @@ def run_ours(args, ws, rank, local):
     assert torch.equal(vel_out[(e2e_steps - 1) & 1], vel_d[(e2e_steps - 1) & 1].cpu())
     e2e_ms = max_over_ranks(ws, e0.elapsed_time(e1))
     e2e_value = ws * S.n * e2e_steps / (e2e_ms / 1e3) / 1e6
+    dropin = dropin_bench(g, S, pos_d[0], vel_d[0], pos_h, vel_h)
 
     poisson = None
     if not args.skip_poisson:
@@ -330,6 +331,7 @@ def run_ours(args, ws, rank, local):
         "solver": {"cycles": last["cycles"], "residual": last["residual"], "div_before": last["div_before"],
                    "div_after": last["div_after"]},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": S.n * 24, "d2h_bytes_per_step": S.n * 12},
+        "dropin_ms": dropin,
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,
@@ -345,18 +347,50 @@ def run_ours(args, ws, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def dropin_bench(g, S, pos, vel, pos_h, vel_h, reps=5):
+    """Device time of the drop-in calls alone on resident AoS arrays: aw_p2g (sort + P2G), then
+    aw_g2p, and aw_advect after another aw_p2g (each reuses the sort of the aw_p2g before it)."""
+    import torch
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    tot = {"p2g": 0.0, "g2p": 0.0, "advect": 0.0}
+    for it in range(reps + 1):
+        pos.copy_(pos_h)
+        vel.copy_(vel_h)
+        ev[0].record()
+        g.p2g(pos, vel)
+        ev[1].record()
+        g.backup_grid_velocity()
+        ev[2].record()
+        g.g2p(vel, pos, S.alpha)
+        ev[3].record()
+        g.p2g(pos, vel)
+        ev[4].record()
+        g.advect(pos, S.dt)
+        ev[5].record()
+        torch.cuda.synchronize()
+        if it:  # the first round warms up
+            tot["p2g"] += ev[0].elapsed_time(ev[1])
+            tot["g2p"] += ev[2].elapsed_time(ev[3])
+            tot["advect"] += ev[4].elapsed_time(ev[5])
+    return {k: v / reps for k, v in tot.items()}
+
+
 def poisson_bench(args):
-    """poisson_256: closed box, level map from 32 spheres, blob divergence; FP32 vs mixed."""
+    """poisson_256: closed box, level map from 32 spheres, blob divergence.  Three forms: the plain
+    FP32 V-cycle iteration, conjugate gradients preconditioned by the same V-cycle with every vector
+    and scalar in FP32 (fp32_pcg), and the mixed form (the same CG with FP64 residual, direction and
+    accumulation, FP16-stored coarse corrections).  fp32_pcg vs mixed isolates the precision."""
     import torch
     import anitowave_adaptive_b200 as aw
     from anitowave_adaptive_b200 import poisson as pz
     prob = pz.build_problem(256)
     out = {"workload": "poisson_256", "cells": int(prob.b.numel())}
-    for name, prec in (("fp32", aw.PRECISION_FP32), ("mixed", aw.PRECISION_MIXED)):
-        for tol in (1e-6, 1e-9):
+    for name, prec in (("fp32", aw.PRECISION_FP32), ("fp32_pcg", aw.PRECISION_FP32_PCG),
+                       ("mixed", aw.PRECISION_MIXED)):
+        for tol in (1e-5, 1e-6, 1e-9):
             sv = aw.Solver(prob.grid, precision=prec, tolerance=tol, max_cycles=60)
             sv.setup(None)
-            p = torch.zeros(prob.b.numel(), dtype=torch.float32 if prec == aw.PRECISION_FP32 else torch.float64,
+            p = torch.zeros(prob.b.numel(), dtype=torch.float64 if prec == aw.PRECISION_MIXED else torch.float32,
                             device="cuda")
             sv.solve(prob.b, p, raise_on_error=False)  # warm
             times = []
@@ -368,12 +402,15 @@ def poisson_bench(args):
                 torch.cuda.synchronize()
                 times.append(1e3 * (time.perf_counter() - t0))
             div = prob.divergence_after(sv, p)
+            div64 = prob.divergence_after(sv, p, fp64=True)
             out[f"{name}_{tol:.0e}"] = {"ms": min(times), "cycles": cyc, "rel_residual": rel,
-                                        "converged": st == 0, "div_after": div}
+                                        "converged": st == 0, "div_after": div, "div_after_fp64": div64}
             sv.close()
-    a, b = out.get("fp32_1e-06"), out.get("mixed_1e-06")
-    if a and b and a["converged"] and b["converged"]:
-        out["speedup_mixed_vs_fp32_1e-6"] = a["ms"] / b["ms"]
+    for base in ("fp32", "fp32_pcg"):
+        for tol in ("1e-05", "1e-06", "1e-09"):
+            a, b = out.get(f"{base}_{tol}"), out.get(f"mixed_{tol}")
+            if a and b and a["converged"] and b["converged"]:
+                out[f"speedup_mixed_vs_{base}_{tol}"] = a["ms"] / b["ms"]
     return out
 
 
@@ -404,7 +441,8 @@ def flip256_bench(steps=5, warmup=2):
     g = aw.build_grid(S)
     tot = g.totals()
     out = {"workload": "dam_drop2_256", "particles": S.n, "cells": tot[0], "faces": sum(tot[1:]), "steps": steps}
-    for name, prec, tol in (("mixed", aw.PRECISION_MIXED, 1e-6), ("fp32", aw.PRECISION_FP32, 1e-5)):
+    for name, prec, tol in (("mixed", aw.PRECISION_MIXED, 1e-6), ("fp32_pcg", aw.PRECISION_FP32_PCG, 1e-5),
+                            ("fp32", aw.PRECISION_FP32, 1e-5)):
         F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=prec, tolerance=tol, max_cycles=60)
         try:
             for _ in range(warmup):

@@ -154,6 +154,12 @@ aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_t n, float 
  * current) and should come before any stream capture.  All calls share the array: calls that
  * overlap on the GPU race. */
 aw_status aw_g2p_noalloc(aw_msbg* g, float* d_vel, const float* d_pos, int64_t n, float alpha, aw_stream s);
+
+/* Test hook, no counterpart in the reference.  The next G2P launch of a FLIP step on this grid arms
+ * its first particle-copy barrier without issuing the copy and polls it only 1,024 times, so that
+ * the bounded wait runs out without any fault: the CTAs drain their other copies and return, the
+ * step returns AW_ERR_STATE, and the following step runs normally. */
+aw_status aw_test_arm_copy_timeout(aw_msbg* g);
 /* G2PManager::advect (G2P.cuh:216-227): Ralston RK3 through VELOCITY_*, clamped to the domain
  * interior (margin 0.01 finest cells). */
 aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw_stream s);
@@ -178,14 +184,25 @@ aw_status aw_add_gravity(aw_msbg* g, const float gravity[3], float dt, aw_stream
  * (device float, must start at 0) receives max |div u| per unit volume */
 aw_status aw_velocity_divergence(aw_msbg* g, const uint8_t* d_fluid, float inv_dt, float* d_out, float* d_max,
                                  aw_stream s);
+/* *d_max (device double) = max over fluid cells (every cell when d_fluid is NULL) of |div u| per unit
+ * volume, the face sums of VELOCITY_* taken in FP64.  No counterpart in the reference: it reports
+ * the divergence an FP32 field really has, free of the rounding of an FP32 sum. */
+aw_status aw_velocity_divergence_max64(aw_msbg* g, const uint8_t* d_fluid, double* d_max, aw_stream s);
 
 /* ---- pressure solver -------------------------------------------------------------------------- */
 enum { AW_OPERATOR_FV = 0, AW_OPERATOR_REFERENCE = 1 };
-enum { AW_PRECISION_FP32 = 0, AW_PRECISION_MIXED = 1 };
+/* AW_PRECISION_FP32: V-cycle iteration on an FP32 pressure (runCycle repeated, VCycle.cuh:251-304).
+ * AW_PRECISION_MIXED: conjugate gradients preconditioned by the V-cycle, FP32 arithmetic inside the
+ *   cycle with FP16-stored coarse corrections (per-block scale), FP64 residual, direction, pressure
+ *   accumulation and coarsest solve; the pressure is FP64.
+ * AW_PRECISION_FP32_PCG: the same preconditioned conjugate gradients with every vector and scalar in
+ *   FP32 and FP32 storage on every level; the pressure is FP32.  No counterpart in the reference: the
+ *   like-for-like FP32 baseline of the mixed form. */
+enum { AW_PRECISION_FP32 = 0, AW_PRECISION_MIXED = 1, AW_PRECISION_FP32_PCG = 2 };
 
 typedef struct aw_solver_desc {
     int32_t operator_mode;       /* AW_OPERATOR_FV (finite-volume, symmetric) or _REFERENCE */
-    int32_t precision;           /* AW_PRECISION_FP32 or AW_PRECISION_MIXED */
+    int32_t precision;           /* AW_PRECISION_FP32, _MIXED or _FP32_PCG */
     int32_t mg_levels;           /* block-structured MG levels (0 = default) */
     int32_t pre_smooth;          /* runCycle pre-smoothing iterations (VCycle.cuh:262) */
     int32_t post_smooth;         /* runCycle post-smoothing iterations (VCycle.cuh:303) */
@@ -214,7 +231,7 @@ aw_status aw_solver_setup(aw_solver* sv, const uint8_t* d_fluid, aw_stream s);
  * Stream-ordered; no counterpart in the reference, whose coefficients are fixed at init. */
 aw_status aw_solver_update_coefficients(aw_solver* sv, aw_stream s);
 aw_status aw_solver_num_levels(const aw_solver* sv, int32_t* n);
-/* precision of the solver (AW_PRECISION_FP32 or AW_PRECISION_MIXED) */
+/* precision of the solver (AW_PRECISION_FP32, _MIXED or _FP32_PCG) */
 aw_status aw_solver_precision(const aw_solver* sv, int32_t* precision);
 /* level arrays: which 0 = x, 1 = b, 2 = r (float), 3..5 = coefficients x/y/z (float),
  * 6 = fluid (u8), 7 = cell offsets, 8..10 = face offsets (u32; MSBG levels only) */

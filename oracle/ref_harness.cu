@@ -13,6 +13,7 @@
 // block-uniform and the kernel is free of the divergent barrier.
 // the reference headers rely on the includes that precede them in main.cu:1-4
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <iostream>
 #include <vector>
@@ -383,88 +384,175 @@ REF_API int ref_normalize(const int dims[3], const uint32_t* levels, const float
     return (int)cudaGetLastError();
 }
 
-// Timing of the reference's own transfer and solver kernels (CUDA events, ms per call) on a
-// uniform single-level grid: P2GTransfer::run, G2PManager::performG2P + advect, runCycle.
-REF_API int ref_time_kernels(const int dims[3], uint32_t level, const float* pos, const float* vel, uint32_t n,
-                             int reps, float* ms_out) {
+// ---- Transfer kernels launched directly (no G2PManager / P2GTransfer calls) --------------------
+// The managers' host paths are avoided on purpose: G2PManager::performG2P copies a pointer table
+// into a host stack array and leaks a device allocation per call (G2P.cuh:198-211).  Here the
+// backup fields and the device pointer table of g2pUpdateKernel are built by the harness.
+namespace {
+
+struct TransferGrid {
+    Grid* G = nullptr;
+    std::vector<float*> fx, fy, fz;
+    float* backup[3] = {nullptr, nullptr, nullptr};
+    float** d_backup = nullptr;
+    uint32_t tot[3] = {0, 0, 0};
+    ~TransferGrid() {
+        for (float* p : backup)
+            if (p) cudaFree(p);
+        if (d_backup) cudaFree(d_backup);
+        delete G;
+    }
+};
+
+// single-level map (every block at `level`), channels allocated, VELOCITY_* = un, backup = uo
+TransferGrid* make_transfer_grid(const int dims[3], uint32_t level, const float* const* un, const float* const* uo) {
+    TransferGrid* T = new TransferGrid();
     uint32_t nb = (uint32_t)dims[0] * dims[1] * dims[2];
     std::vector<uint32_t> lv(nb, level);
-    Grid* G = make_grid(dims, lv.data(), true);
-    MSBGManager& mg = *G->mg;
-    float3 *dp, *dv;
-    cudaMalloc(&dp, n * sizeof(float3));
-    cudaMalloc(&dv, n * sizeof(float3));
+    T->G = make_grid(dims, lv.data(), true);
+    MSBG& g = T->G->mg->grid;
+    T->fx = channel_table(g.d_faceXData);
+    T->fy = channel_table(g.d_faceYData);
+    T->fz = channel_table(g.d_faceZData);
+    T->tot[0] = g.totalFacesX;
+    T->tot[1] = g.totalFacesY;
+    T->tot[2] = g.totalFacesZ;
+    float* vel[3] = {T->fx[VELOCITY_X], T->fy[VELOCITY_Y], T->fz[VELOCITY_Z]};
+    for (int a = 0; a < 3; ++a) {
+        if (un) cudaMemcpy(vel[a], un[a], T->tot[a] * sizeof(float), cudaMemcpyHostToDevice);
+        else cudaMemset(vel[a], 0, T->tot[a] * sizeof(float));
+        cudaMalloc(&T->backup[a], std::max<uint32_t>(T->tot[a], 1) * sizeof(float));
+        if (uo) cudaMemcpy(T->backup[a], uo[a], T->tot[a] * sizeof(float), cudaMemcpyHostToDevice);
+        else cudaMemcpy(T->backup[a], vel[a], T->tot[a] * sizeof(float), cudaMemcpyDeviceToDevice);
+    }
+    cudaMalloc(&T->d_backup, 3 * sizeof(float*));
+    cudaMemcpy(T->d_backup, T->backup, 3 * sizeof(float*), cudaMemcpyHostToDevice);
+    return T;
+}
+
+float3 domain_size(const MSBG& g) {
+    return make_float3(g.indexDims.x * g.blockSize, g.indexDims.y * g.blockSize, g.indexDims.z * g.blockSize);
+}
+
+}  // namespace
+
+// g2pUpdateKernel (G2P.cuh:87-128) on a single-level map: VELOCITY_* = un, backup fields = uo;
+// vel (n float3, in/out), pos (n float3)
+REF_API int ref_g2p_blend(const int dims[3], uint32_t level, const float* const* un, const float* const* uo,
+                          const float* pos, float* vel, uint32_t n, float alpha) {
+    TransferGrid* T = make_transfer_grid(dims, level, un, uo);
+    float3 *dp = nullptr, *dv = nullptr;
+    cudaMalloc(&dp, std::max<uint32_t>(n, 1) * sizeof(float3));
+    cudaMalloc(&dv, std::max<uint32_t>(n, 1) * sizeof(float3));
     cudaMemcpy(dp, pos, n * sizeof(float3), cudaMemcpyHostToDevice);
     cudaMemcpy(dv, vel, n * sizeof(float3), cudaMemcpyHostToDevice);
-    std::vector<float*> fx = channel_table(mg.grid.d_faceXData), fy = channel_table(mg.grid.d_faceYData),
-                        fz = channel_table(mg.grid.d_faceZData), cc = channel_table(mg.grid.d_cellData);
-    cudaMemset(fx[BETA_COEFF_X], 0, mg.grid.totalFacesX * 4);
-    std::vector<float> ones(std::max({mg.grid.totalFacesX, mg.grid.totalFacesY, mg.grid.totalFacesZ}), 1.f);
-    cudaMemcpy(fx[BETA_COEFF_X], ones.data(), mg.grid.totalFacesX * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(fy[BETA_COEFF_Y], ones.data(), mg.grid.totalFacesY * 4, cudaMemcpyHostToDevice);
-    cudaMemcpy(fz[BETA_COEFF_Z], ones.data(), mg.grid.totalFacesZ * 4, cudaMemcpyHostToDevice);
-    const int ch[] = {MOMENTUM_X, MASS_DENSITY_X, VELOCITY_X};
-    for (int c : ch) {
-        cudaMemset(fx[c], 0, mg.grid.totalFacesX * 4);
-        cudaMemset(fy[c + 1], 0, mg.grid.totalFacesY * 4);
-        cudaMemset(fz[c + 2], 0, mg.grid.totalFacesZ * 4);
+    if (n) g2pUpdateKernel<<<(n + 255) / 256, 256>>>(T->G->mg->grid, dv, dp, n, T->d_backup, alpha);
+    cudaDeviceSynchronize();
+    cudaMemcpy(vel, dv, n * sizeof(float3), cudaMemcpyDeviceToHost);
+    cudaFree(dp);
+    cudaFree(dv);
+    int err = (int)cudaGetLastError();
+    delete T;
+    return err;
+}
+
+// advectParticlesKernel (G2P.cuh:131-173) on a single-level map with VELOCITY_* = u; pos in/out
+REF_API int ref_advect(const int dims[3], uint32_t level, const float* const* u, float* pos, uint32_t n, float dt) {
+    TransferGrid* T = make_transfer_grid(dims, level, u, nullptr);
+    float3* dp = nullptr;
+    cudaMalloc(&dp, std::max<uint32_t>(n, 1) * sizeof(float3));
+    cudaMemcpy(dp, pos, n * sizeof(float3), cudaMemcpyHostToDevice);
+    if (n) advectParticlesKernel<<<(n + 255) / 256, 256>>>(T->G->mg->grid, dp, n, dt, domain_size(T->G->mg->grid));
+    cudaDeviceSynchronize();
+    cudaMemcpy(pos, dp, n * sizeof(float3), cudaMemcpyDeviceToHost);
+    cudaFree(dp);
+    int err = (int)cudaGetLastError();
+    delete T;
+    return err;
+}
+
+// Timing of the reference's own kernels (CUDA events, ms per call) on a single-level map with every
+// block active, launched directly in the launch shapes of the reference's managers:
+//   ms_out[0] p2g + the three normalizeVelocity launches     (P2GTransfer::run, P2G.cuh:175-195)
+//   ms_out[1] three D2D backup copies + g2pUpdateKernel      (G2PManager, G2P.cuh:192-211)
+//   ms_out[2] advectParticlesKernel                          (G2PManager::advect, G2P.cuh:216-227)
+//   ms_out[3] one V-cycle from level 0 with 1-thread smoother CTAs (runCycle, VCycle.cuh:251-304)
+// Progress goes to stderr after each stage.  The velocity fields are zero and the coefficients one.
+REF_API int ref_time_kernels(const int dims[3], uint32_t level, const float* pos, const float* vel, uint32_t n,
+                             int reps, float* ms_out) {
+    TransferGrid* T = make_transfer_grid(dims, level, nullptr, nullptr);
+    MSBGManager& mg = *T->G->mg;
+    MSBG& g = mg.grid;
+    float3 *dp = nullptr, *dv = nullptr, *dp2 = nullptr;
+    cudaMalloc(&dp, std::max<uint32_t>(n, 1) * sizeof(float3));
+    cudaMalloc(&dv, std::max<uint32_t>(n, 1) * sizeof(float3));
+    cudaMalloc(&dp2, std::max<uint32_t>(n, 1) * sizeof(float3));
+    cudaMemcpy(dp, pos, n * sizeof(float3), cudaMemcpyHostToDevice);
+    cudaMemcpy(dv, vel, n * sizeof(float3), cudaMemcpyHostToDevice);
+    cudaMemcpy(dp2, dp, n * sizeof(float3), cudaMemcpyDeviceToDevice);
+    std::vector<float*> cc = channel_table(g.d_cellData);
+    const int face_ch[] = {BETA_COEFF_X, MASS_DENSITY_X, MOMENTUM_X, PHASE_FIELD_X};
+    std::vector<float> ones(std::max({T->tot[0], T->tot[1], T->tot[2], 1u}), 1.f);
+    for (int c : face_ch) {
+        cudaMemset(T->fx[c], 0, T->tot[0] * 4);
+        cudaMemset(T->fy[c + 1], 0, T->tot[1] * 4);
+        cudaMemset(T->fz[c + 2], 0, T->tot[2] * 4);
     }
-    cudaMemset(cc[PRESSURE], 0, mg.grid.totalCells * 4);
-    cudaMemset(cc[DIVERGENCE], 0, mg.grid.totalCells * 4);
+    cudaMemcpy(T->fx[BETA_COEFF_X], ones.data(), T->tot[0] * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(T->fy[BETA_COEFF_Y], ones.data(), T->tot[1] * 4, cudaMemcpyHostToDevice);
+    cudaMemcpy(T->fz[BETA_COEFF_Z], ones.data(), T->tot[2] * 4, cudaMemcpyHostToDevice);
+    cudaMemset(cc[PRESSURE], 0, g.totalCells * 4);
+    cudaMemset(cc[DIVERGENCE], 0, g.totalCells * 4);
+    cudaDeviceSynchronize();
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    P2GTransfer p2g;
-    G2PManager g2p;
-    g2p.init(mg);
-    float t;
-    // P2G
-    p2g.run(mg, dp, dv, n);
-    cudaEventRecord(e0);
-    for (int i = 0; i < reps; ++i) p2g.run(mg, dp, dv, n);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&t, e0, e1);
-    ms_out[0] = t / reps;
-    // G2P (backup + FLIP blend)
-    g2p.backupGridVelocity(mg);
-    g2p.performG2P(mg, dv, dp, n, 0.95f);
-    cudaEventRecord(e0);
-    for (int i = 0; i < reps; ++i) {
-        g2p.backupGridVelocity(mg);
-        g2p.performG2P(mg, dv, dp, n, 0.95f);
+    const unsigned pb = (n + 255) / 256;
+    auto run_p2g = [&]() {
+        if (n) p2g<<<pb, 256>>>(g, dp, dv, n, 1.0f, 0.0f);
+        normalizeVelocity<<<g.numBlocks, 256>>>(g, MOMENTUM_X, MASS_DENSITY_X, VELOCITY_X, AXIS_X);
+        normalizeVelocity<<<g.numBlocks, 256>>>(g, MOMENTUM_Y, MASS_DENSITY_Y, VELOCITY_Y, AXIS_Y);
+        normalizeVelocity<<<g.numBlocks, 256>>>(g, MOMENTUM_Z, MASS_DENSITY_Z, VELOCITY_Z, AXIS_Z);
+    };
+    float* vch[3] = {T->fx[VELOCITY_X], T->fy[VELOCITY_Y], T->fz[VELOCITY_Z]};
+    auto run_g2p = [&]() {
+        for (int a = 0; a < 3; ++a)
+            cudaMemcpyAsync(T->backup[a], vch[a], T->tot[a] * sizeof(float), cudaMemcpyDeviceToDevice);
+        if (n) g2pUpdateKernel<<<pb, 256>>>(g, dv, dp, n, T->d_backup, 0.95f);
+    };
+    auto run_advect = [&]() {
+        if (n) advectParticlesKernel<<<pb, 256>>>(g, dp2, n, 1.0f / 240, domain_size(g));
+    };
+    auto timed = [&](auto&& fn, int r) {
+        fn();
+        cudaDeviceSynchronize();
+        cudaEventRecord(e0);
+        for (int i = 0; i < r; ++i) fn();
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        return t / r;
+    };
+    ms_out[0] = timed(run_p2g, reps);
+    fprintf(stderr, "ref_time_kernels: p2g %.4f ms (%s)\n", ms_out[0], cudaGetErrorString(cudaGetLastError()));
+    ms_out[1] = timed(run_g2p, reps);
+    fprintf(stderr, "ref_time_kernels: g2p %.4f ms (%s)\n", ms_out[1], cudaGetErrorString(cudaGetLastError()));
+    ms_out[2] = timed(run_advect, reps);
+    fprintf(stderr, "ref_time_kernels: advect %.4f ms (%s)\n", ms_out[2], cudaGetErrorString(cudaGetLastError()));
+    {
+        VCycleSolver S(MAX_LEVELS, g.numBlocks);
+        S.init(mg);
+        ms_out[3] = timed([&]() { run_cycle_1t(S, mg, 0); }, 1);
+        fprintf(stderr, "ref_time_kernels: vcycle (1-thread smoother CTAs) %.4f ms (%s)\n", ms_out[3],
+                cudaGetErrorString(cudaGetLastError()));
     }
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&t, e0, e1);
-    ms_out[1] = t / reps;
-    // advect (RK3), on a copy of the positions
-    float3* dp2;
-    cudaMalloc(&dp2, n * sizeof(float3));
-    cudaMemcpy(dp2, dp, n * sizeof(float3), cudaMemcpyDeviceToDevice);
-    g2p.advect(mg, dp2, n, 1.0f / 240);
-    cudaEventRecord(e0);
-    for (int i = 0; i < reps; ++i) g2p.advect(mg, dp2, n, 1.0f / 240);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&t, e0, e1);
-    ms_out[2] = t / reps;
-    // one V-cycle (1-thread smoother CTAs)
-    VCycleSolver S(MAX_LEVELS, mg.grid.numBlocks);
-    S.init(mg);
-    run_cycle_1t(S, mg, 0);
-    cudaEventRecord(e0);
-    run_cycle_1t(S, mg, 0);
-    cudaEventRecord(e1);
-    cudaEventSynchronize(e1);
-    cudaEventElapsedTime(&t, e0, e1);
-    ms_out[3] = t;
-    g2p.cleanup();
     cudaFree(dp);
     cudaFree(dv);
     cudaFree(dp2);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    delete G;
-    return (int)cudaGetLastError();
+    int err = (int)cudaGetLastError();
+    delete T;
+    return err;
 }

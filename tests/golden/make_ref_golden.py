@@ -7,7 +7,7 @@ constants: 16^3 base blocks, 3 levels).  Writes tests/golden/ref_*.npz (or the d
 the first argument).  The fixtures pin the oracle (tests/test_golden.py, CPU) and the library's
 reference-operator mode (tests/test_golden_gpu.py).
 
-    python tests/golden/make_ref_golden.py [outdir]
+    python tests/golden/make_ref_golden.py [outdir] [--only=transfer]
 """
 from __future__ import annotations
 
@@ -43,6 +43,8 @@ def load():
                             C.c_void_p, C.c_void_p]
     L.ref_level_beta.argtypes = [i32p, u32p, PP, C.c_int, PP]
     L.ref_normalize.argtypes = [i32p, u32p, PP, PP, PP]
+    L.ref_g2p_blend.argtypes = [i32p, C.c_uint32, PP, PP, f32p, f32p, C.c_uint32, C.c_float]
+    L.ref_advect.argtypes = [i32p, C.c_uint32, PP, f32p, C.c_uint32, C.c_float]
     return L
 
 
@@ -62,10 +64,48 @@ def coarse_offsets(L, dims, lv, m):
     return out, tot
 
 
-def main(outdir):
+def transfer_fixtures(L, outdir):
+    """g2pUpdateKernel (G2P.cuh:87-128) and advectParticlesKernel (G2P.cuh:131-173) on inputs where
+    the reference is in bounds and its MAC staggering defects do not matter: single-level maps with
+    every block active, a velocity field uniform per axis, and particles at least two cells from the
+    domain walls (the reference samples 0 across the wall).  This pins the FLIP blend algebra and the
+    RK3 stages given identical sampled velocities.  Reference grid: block size 1, origin 0."""
+    rng = np.random.default_rng(2025)
+    out = {}
+    for case, (dims, level) in enumerate((((2, 2, 2), 0), ((3, 2, 2), 1))):
+        d = np.array(dims, np.int32)
+        nb = int(np.prod(dims))
+        lv = np.full(nb, level, np.uint32)
+        _, t = coarse_offsets(L, dims, lv, 0)
+        h = 1.0 / (16 >> level)
+        n = 4096
+        lo = np.array([2 * h] * 3)
+        hi = np.array(dims, np.float64) - 2 * h
+        pos = (lo + rng.random((n, 3)) * (hi - lo)).astype(np.float32)
+        vel = rng.standard_normal((n, 3)).astype(np.float32)
+        cn = rng.standard_normal(3).astype(np.float32)
+        co = rng.standard_normal(3).astype(np.float32)
+        un = [np.full(int(t[1 + a]), cn[a], np.float32) for a in range(3)]
+        uo = [np.full(int(t[1 + a]), co[a], np.float32) for a in range(3)]
+        alpha, dt = np.float32(0.95), np.float32(1.0 / 240)
+        v_out = vel.copy()
+        assert L.ref_g2p_blend(d, level, ptrs(un), ptrs(uo), pos.reshape(-1), v_out.reshape(-1), n, alpha) == 0
+        x_out = pos.copy()
+        assert L.ref_advect(d, level, ptrs(un), x_out.reshape(-1), n, dt) == 0
+        k = f"c{case}_"
+        out.update({k + "dims": d, k + "level": np.uint32(level), k + "pos": pos, k + "vel": vel, k + "u_new": cn,
+                    k + "u_old": co, k + "alpha": alpha, k + "dt": dt, k + "vel_out": v_out, k + "pos_out": x_out})
+    np.savez_compressed(os.path.join(outdir, "ref_transfer.npz"), **out)
+
+
+def main(outdir, only=None):
     L = load()
     assert L.ref_device_ok(), "needs a CUDA device"
     os.makedirs(outdir, exist_ok=True)
+    if only == "transfer":
+        transfer_fixtures(L, outdir)
+        print("transfer fixtures written to", outdir)
+        return
     const = np.zeros(2, np.int32)
     L.ref_constants(const)
     R0, ML = int(const[0]), int(const[1])
@@ -191,8 +231,11 @@ def main(outdir):
     np.savez_compressed(os.path.join(outdir, "ref_normalize.npz"), dims=dims, levels=lvn,
                         **{f"mom{a}": mom[a] for a in range(3)}, **{f"mass{a}": mass[a] for a in range(3)},
                         **{f"vel{a}": vel[a] for a in range(3)})
+    transfer_fixtures(L, outdir)
     print("golden fixtures written to", outdir)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else HERE)
+    args = [a for a in sys.argv[1:] if not a.startswith("--only=")]
+    only = next((a.split("=", 1)[1] for a in sys.argv[1:] if a.startswith("--only=")), None)
+    main(args[0] if args else HERE, only)

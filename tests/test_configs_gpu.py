@@ -1,0 +1,187 @@
+"""Parity at the benchmark workloads themselves, on the GPU against the FP64 oracle.
+
+- poisson_256 (256^3 effective, 4 levels, 4.7M cells): the 32-sphere level map bit-exact, the
+  mixed-precision pressure against the oracle's PCG solve to 1e-12, and the divergence left by each
+  solver form, evaluated in FP64.
+- dam_drop2_256 (256^3 effective, 4 levels, 34.7M particles): one FLIP step, mixed to 1e-6 and plain
+  FP32 to 1e-5, against the oracle's step.
+- the differentiable rollout on the dam_break_64 layout (505,856 particles, 50 steps, checkpoints
+  every 10): the GPU VJP against the FP64 adjoint evaluated along the GPU's own trajectory, and, over
+  10 steps, against the oracle's own FP64 rollout gradient.
+
+Each oracle leg takes 10-20 s on the host cores.  Bars are written beside each assertion.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+import anitowave_adaptive_b200 as aw  # noqa: E402
+from anitowave_adaptive_b200 import scenes  # noqa: E402
+from oracle import pyoracle as po  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_l2(a, b):
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    d = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / (d if d > 0 else 1.0))
+
+
+# ------------------------------------------------------------------------------------------------
+# poisson_256
+# ------------------------------------------------------------------------------------------------
+@pytest.fixture(scope="module")
+def poisson():
+    from anitowave_adaptive_b200 import poisson as pz
+    prob = pz.build_problem(256)
+    g = prob.grid
+    c, r = scenes.poisson_spheres()
+    pts = scenes.sphere_surface_points(256, c, r)
+    lv = po.levels_from_particles(g.dims, g.block_size, g.domain_min, g.base_res, g.num_levels, pts, (8, 24, 56))
+    lv, _ = po.enforce_grading(g.dims, g.num_levels, lv)
+    O = po.Oracle(g.dims, g.block_size, g.domain_min, g.base_res, g.num_levels, lv)
+    fluid = np.ones(int(O.tot0[0]), np.uint8)
+    O.set_params(mode=0)
+    O.build(fluid=fluid)
+    b = prob.b.double().cpu().numpy()
+    p_o, hist = O.solve(b, tol=1e-12, max_cycles=60, method="pcg")
+    yield prob, lv, O, fluid, b, p_o, hist
+    g.close()
+
+
+def projected_faces(prob, solver, p):
+    """Face velocities after the pressure-gradient update with p (dt = 1), read back; the grid's
+    velocity is restored."""
+    g = prob.grid
+    saved = [g.channel(aw.VELOCITY_X + a).clone() for a in range(3)]
+    g.pressure_gradient(solver, p, prob.fluid, 1.0)
+    g.face_sync(aw.VELOCITY_X)
+    g.wall_bc(aw.VELOCITY_X)
+    u = [g.channel(aw.VELOCITY_X + a).double().cpu().numpy() for a in range(3)]
+    for a in range(3):
+        g.channel(aw.VELOCITY_X + a).copy_(saved[a])
+    torch.cuda.synchronize()
+    return u
+
+
+def test_poisson_256_level_map_bit_exact(poisson):
+    prob, lv, O, fluid, b, p_o, hist = poisson
+    assert np.array_equal(prob.grid.refinement_map(), lv)
+    assert np.array_equal(O.tot0, np.asarray(prob.grid.totals(), np.uint32))
+
+
+def test_poisson_256_pressure_and_fp64_divergence(poisson):
+    prob, lv, O, fluid, b, p_o, hist = poisson
+    assert hist[-1] < 1e-12
+    # closed box, all fluid: the pressure is defined up to a constant, compared with the mean removed
+    sv = aw.Solver(prob.grid, precision=aw.PRECISION_MIXED, tolerance=1e-10, max_cycles=60)
+    sv.setup(None)
+    p = torch.zeros(b.size, dtype=torch.float64, device="cuda")
+    cyc, rel, st = sv.solve(prob.b, p)
+    assert rel < 1e-10
+    pg = p.cpu().numpy()
+    # bar: 1e-6 relative L2 of the mean-free pressure (solved to 1e-10; W and b are FP32 on the GPU)
+    assert rel_l2(pg - pg.mean(), p_o - p_o.mean()) < 1e-6
+    # net volume flux out of every cell, evaluated in FP64 on each form's projected FP32 field
+    flux = {}
+    for name, prec, tol in (("mixed_1e-6", aw.PRECISION_MIXED, 1e-6), ("fp32", aw.PRECISION_FP32, 1e-6)):
+        s2 = aw.Solver(prob.grid, precision=prec, tolerance=tol, max_cycles=60)
+        s2.setup(None)
+        q = torch.zeros(b.size, dtype=torch.float64 if prec == aw.PRECISION_MIXED else torch.float32, device="cuda")
+        s2.solve(prob.b, q, raise_on_error=False)  # plain FP32 stalls above 1e-6 here: kept as it ends
+        u = projected_faces(prob, s2, q)
+        flux[name] = float(np.abs(O.divergence(u, fluid, 1.0)).max())
+        s2.close()
+    u_o = O.gradient_update(p_o, 1.0, [prob.grid.channel(aw.VELOCITY_X + a).double().cpu().numpy() for a in range(3)])
+    u_o = O.wall_bc(O.face_sync(u_o))
+    flux_o = float(np.abs(O.divergence(u_o, fluid, 1.0)).max())
+    flux_in = float(np.abs(b).max())
+    # the mixed form's FP64-evaluated divergence is at most 1e-4 of the initial one, and below the
+    # plain FP32 V-cycle's; the oracle's own FP64 field is the floor
+    assert flux["mixed_1e-6"] < 1e-4 * flux_in, (flux, flux_in)
+    assert flux["mixed_1e-6"] < flux["fp32"], flux
+    assert flux_o < flux["mixed_1e-6"], (flux_o, flux)
+    sv.close()
+
+
+# ------------------------------------------------------------------------------------------------
+# dam_drop2_256
+# ------------------------------------------------------------------------------------------------
+def test_dam_drop2_256_step_matches_oracle():
+    S = scenes.config("dam_drop2_256")
+    grav = (0.0, S.gravity, 0.0)
+    g = aw.build_grid(S)
+    lv = po.levels_from_particles(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, S.pos, S.thresholds)
+    lv, _ = po.enforce_grading(S.dims, S.num_levels, lv)
+    assert np.array_equal(g.refinement_map(), lv)
+    O = po.Oracle(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, lv)
+    xo, vo, perm, det = po.flip_step(O, S.pos, S.vel, S.dt, S.alpha, grav, tol=1e-12, method="pcg")
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(perm.size)
+    un_o = np.concatenate(det["u_new"])
+    for prec, tol in ((aw.PRECISION_MIXED, 1e-6), (aw.PRECISION_FP32, 1e-5)):
+        F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, grav, precision=prec, tolerance=tol, max_cycles=100)
+        F.step()
+        st = F.stats()
+        assert st["residual"] < tol
+        u = np.concatenate([g.channel(aw.VELOCITY_X + a).double().cpu().numpy() for a in range(3)])
+        p, v = F.particles()
+        # bar: 1e-5 relative L2 for the FP32 results (the mixed form lands near 3e-8, FP32 near 4e-7)
+        assert rel_l2(u, un_o) < 1e-5, prec
+        assert rel_l2(v, vo[inv]) < 1e-5, prec
+        disp = np.abs(xo[inv] - S.pos).max()
+        assert np.abs(p.astype(np.float64) - xo[inv]).max() < 1e-5 * disp + 4 * np.spacing(np.float32(1.0)), prec
+        F.close()
+    g.close()
+
+
+# ------------------------------------------------------------------------------------------------
+# differentiable rollout, dam_break_64 layout
+# ------------------------------------------------------------------------------------------------
+def _rollout(steps):
+    S = scenes.config("dam_break_64")
+    g = aw.build_grid(S)
+    O = po.Oracle(S.dims, S.block_size, S.domain_min, S.base_res, S.num_levels, g.refinement_map())
+    rng = np.random.default_rng(5)
+    target = (S.pos.astype(np.float64) + np.array([0.1, 0, 0]) + 0.01 * rng.standard_normal(S.pos.shape))
+    target = target.astype(np.float32)
+    R = aw.Rollout(g, S.pos, steps, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_MIXED, tolerance=1e-8,
+                   checkpoint_every=10)
+    u0 = torch.zeros(R.nfaces, device="cuda")
+    loss = R.forward(u0, torch.as_tensor(target, device="cuda"))
+    G = R.vjp().double().cpu().numpy()
+    R.close()
+    return S, g, O, target, loss, G
+
+
+def test_rollout_50_steps_vjp_along_gpu_trajectory():
+    S, g, O, target, loss, G = _rollout(50)
+    F = aw.Flip(g, S.pos, np.zeros_like(S.pos), S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_MIXED,
+                tolerance=1e-8)
+    xs, vs = [S.pos.astype(np.float64)], [np.zeros(S.pos.shape)]
+    for _ in range(50):
+        F.step()
+        p, v = F.particles()
+        xs.append(p.astype(np.float64))
+        vs.append(v.astype(np.float64))
+    F.close()
+    assert abs(float(((xs[-1] - target) ** 2).sum(1).mean()) - loss) < 1e-6 * loss
+    go = np.concatenate(po.grad_along_states(O, xs, vs, O._faces(), target.astype(np.float64), S.dt, S.alpha,
+                                             (0, S.gravity, 0)))
+    # bar: 1e-3 relative L2 (the adjoint requirement; measured 1.7e-5)
+    assert rel_l2(G, go) < 1e-3
+    g.close()
+
+
+def test_rollout_10_steps_vjp_matches_oracle_gradient():
+    S, g, O, target, loss, G = _rollout(10)
+    x0, tg = S.pos.astype(np.float64), target.astype(np.float64)
+    Lo, xN, recs = po.rollout64(O, x0, O._faces(), 10, S.dt, S.alpha, (0, S.gravity, 0), tg, tol=1e-12)
+    go = np.concatenate(po.rollout64_grad(O, x0, O._faces(), recs, xN, tg, S.dt, S.alpha, tol=1e-12))
+    assert abs(Lo - loss) < 1e-6 * Lo
+    # bar: 1e-3 relative L2 against the FP64 oracle's own gradient (measured 8e-7 over 10 steps; over
+    # 50 steps the FP32 and FP64 trajectories part, which the along-trajectory test covers)
+    assert rel_l2(G, go) < 1e-3
+    g.close()

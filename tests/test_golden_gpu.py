@@ -124,3 +124,39 @@ def test_reference_mode_kernels(variant):
     sv.vcycle()
     torch.cuda.synchronize()
     assert rel_l2(X.cpu().numpy(), f[key + "_x"]) < 1e-5
+
+
+def test_flip_blend_and_rk3_match_reference_kernels():
+    # aw_g2p / aw_advect against g2pUpdateKernel / advectParticlesKernel (G2P.cuh:87-173) run on a
+    # B200, on single-level maps with a velocity uniform per axis and particles two cells from the
+    # walls.  Bars: velocity 1e-5 relative L2; positions 1e-6 and the RK3 displacement 1e-4 (both
+    # sides FP32: x + dt v rounds at 6e-8 against a 5e-3 displacement).
+    f = load("ref_transfer.npz")
+    n = 0
+    i = 0
+    while f"c{i}_dims" in f:
+        k = f"c{i}_"
+        dims = tuple(int(v) for v in f[k + "dims"])
+        g = aw.MSBG(dims, 1.0, (0, 0, 0), 16, 3)
+        g.init_refinement_map(int(f[k + "level"]))
+        g.enforce_grading()
+        g.allocate()
+        for a in range(3):
+            g.channel(aw.VELOCITY_X + a).fill_(float(f[k + "u_new"][a]))
+            g.channel(aw.VELOCITY_OLD_X + a).fill_(float(f[k + "u_old"][a]))
+        pos = torch.as_tensor(f[k + "pos"], device="cuda")
+        vel = torch.as_tensor(f[k + "vel"], device="cuda")
+        g.g2p(vel, pos, float(f[k + "alpha"]))
+        torch.cuda.synchronize()
+        assert rel_l2(vel.cpu().numpy(), f[k + "vel_out"]) < 1e-5, i
+        x = pos.clone()
+        g.advect(x, float(f[k + "dt"]))
+        torch.cuda.synchronize()
+        x = x.cpu().numpy().astype(np.float64)
+        p0 = f[k + "pos"].astype(np.float64)
+        assert rel_l2(x, f[k + "pos_out"]) < 1e-6, i
+        assert rel_l2(x - p0, f[k + "pos_out"].astype(np.float64) - p0) < 1e-4, i
+        g.close()
+        n += 1
+        i += 1
+    assert n >= 2

@@ -117,6 +117,46 @@ def test_g2p_and_advect_match_oracle(case):
     check_positions(pos_t.cpu().numpy(), xr, S.pos)
 
 
+def test_dropin_g2p_advect_after_p2g_match_oracle(case):
+    # aw_g2p / aw_advect on the arrays the preceding aw_p2g sorted take the block-sorted kernels
+    # (the caller's arrays hash as they did at the sort); once the arrays change, the general path.
+    S, lv, O, g = case
+    rng = np.random.default_rng(17)
+    vel = (rng.standard_normal((S.n, 3))).astype(np.float32)
+    pos_t = torch.as_tensor(S.pos, device="cuda")
+    vel_t = torch.as_tensor(vel, device="cuda")
+    g.p2g(pos_t, vel_t)
+    un = _random_fields(O, rng)
+    uo = _random_fields(O, rng)
+    for a in range(3):
+        g.channel(aw.VELOCITY_X + a).copy_(torch.as_tensor(un[a], dtype=torch.float32))
+        g.channel(aw.VELOCITY_OLD_X + a).copy_(torch.as_tensor(uo[a], dtype=torch.float32))
+    un32 = [x.astype(np.float32).astype(np.float64) for x in un]
+    uo32 = [x.astype(np.float32).astype(np.float64) for x in uo]
+    g.g2p(vel_t, pos_t, 0.95)  # sorted path
+    v1 = vel_t.cpu().numpy()
+    assert rel_l2(v1, O.g2p(S.pos, un32, uo32, 0.95, vel)) < RTOL
+    g.g2p(vel_t, pos_t, 0.6)  # the velocities changed: general path
+    assert rel_l2(vel_t.cpu().numpy(), O.g2p(S.pos, un32, uo32, 0.6, v1)) < RTOL
+    g.p2g(pos_t, vel_t)
+    for a in range(3):
+        g.channel(aw.VELOCITY_X + a).copy_(torch.as_tensor(un[a], dtype=torch.float32))
+    dt = S.dt * 0.05
+    xr = O.advect(un32, dt, S.pos.astype(np.float64))
+    g.advect(pos_t, dt)  # sorted path
+    check_positions(pos_t.cpu().numpy(), xr, S.pos)
+    # a position moved in place after the sort: the general path, still exact
+    g.p2g(pos_t, vel_t)
+    for a in range(3):
+        g.channel(aw.VELOCITY_X + a).copy_(torch.as_tensor(un[a], dtype=torch.float32))
+    x1 = pos_t.cpu().numpy().astype(np.float64)
+    pos_t[0, 0] += 1e-3
+    x1[0, 0] = float(pos_t[0, 0])
+    v2 = vel_t.cpu().numpy()
+    g.g2p(vel_t, pos_t, 0.95)
+    assert rel_l2(vel_t.cpu().numpy(), O.g2p(x1.astype(np.float32), un32, uo32, 0.95, v2)) < RTOL
+
+
 def check_positions(x_gpu, x_ref, x0):
     """Positions are FP32: compare per particle with a bound of 1e-5 of the displacement plus the
     rounding of an FP32 position (4 ulps of the domain extent 1.0)."""
@@ -179,7 +219,7 @@ def test_fv_residual_smoother_vcycle_match_oracle(case):
     assert rel_l2(X.cpu().numpy(), O.get(0, 0)) < RTOL
 
 
-@pytest.mark.parametrize("precision", [aw.PRECISION_FP32, aw.PRECISION_MIXED])
+@pytest.mark.parametrize("precision", [aw.PRECISION_FP32, aw.PRECISION_MIXED, aw.PRECISION_FP32_PCG])
 def test_fv_solve_reaches_tolerance(case, precision):
     S, lv, O, g = case
     x, v, perm, d = po.flip_step(O, S.pos, S.vel, S.dt, 0.95, (0, S.gravity, 0), tol=1e-12)
@@ -187,10 +227,11 @@ def test_fv_solve_reaches_tolerance(case, precision):
     b = d["b"].astype(np.float32)
     # plain FP32 stalls near 5e-6 on these problems: the rounding of an FP32 pressure alone
     # leaves a relative residual of that order; the mixed form carries the pressure in FP64
-    tol = 2e-5 if precision == aw.PRECISION_FP32 else 1e-9
+    # FP32 conjugate gradients carry the same FP32 rounding floor as the plain FP32 iteration
+    tol = 1e-9 if precision == aw.PRECISION_MIXED else 2e-5
     sv = _fv_solver_pair(S, O, g, fluid, precision=precision, tolerance=tol, max_cycles=60)
     bt = torch.as_tensor(b, device="cuda")
-    pt = torch.zeros(b.shape[0], dtype=torch.float32 if precision == aw.PRECISION_FP32 else torch.float64,
+    pt = torch.zeros(b.shape[0], dtype=torch.float64 if precision == aw.PRECISION_MIXED else torch.float32,
                      device="cuda")
     cyc, rel, st = sv.solve(bt, pt)
     assert rel < tol
@@ -199,7 +240,7 @@ def test_fv_solve_reaches_tolerance(case, precision):
     r = b.astype(np.float64) - O.apply(0, p)
     # under the FP64 oracle operator (FP64 conductances): FP32 storage of W and b bounds the mixed
     # result near 1e-8
-    assert np.linalg.norm(r * fluid) / np.linalg.norm(b * fluid) < (5e-5 if precision == aw.PRECISION_FP32 else 1e-7)
+    assert np.linalg.norm(r * fluid) / np.linalg.norm(b * fluid) < (1e-7 if precision == aw.PRECISION_MIXED else 5e-5)
 
 
 def swirl(pos):
