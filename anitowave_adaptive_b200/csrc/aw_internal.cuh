@@ -287,6 +287,8 @@ aw_status advect_launch(MsbgState& G, float* pos, int pos_soa, int64_t n, float 
 // (written here), tn and to at least the grid's total tile size in floats each.
 aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t n, float alpha, uint32_t* toff,
                          float* tn, float* to, cudaStream_t s);
+// loads g2p_with_tiles' kernels on the current device ahead of their first launch
+aw_status preload_g2p_with_tiles();
 // total tile floats of a grid whose blocks have resolutions h_res (one velocity field)
 uint64_t tile_total(const std::vector<int>& h_res);
 aw_status build_tiles2(MsbgState& G, const float* un[3], const float* uo[3], cudaStream_t s);

@@ -18,9 +18,11 @@
 // same call, in stream order.  Calls that overlap on the GPU (on different streams, or from several
 // host threads without ordering) race on the array and give undefined results.
 //
-// The first call on a device looks up the array's device address (cudaGetSymbolAddress, which
-// loads this module on that device) with that device current; it should come before any stream
-// capture on that device.
+// The first call on a device, with that device current, looks up the array's device address
+// (cudaGetSymbolAddress, which loads this module on that device) and loads the three kernels the
+// call launches; it does so even when it has no particles to transfer.  After it, a call neither
+// loads code nor takes device memory.  That first call should come before any stream capture on the
+// device.
 
 #include <mutex>
 
@@ -51,6 +53,9 @@ aw_status scratch_on_current_device(uint32_t** out) {
         if (e != cudaSuccess || !p)
             return aw::set_error(AW_ERR_CUDA, "cudaGetSymbolAddress of the G2P scratch array failed on device %d: %s",
                                  dev, cudaGetErrorString(e));
+        // CUDA loads kernels at their first launch unless asked earlier: load them now, so that no
+        // later call loads code or takes device memory
+        AW_TRY(aw::preload_g2p_with_tiles());
         g_scratch_dev[dev] = (uint32_t*)p;
     }
     *out = g_scratch_dev[dev];

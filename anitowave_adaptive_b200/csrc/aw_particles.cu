@@ -1585,6 +1585,16 @@ aw_status g2p_with_tiles(MsbgState& G, float* d_vel, const float* d_pos, int64_t
     return AW_OK;
 }
 
+// Loads the kernels g2p_with_tiles launches on the current device (CUDA loads kernels lazily, at
+// their first launch), so that the first launch neither loads code nor takes device memory.
+aw_status preload_g2p_with_tiles() {
+    cudaFuncAttributes fa;
+    AW_CUDA(cudaFuncGetAttributes(&fa, k_tile_offsets));
+    AW_CUDA(cudaFuncGetAttributes(&fa, k_build_tiles));
+    AW_CUDA(cudaFuncGetAttributes(&fa, k_g2p_tiles));
+    return AW_OK;
+}
+
 // ================================================================================================
 // Adjoint (vector-Jacobian products) of P2G, G2P, RK3 advection and MAC sampling.  No counterpart
 // in the reference.  The forward map is differentiated with its discrete decisions held: the cell

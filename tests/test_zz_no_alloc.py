@@ -30,6 +30,12 @@ def g2p_noalloc(g, vel, pos, alpha):
                                    C.c_int64(pos.shape[0]), C.c_float(alpha), stream)
 
 
+def _fresh_fields(g, rng):
+    for a in range(3):
+        for ch in (aw.VELOCITY_X + a, aw.VELOCITY_OLD_X + a):
+            g.channel(ch).copy_(torch.as_tensor(rng.standard_normal(g.channel(ch).numel()), dtype=torch.float32))
+
+
 def test_g2p_noalloc_matches_g2p_on_two_calls():
     S = scenes.config("dam_break_64")
     g = aw.build_grid(S)
@@ -37,21 +43,37 @@ def test_g2p_noalloc_matches_g2p_on_two_calls():
     pos = torch.as_tensor(S.pos, device="cuda")
     for call, alpha in enumerate((0.95, 0.6)):
         # fresh fields and velocities on each call, so the second call cannot pass on what the
-        # first one left in the shared scratch array
-        for a in range(3):
-            g.channel(aw.VELOCITY_X + a).copy_(torch.as_tensor(rng.standard_normal(g.channel(aw.VELOCITY_X + a).numel()),
-                                                               dtype=torch.float32))
-            g.channel(aw.VELOCITY_OLD_X + a).copy_(
-                torch.as_tensor(rng.standard_normal(g.channel(aw.VELOCITY_OLD_X + a).numel()), dtype=torch.float32))
+        # first one left in the shared scratch array; the allocation-free call runs first, on a grid
+        # whose own G2P buffers aw_g2p has not allocated yet
+        _fresh_fields(g, rng)
         vel0 = torch.as_tensor(rng.standard_normal((S.n, 3)).astype(np.float32), device="cuda")
         ref = vel0.clone()
         got = vel0.clone()
-        g.g2p(ref, pos, alpha)
         st = g2p_noalloc(g, got, pos, alpha)
         assert st == aw.AW_OK, aw.lib().aw_last_error().decode()
+        g.g2p(ref, pos, alpha)
         torch.cuda.synchronize()
         err = rel_l2(got.cpu().numpy(), ref.cpu().numpy())
         assert err < RTOL, (call, err)
+
+
+def test_g2p_noalloc_takes_no_device_memory():
+    # after a first call has set the device up, a call on a new grid leaves the free device memory
+    # exactly as it was
+    S = scenes.config("dam_break_32")
+    g0 = aw.build_grid(S)
+    pos = torch.as_tensor(S.pos, device="cuda")
+    vel = torch.zeros((S.n, 3), device="cuda")
+    assert g2p_noalloc(g0, vel, pos, 0.95) == aw.AW_OK
+    g = aw.build_grid(S)
+    _fresh_fields(g, np.random.default_rng(3))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    st = g2p_noalloc(g, vel, pos, 0.95)
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert st == aw.AW_OK, aw.lib().aw_last_error().decode()
+    assert free1 == free0, (free0, free1)
 
 
 def test_g2p_noalloc_rejects_grid_beyond_its_scratch():
