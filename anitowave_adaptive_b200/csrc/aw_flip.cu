@@ -879,15 +879,11 @@ extern "C" aw_status aw_flip_rebuild_levels(aw_flip* F, const int32_t* h_thresho
     cudaStream_t s = (cudaStream_t)s_;
     MsbgState& G = F->g->st;
     if (changed) *changed = 0;
-    const std::vector<uint32_t> old = G.h_level;
     const float* soa = F->soa[F->cur].p;
-    AW_TRY(levels_from_positions(G, soa, 1, F->n, F->n, h_thresholds, s));
-    int32_t passes = 0;
-    AW_TRY(aw_msbg_enforce_grading(F->g, &passes, s_));
-    std::vector<uint32_t> now((size_t)G.nb);
-    AW_CUDA(cudaMemcpyAsync(now.data(), G.level.p, G.nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-    AW_CUDA(cudaStreamSynchronize(s));
-    if (now == old) {  // same layout: keep the channels and the solver
+    // map, grading and comparison on the device; the host reads one count
+    int ndiff = 0;
+    AW_TRY(relevel_on_device(G, soa, 1, F->n, F->n, h_thresholds, &ndiff, nullptr, s));
+    if (ndiff == 0) {  // same layout: keep the channels and the solver
         G.allocated = true;
         return AW_OK;
     }

@@ -238,6 +238,76 @@ __global__ void k_grading(Geo g, const uint32_t* __restrict__ in, uint32_t* __re
     if (best != l) *changed = 1;
 }
 
+// enforceGrading's rule (MSBG.cuh:316-351) to its fixpoint in one CTA, in place, then the number of
+// blocks whose level differs from `prev`.  Levels only decrease under the rule, so visiting the
+// blocks in any order reaches the same fixpoint as the Jacobi passes of aw_msbg_enforce_grading;
+// one launch replaces a host round trip per pass.  out[0] = changed blocks, out[1] = passes
+// (-1 when max_passes did not reach the fixpoint).
+__global__ void __launch_bounds__(1024) k_grading_fixpoint(Geo g, uint32_t* level, const uint32_t* __restrict__ prev,
+                                                           int max_passes, int* out) {
+    __shared__ int changed, ndiff;
+    int pass = 0;
+    for (;;) {
+        if (threadIdx.x == 0) changed = 0;
+        __syncthreads();
+        for (int b = threadIdx.x; b < g.nb; b += blockDim.x) {
+            const uint32_t l = level[b];
+            if ((int)l == g.L) continue;
+            uint32_t best = l;
+            int cb[3];
+            bcoord(g, b, cb);
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        if (!dx && !dy && !dz) continue;
+                        int nc[3] = {cb[0] + dx, cb[1] + dy, cb[2] + dz};
+                        if (!inside(g, nc)) continue;
+                        const uint32_t nl = ((volatile const uint32_t*)level)[bidx(g, nc[0], nc[1], nc[2])];
+                        if ((int)nl == g.L) continue;
+                        if ((int)l - (int)nl > 1) best = min(best, nl + 1u);
+                    }
+            if (best != l) {
+                level[b] = best;
+                changed = 1;
+            }
+        }
+        __syncthreads();
+        ++pass;
+        const int c = changed;
+        __syncthreads();
+        if (!c || pass > max_passes) break;
+    }
+    if (threadIdx.x == 0) ndiff = 0;
+    __syncthreads();
+    int d = 0;
+    for (int b = threadIdx.x; b < g.nb; b += blockDim.x) d += level[b] != prev[b];
+    if (d) atomicAdd(&ndiff, d);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        out[0] = ndiff;
+        out[1] = changed ? -1 : pass;
+    }
+}
+
+// The level map of the current particles, graded, compared with the map in use on the device: one
+// 8-byte read-back.  *changed = blocks whose level differs.
+aw_status relevel_on_device(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
+                            const int32_t* thresholds, int* changed, int* passes, cudaStream_t s) {
+    AW_TRY(G.level_prev.ensure((size_t)G.nb));
+    AW_CUDA(cudaMemcpyAsync(G.level_prev.p, G.level.p, G.nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+    AW_TRY(levels_from_positions(G, d_pos, si, sa, n, thresholds, s));
+    AW_TRY(G.flag.ensure(2));
+    k_grading_fixpoint<<<1, 1024, 0, s>>>(G.geo, G.level.p, G.level_prev.p, 4 * G.geo.L + 8, G.flag.p);
+    AW_LAUNCH();
+    int h[2];
+    AW_CUDA(cudaMemcpyAsync(h, G.flag.p, sizeof h, cudaMemcpyDeviceToHost, s));
+    AW_CUDA(cudaStreamSynchronize(s));
+    if (h[1] < 0) return set_error(AW_ERR_STATE, "grading did not reach a fixpoint in %d passes", 4 * G.geo.L + 8);
+    *changed = h[0];
+    if (passes) *passes = h[1];
+    return AW_OK;
+}
+
 // countBlockElements (MSBG.cuh:353-376) at MG level m; vanish: res < 1 -> 0 (reference),
 // else clamp to 1.  Also writes the per-block res.
 __global__ void k_count(Geo g, const uint32_t* __restrict__ level, int m, int vanish, uint32_t* cnt, int* res) {

@@ -207,6 +207,7 @@ struct MsbgState {
     Geo geo;
     int nb = 0;
     DBuf<uint32_t> level;       // refinement map
+    DBuf<uint32_t> level_prev;  // the map before a re-derivation (aw_flip_rebuild_levels)
     DBuf<int> res;              // native res per block (0 inactive), after allocate
     DBuf<uint32_t> off[4];      // level-0 offsets
     bool allocated = false;
@@ -247,6 +248,12 @@ struct MsbgState {
 // grid unallocated.
 aw_status levels_from_positions(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
                                 const int32_t* thresholds, cudaStream_t s);
+
+// Re-derives the level map from particle positions and grades it on the device; *changed receives
+// the number of blocks whose level differs from the map before (one small read-back, no per-pass
+// host synchronisation).  Marks the grid unallocated.
+aw_status relevel_on_device(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
+                            const int32_t* thresholds, int* changed, int* passes, cudaStream_t s);
 
 // Exclusive scan of n u32 values into out[0..n] (out[n] = total).  tmp: scan scratch.
 aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<uint32_t>& tmp, cudaStream_t s);

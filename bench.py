@@ -308,6 +308,9 @@ def run_ours(args, ws, rank, local):
     two_phase = None
     if not args.skip_two_phase:
         two_phase = two_phase_bench()
+    rebuild = None
+    if not args.skip_rebuild:
+        rebuild = rebuild_bench()
     # clocks sampled from the first timed FLIP step through the last timed region of this run
     clocks = clk.stop() if clk else None
 
@@ -349,6 +352,8 @@ def run_ours(args, ws, rank, local):
         line["flip_256"] = flip256
     if two_phase is not None:
         line["two_phase_128"] = two_phase
+    if rebuild is not None:
+        line["rebuild_128"] = rebuild
     if resample is not None:
         line["resample_256"] = resample
     print(json.dumps(line), flush=True)
@@ -507,6 +512,34 @@ def resample_bench(g, aw, dims=(256, 256, 256), reps=10, warmup=3):
     return out
 
 
+def rebuild_bench(steps=20, warmup=3):
+    """dam_drop_128 with the level map re-derived from the particles after every FLIP step
+    (aw_flip_rebuild_levels): host wall time of the rebuild when the map is unchanged (map, grading
+    and comparison on the device, one read-back) and when it changed (new layout and solver)."""
+    import torch
+    import anitowave_adaptive_b200 as aw
+    from anitowave_adaptive_b200 import scenes
+    S = scenes.config(WORKLOAD)
+    g = aw.build_grid(S)
+    F = aw.Flip(g, S.pos, S.vel, S.dt, S.alpha, (0, S.gravity, 0), precision=aw.PRECISION_MIXED, tolerance=1e-6,
+                max_cycles=100)
+    for _ in range(warmup):
+        F.step()
+    same, new = [], []
+    for _ in range(steps):
+        F.step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        changed = F.rebuild_levels(S.thresholds)
+        dt = 1e3 * (time.perf_counter() - t0)
+        (new if changed else same).append(dt)
+    F.close()
+    g.close()
+    return {"workload": WORKLOAD, "steps": steps, "layout_changes": len(new),
+            "ms_unchanged": float(np.median(same)) if same else None,
+            "ms_changed": float(np.median(new)) if new else None}
+
+
 def two_phase_bench(steps=10, warmup=3, rho=(1.0, 3.0)):
     """dam_drop_128 with the falling sphere as a second, heavier liquid (rho 3 vs 1): FLIP steps with
     beta = 1/rho from the P2G phase field (coefficients rebuilt every step), beside the one-phase step
@@ -555,6 +588,7 @@ def main():
     ap.add_argument("--skip-flip256", action="store_true", help="skip the dam_drop2_256 FLIP steps/s section")
     ap.add_argument("--skip-two-phase", action="store_true", help="skip the two-phase dam_drop_128 section")
     ap.add_argument("--skip-resample", action="store_true", help="skip the 256^3 resampling section")
+    ap.add_argument("--skip-rebuild", action="store_true", help="skip the level-map rebuild section")
     ap.add_argument("--poisson-only", action="store_true",
                     help="only the poisson_256 projection comparison (for profiling the solver)")
     ap.add_argument("--poisson-solve-once", action="store_true",

@@ -290,12 +290,14 @@ aw_status aw_flip_stats_get(aw_flip* f, aw_flip_stats* out);
 aw_status aw_flip_particles(aw_flip* f, float* h_pos, float* h_vel);
 aw_status aw_flip_solver(aw_flip* f, aw_solver** out);
 /* Between steps: rebuild the level map from the simulation's current particle positions (the rule
- * of aw_msbg_levels_from_particles with these thresholds, then aw_msbg_enforce_grading).  When the
- * map changed, the grid is laid out again (aw_msbg_allocate) and the solver hierarchy rebuilt;
- * channel pointers and solver handles obtained before are then stale.  No grid state needs
- * remapping: P2G regenerates it from the particles every step.  *changed (optional) = 1 when the
- * layout changed.  syncs.  No counterpart in the reference (markActiveBlocks + grading +
- * allocateChannels were a one-time setup there, main.cu:154-278). */
+ * of aw_msbg_levels_from_particles with these thresholds, graded to the same fixpoint as
+ * aw_msbg_enforce_grading).  The map, its grading and the comparison with the map in use run on the
+ * device; the host reads back one count.  When the map is unchanged nothing else happens.  When it
+ * changed, the grid is laid out again (aw_msbg_allocate) and the solver hierarchy rebuilt; channel
+ * pointers and solver handles obtained before are then stale.  No grid state needs remapping: P2G
+ * regenerates it from the particles every step.  *changed (optional) = 1 when the layout changed.
+ * syncs.  No counterpart in the reference (markActiveBlocks + grading + allocateChannels were a
+ * one-time setup there, main.cu:154-278). */
 aw_status aw_flip_rebuild_levels(aw_flip* f, const int32_t* h_thresholds, int32_t* changed, aw_stream s);
 /* Two-phase simulation: h_phase[i] in [0,1] is the phase of particle i (original order) and rho0,
  * rho1 > 0 the densities of phase 0 and 1.  Every later step runs aw_p2g_phase's deposit, rebuilds
