@@ -182,7 +182,8 @@ struct ParticleWork {
     int64_t n = 0;
     // The particle arrays the last aw_p2g sorted (caller pointers and count) and 64-bit hashes of
     // their contents then: hash[0] positions, hash[1] velocities; hash[2..3] receive the hashes of
-    // the arrays at a later drop-in G2P or advection, which reuses this sort when they match.
+    // the arrays at a later drop-in G2P or advection, which reuses this sort when they match;
+    // hash[4..] holds the partial sums of the hashing kernels.
     const float* src_pos = nullptr;
     const float* src_vel = nullptr;
     int64_t src_n = -1;

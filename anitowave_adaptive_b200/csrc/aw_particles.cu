@@ -167,9 +167,48 @@ __device__ inline unsigned long long warp_sum_u64(unsigned long long v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
+// Hash partial sums land in kHashSlots slot pairs (CTA b in slot b mod kHashSlots), so that the
+// atomics of many CTAs do not queue on one address; k_hash_fold then sums the slots.
+constexpr int kHashSlots = 128;
+__device__ inline void hash_block_add(unsigned long long hp, unsigned long long hv, unsigned long long* slots) {
+    __shared__ unsigned long long red[2][32];
+    hp = warp_sum_u64(hp);
+    hv = warp_sum_u64(hv);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    if (lane == 0) {
+        red[0][w] = hp;
+        red[1][w] = hv;
+    }
+    __syncthreads();
+    if (w == 0) {
+        hp = lane < nw ? red[0][lane] : 0ull;
+        hv = lane < nw ? red[1][lane] : 0ull;
+        hp = warp_sum_u64(hp);
+        hv = warp_sum_u64(hv);
+        if (lane == 0) {
+            unsigned long long* d = slots + 2 * (blockIdx.x % kHashSlots);
+            atomicAdd(d, hp);
+            atomicAdd(d + 1, hv);
+        }
+    }
+}
+// out[0], out[1] = sums of the slot pairs
+__global__ void k_hash_fold(const unsigned long long* __restrict__ slots, unsigned long long* out) {
+    unsigned long long hp = 0, hv = 0;
+    for (int i = threadIdx.x; i < kHashSlots; i += 32) {
+        hp += slots[2 * i];
+        hv += slots[2 * i + 1];
+    }
+    hp = warp_sum_u64(hp);
+    hv = warp_sum_u64(hv);
+    if (threadIdx.x == 0) {
+        out[0] = hp;
+        out[1] = hv;
+    }
+}
 
 // gather pos/vel into SoA sorted order, carry the original ids; with hash, add the content hashes
-// of the input positions (hash[0]) and velocities (hash[1])
+// of the input positions and velocities into the slot pairs of `hash` (kHashSlots pairs)
 __global__ void k_gather(const uint32_t* __restrict__ src, int64_t n, PArr pos, PArr vel, float* __restrict__ soa,
                          const uint32_t* __restrict__ ids_in, uint32_t* __restrict__ ids_out,
                          const uint32_t* __restrict__ keys, uint32_t* __restrict__ keys_sorted,
@@ -193,30 +232,18 @@ __global__ void k_gather(const uint32_t* __restrict__ src, int64_t n, PArr pos, 
         if (ids_out) ids_out[j] = ids_in ? ids_in[i] : i;
         if (keys_sorted) keys_sorted[j] = keys[i];
     }
-    if (hash) {  // uniform across the CTA
-        hp = warp_sum_u64(hp);
-        hv = warp_sum_u64(hv);
-        if ((threadIdx.x & 31) == 0) {
-            atomicAdd(hash, hp);
-            atomicAdd(hash + 1, hv);
-        }
-    }
+    if (hash) hash_block_add(hp, hv, hash);  // uniform across the CTA
 }
 
-// content hashes of AoS positions (out[0]) and, when given, velocities (out[1]); out must start at 0
+// content hashes of AoS positions and, when given, velocities into the slot pairs (must start at 0)
 __global__ void k_hash_aos(const float* __restrict__ pos, const float* __restrict__ vel, int64_t n,
-                           unsigned long long* out) {
+                           unsigned long long* slots) {
     unsigned long long hp = 0, hv = 0;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         hp += hash3((uint32_t)i, pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
         if (vel) hv += hash3((uint32_t)i, vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
     }
-    hp = warp_sum_u64(hp);
-    hv = warp_sum_u64(hv);
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(out, hp);
-        if (vel) atomicAdd(out + 1, hv);
-    }
+    hash_block_add(hp, hv, slots);
 }
 
 // the caller's arrays still hold what the last aw_p2g sorted (positions; velocities too if asked)
@@ -268,12 +295,16 @@ aw_status sort_particles_soa(MsbgState& G, const float* pos_aos, const float* ve
     ParticleWork& W = G.pw;
     unsigned long long* hash = nullptr;
     if (record) {
-        AW_TRY(W.hash.ensure(4));
-        AW_CUDA(cudaMemsetAsync(W.hash.p, 0, 2 * sizeof(unsigned long long), s));
-        hash = W.hash.p;
+        AW_TRY(W.hash.ensure(4 + 2 * kHashSlots));
+        AW_CUDA(cudaMemsetAsync(W.hash.p + 4, 0, 2 * kHashSlots * sizeof(unsigned long long), s));
+        hash = W.hash.p + 4;
     }
     if (n > 0) {
         k_gather<<<nblk(n), 256, 0, s>>>(W.sorted, n, pos, vel, W.soa.p, nullptr, nullptr, nullptr, nullptr, hash);
+        AW_LAUNCH();
+    }
+    if (record) {
+        k_hash_fold<<<1, 32, 0, s>>>(W.hash.p + 4, W.hash.p);
         AW_LAUNCH();
     }
     if (record) {
@@ -2040,8 +2071,10 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
     AW_TRY(ensure_tiles(G));
     const unsigned long long* skip = nullptr;
     if (W.src_valid && W.src_pos == d_pos && W.src_vel == d_vel && W.src_n == n) {
-        AW_CUDA(cudaMemsetAsync(W.hash.p + 2, 0, 2 * sizeof(unsigned long long), s));
-        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, d_vel, n, W.hash.p + 2);
+        AW_CUDA(cudaMemsetAsync(W.hash.p + 4, 0, 2 * kHashSlots * sizeof(unsigned long long), s));
+        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, d_vel, n, W.hash.p + 4);
+        AW_LAUNCH();
+        k_hash_fold<<<1, 32, 0, s>>>(W.hash.p + 4, W.hash.p + 2);
         AW_LAUNCH();
         int maxres = 0;
         for (int r : G.h_res) maxres = std::max(maxres, r);
@@ -2076,8 +2109,10 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
     AW_TRY(build_tiles(G, u, G.tiles_new.p, s));  // both paths sample neighbouring blocks' u_new tiles
     const unsigned long long* skip = nullptr;
     if (W.src_valid && W.src_pos == d_pos && W.src_n == n) {
-        AW_CUDA(cudaMemsetAsync(W.hash.p + 2, 0, 2 * sizeof(unsigned long long), s));
-        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, nullptr, n, W.hash.p + 2);
+        AW_CUDA(cudaMemsetAsync(W.hash.p + 4, 0, 2 * kHashSlots * sizeof(unsigned long long), s));
+        k_hash_aos<<<4 * 148, 256, 0, s>>>(d_pos, nullptr, n, W.hash.p + 4);
+        AW_LAUNCH();
+        k_hash_fold<<<1, 32, 0, s>>>(W.hash.p + 4, W.hash.p + 2);
         AW_LAUNCH();
         int maxres = 0;
         for (int r : G.h_res) maxres = std::max(maxres, r);

@@ -76,13 +76,13 @@ def test_poisson_256_pressure_and_fp64_divergence(poisson):
     prob, lv, O, fluid, b, p_o, hist = poisson
     assert hist[-1] < 1e-12
     # closed box, all fluid: the pressure is defined up to a constant, compared with the mean removed
-    sv = aw.Solver(prob.grid, precision=aw.PRECISION_MIXED, tolerance=1e-10, max_cycles=60)
+    sv = aw.Solver(prob.grid, precision=aw.PRECISION_MIXED, tolerance=1e-9, max_cycles=60)
     sv.setup(None)
     p = torch.zeros(b.size, dtype=torch.float64, device="cuda")
     cyc, rel, st = sv.solve(prob.b, p)
-    assert rel < 1e-10
+    assert rel < 1e-9
     pg = p.cpu().numpy()
-    # bar: 1e-6 relative L2 of the mean-free pressure (solved to 1e-10; W and b are FP32 on the GPU)
+    # bar: 1e-6 relative L2 of the mean-free pressure (solved to 1e-9; W and b are FP32 on the GPU)
     assert rel_l2(pg - pg.mean(), p_o - p_o.mean()) < 1e-6
     # net volume flux out of every cell, evaluated in FP64 on each form's projected FP32 field
     flux = {}
