@@ -409,6 +409,7 @@ constexpr int P2G_XQ = 96;  // per-warp queue of cross-resolution pairs: < 32 wa
 constexpr int P2G_SLICE = 16;  // particles of one cell per register-accumulation task
 constexpr int P2G_MAX_SLICES = 1 << 19;  // 6 * 8^3 * this stays below 2^31
 constexpr int P2G_MAX_CELLS = 16 * 16 * 16;  // cells of the largest block (base resolution <= 16)
+constexpr int P2G_NEAR_CELLS = 8 * 8 * 8;    // blocks up to this size list their near cells
 
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
@@ -438,7 +439,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __shared__ uint32_t maxcnt;
     __shared__ int ccount[P2G_MAX_CELLS / 32];
     __shared__ uint16_t clist[P2G_MAX_CELLS];
-    __shared__ int nonempty;
+    __shared__ int nonempty, nnear;
+    // near-cell list of the cross-resolution pass (blocks of at most P2G_NEAR_CELLS cells)
+    __shared__ uint16_t nl_cell[P2G_NEAR_CELLS];
+    __shared__ uint32_t nl_mask[P2G_NEAR_CELLS], nl_pre[P2G_NEAR_CELLS + 1];
+    __shared__ uint32_t nmask_tmp[P2G_NEAR_CELLS];
+    __shared__ int ncnt_tmp[P2G_NEAR_CELLS];
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
@@ -656,15 +662,109 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
     // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
     // at a time, one pair per lane, instead of one divergent pass per neighbour direction.
-    const uint32_t T = p1 - p0;
+    // Blocks of up to 8^3 cells visit only the particles of cells near a side that faces a
+    // neighbour at another resolution, and test only those directions.  A cell qualifies for
+    // direction d when, on every axis d crosses, it lies within reach + 1 cells of that side
+    // (reach: two of b's cells towards a coarser neighbour, one towards a finer; the extra cell
+    // covers the rounding between a particle's key cell and its position in cell units).
     const int w = wid, nw = nwarp;
+    const bool listed = nc3 <= P2G_NEAR_CELLS;
+    if (xmask && listed) {
+        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
+            const int k = ch * 32 + lane;
+            uint32_t cm = 0;
+            int cnt = 0;
+            if (k < ncell) {
+                const int c = clist[k];
+                const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
+                for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
+                    const int d = __ffs(mm) - 1;
+                    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+                    const int reach = nres[d] < r ? 2 : 1;
+                    bool nr = true;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        nr = nr && (dd[a] == 0 || (dd[a] < 0 ? cc[a] <= reach : cc[a] >= r - 1 - reach));
+                    if (nr) cm |= 1u << d;
+                }
+                if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (lane == 0) ccount[ch] = __popc(bal);
+            // stash this lane's result in the slot the final list will give it: first the chunk counts
+            nmask_tmp[k < P2G_NEAR_CELLS ? k : 0] = k < ncell ? cm : 0u;
+            ncnt_tmp[k < P2G_NEAR_CELLS ? k : 0] = cnt;
+        }
+        __syncthreads();
+        if (wid == 0) {  // exclusive scan of the per-chunk counts of near cells
+            int carry = 0;
+            const int nch = (ncell + 31) / 32;
+            for (int base = 0; base < nch; base += 32) {
+                const int ch = base + lane;
+                const int v = ch < nch ? ccount[ch] : 0;
+                int incl = v;
+#pragma unroll
+                for (int sh = 1; sh < 32; sh <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                    if (lane >= sh) incl += y;
+                }
+                if (ch < nch) ccount[ch] = carry + incl - v;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) nnear = carry;
+        }
+        __syncthreads();
+        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
+            const int k = ch * 32 + lane;
+            const uint32_t cm = k < ncell ? nmask_tmp[k] : 0u;
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (cm) {
+                const int at = ccount[ch] + __popc(bal & ((1u << lane) - 1u));
+                nl_cell[at] = clist[k];
+                nl_mask[at] = cm;
+                nl_pre[at + 1] = ncnt_tmp[k];
+            }
+        }
+        __syncthreads();
+        if (wid == 0) {  // inclusive scan of the near cells' particle counts -> nl_pre[0..nnear]
+            int carry = 0;
+            const int nn = nnear;
+            for (int base = 0; base < nn; base += 32) {
+                const int k = base + lane;
+                const int v = k < nn ? (int)nl_pre[k + 1] : 0;
+                int incl = v;
+#pragma unroll
+                for (int sh = 1; sh < 32; sh <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                    if (lane >= sh) incl += y;
+                }
+                if (k < nn) nl_pre[k + 1] = (uint32_t)(carry + incl);
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) nl_pre[0] = 0;
+        }
+        __syncthreads();
+    }
+    const int nn = listed ? nnear : 0;
+    const uint32_t T = listed ? (xmask ? nl_pre[nn] : 0u) : p1 - p0;
     const uint32_t Ls = (T + 31) / 32;
     uint32_t* qv = xq_v + w * P2G_XQ;
     uint8_t* qd = xq_d + w * P2G_XQ;
     int qn = 0;
     for (uint32_t i = w; xmask && i < Ls; i += nw) {
-        const uint32_t v = lane * Ls + i;
-        const bool valid = v < T;
+        const uint32_t f = lane * Ls + i;
+        const bool valid = f < T;
+        uint32_t v = f, dirs = (uint32_t)xmask;
+        if (valid && listed) {  // near cell k holding flat index f: nl_pre[k] <= f < nl_pre[k + 1]
+            int lo = 0, hi = nn - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (nl_pre[mid] <= f) lo = mid;
+                else hi = mid - 1;
+            }
+            v = cs[c0 + nl_cell[lo]] - p0 + (f - nl_pre[lo]);
+            dirs = nl_mask[lo];
+        }
         float q[3];
         if (valid) {
             const uint32_t sidx = p0 + v;
@@ -674,7 +774,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
         uint32_t near = 0;
         if (valid) {
-            for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
+            for (uint32_t mm = dirs; mm; mm &= mm - 1) {
                 const int d = __ffs(mm) - 1;
                 const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
                 const float reach = nres[d] < r ? 2.f : 1.f;
@@ -904,6 +1004,38 @@ __device__ inline uint32_t face_source(const LevelView& L, int a, int b, const i
     q[t1] = min(max((rel1 * rn) >> sh, 0), rn - 1);
     q[t2] = min(max((rel2 * rn) >> sh, 0), rn - 1);
     return L.off[1 + a][n] + fidx(a, q[0], q[1], q[2], rn);
+}
+
+// face_source with the 27-neighbourhood (index (dx+1) + 3 (dy+1) + 9 (dz+1), 13 = the block
+// itself) already in shared memory: resolution (0 = outside or inactive) and face offsets per axis
+struct NbFaces {
+    int r;
+    uint32_t off[3];
+};
+__device__ inline uint32_t face_source_nb(const NbFaces* nbr, int a, int r, const int fi[3]) {
+    const int t1 = a == 0 ? 1 : 0, t2 = a == 2 ? 1 : 2;
+    const int o1 = fi[t1] < 0 ? -1 : (fi[t1] >= r ? 1 : 0);
+    const int o2 = fi[t2] < 0 ? -1 : (fi[t2] >= r ? 1 : 0);
+    if (!o1 && !o2) return nbr[13].off[a] + fidx(a, fi[0], fi[1], fi[2], r);
+    int dd[3] = {0, 0, 0};
+    dd[t1] = o1;
+    dd[t2] = o2;
+    const NbFaces& N = nbr[(dd[0] + 1) + 3 * (dd[1] + 1) + 9 * (dd[2] + 1)];
+    const int rn = N.r;
+    if (!rn) {
+        int q[3] = {fi[0], fi[1], fi[2]};
+        q[t1] = min(max(q[t1], 0), r - 1);
+        q[t2] = min(max(q[t2], 0), r - 1);
+        return nbr[13].off[a] + fidx(a, q[0], q[1], q[2], r);
+    }
+    const int sh = __ffs(2 * r) - 1;
+    int q[3];
+    q[a] = (2 * fi[a] * rn + r) >> sh;
+    const int rel1 = 2 * fi[t1] + 1 - o1 * 2 * r;
+    const int rel2 = 2 * fi[t2] + 1 - o2 * 2 * r;
+    q[t1] = min(max((rel1 * rn) >> sh, 0), rn - 1);
+    q[t2] = min(max((rel2 * rn) >> sh, 0), rn - 1);
+    return N.off[a] + fidx(a, q[0], q[1], q[2], rn);
 }
 
 __device__ inline float face_value(const LevelView& L, const float* __restrict__ u, int a, int b, const int cb[3], int r,
@@ -1157,6 +1289,7 @@ struct DropIn {
     const unsigned long long* hash;  // {pos, vel} at sort time, {pos, vel} now
 };
 constexpr int G2P_THREADS = 256;
+constexpr int G2P_TB = 4;  // tile entries whose loads a thread issues together
 constexpr int G2P_CHUNK = 512;
 constexpr int G2P_SLOT = G2P_CHUNK + 8;  // floats per staged array: chunk + alignment head and tail
 
@@ -1186,6 +1319,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                                                            DropIn D) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar[2];
+    __shared__ NbFaces nbr[27];
     const int b = blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
@@ -1208,9 +1342,21 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                 g2p_stage_chunk(soa, n, q0, q1, stage + c * 6 * G2P_SLOT, &bar[c], !(arm_only && c == 0));
             }
     }
-    // ghosted tiles (the copies above are in flight meanwhile)
+    // ghosted tiles (the copies above are in flight meanwhile).  The 26 neighbours' resolutions
+    // and face offsets are read once into shared memory; each thread then locates G2P_TB entries
+    // and issues their loads together.
     int cb[3];
     bcoord(L.g, b, cb);
+    if (threadIdx.x < 27) {
+        const int d = threadIdx.x;
+        const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
+        const int nb = inside(L.g, nc) ? bidx(L.g, nc[0], nc[1], nc[2]) : -1;
+        const int rn = nb >= 0 ? L.res[nb] : 0;
+        nbr[d].r = rn;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) nbr[d].off[k] = rn ? L.off[1 + k][nb] : 0u;
+    }
+    __syncthreads();
     {
         const int R1 = r + 1, R2 = r + 2;
         const int TA = (int)tile_axis(r);
@@ -1218,15 +1364,37 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-            for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
-                int fi[3];
-                fi[a] = rem % R1;
-                fi[t1] = (rem / R1) % R2 - 1;
-                fi[t2] = rem / (R1 * R2) - 1;
-                const uint32_t src = face_source(L, a, b, cb, r, fi);
-                const float vn = un.c[a][src];
-                if (tno) tno[a * TA + rem] = vn;
-                tw[a * TA + rem] = vn - alpha * uo.c[a][src];
+            const float* __restrict__ ua = un.c[a];
+            const float* __restrict__ va = uo.c[a];
+            for (int base = threadIdx.x; base < TA; base += G2P_TB * blockDim.x) {
+                uint32_t src[G2P_TB];
+#pragma unroll
+                for (int k = 0; k < G2P_TB; ++k) {
+                    const int rem = base + k * blockDim.x;
+                    src[k] = 0;
+                    if (rem < TA) {
+                        int fi[3];
+                        fi[a] = rem % R1;
+                        fi[t1] = (rem / R1) % R2 - 1;
+                        fi[t2] = rem / (R1 * R2) - 1;
+                        src[k] = face_source_nb(nbr, a, r, fi);
+                    }
+                }
+                float vn[G2P_TB], vo[G2P_TB];
+#pragma unroll
+                for (int k = 0; k < G2P_TB; ++k) {
+                    const bool ok = base + k * (int)blockDim.x < TA;
+                    vn[k] = ok ? ua[src[k]] : 0.f;
+                    vo[k] = ok ? va[src[k]] : 0.f;
+                }
+#pragma unroll
+                for (int k = 0; k < G2P_TB; ++k) {
+                    const int rem = base + k * blockDim.x;
+                    if (rem < TA) {
+                        if (tno) tno[a * TA + rem] = vn[k];
+                        tw[a * TA + rem] = vn[k] - alpha * vo[k];
+                    }
+                }
             }
         }
     }
