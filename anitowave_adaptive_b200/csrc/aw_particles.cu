@@ -545,6 +545,86 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     }
     __syncthreads();
     const int ncell = nonempty;
+    // Near-cell list of the cross-resolution pass (built here, so that warps that finish their
+    // deposit tasks go on to the pass without waiting for the others)
+    const int w = wid, nw = nwarp;
+    const bool listed = nc3 <= P2G_NEAR_CELLS;
+    if (xmask && listed) {
+        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
+            const int k = ch * 32 + lane;
+            uint32_t cm = 0;
+            int cnt = 0;
+            if (k < ncell) {
+                const int c = clist[k];
+                const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
+                for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
+                    const int d = __ffs(mm) - 1;
+                    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+                    const int reach = nres[d] < r ? 2 : 1;
+                    bool nr = true;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a)
+                        nr = nr && (dd[a] == 0 || (dd[a] < 0 ? cc[a] <= reach : cc[a] >= r - 1 - reach));
+                    if (nr) cm |= 1u << d;
+                }
+                if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (lane == 0) ccount[ch] = __popc(bal);
+            // stash this lane's result in the slot the final list will give it: first the chunk counts
+            nmask_tmp[k < P2G_NEAR_CELLS ? k : 0] = k < ncell ? cm : 0u;
+            ncnt_tmp[k < P2G_NEAR_CELLS ? k : 0] = cnt;
+        }
+        __syncthreads();
+        if (wid == 0) {  // exclusive scan of the per-chunk counts of near cells
+            int carry = 0;
+            const int nch = (ncell + 31) / 32;
+            for (int base = 0; base < nch; base += 32) {
+                const int ch = base + lane;
+                const int v = ch < nch ? ccount[ch] : 0;
+                int incl = v;
+#pragma unroll
+                for (int sh = 1; sh < 32; sh <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                    if (lane >= sh) incl += y;
+                }
+                if (ch < nch) ccount[ch] = carry + incl - v;
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) nnear = carry;
+        }
+        __syncthreads();
+        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
+            const int k = ch * 32 + lane;
+            const uint32_t cm = k < ncell ? nmask_tmp[k] : 0u;
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (cm) {
+                const int at = ccount[ch] + __popc(bal & ((1u << lane) - 1u));
+                nl_cell[at] = clist[k];
+                nl_mask[at] = cm;
+                nl_pre[at + 1] = ncnt_tmp[k];
+            }
+        }
+        __syncthreads();
+        if (wid == 0) {  // inclusive scan of the near cells' particle counts -> nl_pre[0..nnear]
+            int carry = 0;
+            const int nn = nnear;
+            for (int base = 0; base < nn; base += 32) {
+                const int k = base + lane;
+                const int v = k < nn ? (int)nl_pre[k + 1] : 0;
+                int incl = v;
+#pragma unroll
+                for (int sh = 1; sh < 32; sh <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
+                    if (lane >= sh) incl += y;
+                }
+                if (k < nn) nl_pre[k + 1] = (uint32_t)(carry + incl);
+                carry += __shfl_sync(0xffffffffu, incl, 31);
+            }
+            if (lane == 0) nl_pre[0] = 0;
+        }
+        __syncthreads();
+    }
     const uint32_t mc = maxcnt;
     const int nsl = (int)min((mc + P2G_SLICE - 1) / P2G_SLICE, (uint32_t)P2G_MAX_SLICES);
     const uint32_t slice = nsl ? (mc + nsl - 1) / nsl : 0;
@@ -667,84 +747,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // direction d when, on every axis d crosses, it lies within reach + 1 cells of that side
     // (reach: two of b's cells towards a coarser neighbour, one towards a finer; the extra cell
     // covers the rounding between a particle's key cell and its position in cell units).
-    const int w = wid, nw = nwarp;
-    const bool listed = nc3 <= P2G_NEAR_CELLS;
-    if (xmask && listed) {
-        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
-            const int k = ch * 32 + lane;
-            uint32_t cm = 0;
-            int cnt = 0;
-            if (k < ncell) {
-                const int c = clist[k];
-                const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
-                for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
-                    const int d = __ffs(mm) - 1;
-                    const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                    const int reach = nres[d] < r ? 2 : 1;
-                    bool nr = true;
-#pragma unroll
-                    for (int a = 0; a < 3; ++a)
-                        nr = nr && (dd[a] == 0 || (dd[a] < 0 ? cc[a] <= reach : cc[a] >= r - 1 - reach));
-                    if (nr) cm |= 1u << d;
-                }
-                if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
-            if (lane == 0) ccount[ch] = __popc(bal);
-            // stash this lane's result in the slot the final list will give it: first the chunk counts
-            nmask_tmp[k < P2G_NEAR_CELLS ? k : 0] = k < ncell ? cm : 0u;
-            ncnt_tmp[k < P2G_NEAR_CELLS ? k : 0] = cnt;
-        }
-        __syncthreads();
-        if (wid == 0) {  // exclusive scan of the per-chunk counts of near cells
-            int carry = 0;
-            const int nch = (ncell + 31) / 32;
-            for (int base = 0; base < nch; base += 32) {
-                const int ch = base + lane;
-                const int v = ch < nch ? ccount[ch] : 0;
-                int incl = v;
-#pragma unroll
-                for (int sh = 1; sh < 32; sh <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
-                    if (lane >= sh) incl += y;
-                }
-                if (ch < nch) ccount[ch] = carry + incl - v;
-                carry += __shfl_sync(0xffffffffu, incl, 31);
-            }
-            if (lane == 0) nnear = carry;
-        }
-        __syncthreads();
-        for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
-            const int k = ch * 32 + lane;
-            const uint32_t cm = k < ncell ? nmask_tmp[k] : 0u;
-            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
-            if (cm) {
-                const int at = ccount[ch] + __popc(bal & ((1u << lane) - 1u));
-                nl_cell[at] = clist[k];
-                nl_mask[at] = cm;
-                nl_pre[at + 1] = ncnt_tmp[k];
-            }
-        }
-        __syncthreads();
-        if (wid == 0) {  // inclusive scan of the near cells' particle counts -> nl_pre[0..nnear]
-            int carry = 0;
-            const int nn = nnear;
-            for (int base = 0; base < nn; base += 32) {
-                const int k = base + lane;
-                const int v = k < nn ? (int)nl_pre[k + 1] : 0;
-                int incl = v;
-#pragma unroll
-                for (int sh = 1; sh < 32; sh <<= 1) {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, sh);
-                    if (lane >= sh) incl += y;
-                }
-                if (k < nn) nl_pre[k + 1] = (uint32_t)(carry + incl);
-                carry += __shfl_sync(0xffffffffu, incl, 31);
-            }
-            if (lane == 0) nl_pre[0] = 0;
-        }
-        __syncthreads();
-    }
     const int nn = listed ? nnear : 0;
     const uint32_t T = listed ? (xmask ? nl_pre[nn] : 0u) : p1 - p0;
     const uint32_t Ls = (T + 31) / 32;
@@ -1271,15 +1273,18 @@ __device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* er
 //   FLIP blend alpha (v + u_new - u_old) + (1 - alpha) u_new equals alpha v + I(w) because the
 //   trilinear interpolation I is linear), and the u_new tile is written to `tn` for the advection
 //   that follows.  Every active block writes its u_new tile, with particles or not.
-// - The block's particles (a contiguous range of each SoA array) are staged in chunks of G2P_CHUNK
-//   by TMA bulk copies (cp.async.bulk, no multicast), two chunks in flight, each behind an mbarrier
-//   with a bounded wait.  A copy starts at the 16-byte boundary at or below the chunk's first
-//   element and its size is rounded up to 16 bytes, so up to 3 floats past the end of the last array
-//   are read: SoA buffers are allocated kSoaPad floats longer.
-// - On a wait that runs out, the CTA waits (again bounded) for every copy it issued before it
-//   returns, so that no copy lands in shared memory that another CTA may then own.
-// arm_only (tests of the timeout path): chunk 0's barrier is armed but its copy is not issued, and
-// the waits poll `polls` times.
+// - The block's particles (a contiguous range of each SoA array) are staged by TMA bulk copies
+//   (cp.async.bulk, no multicast) in chunks of G2P_WCH.  Each warp runs its own two-stage pipeline
+//   over chunks w, w + 8, w + 16, ... with its own mbarriers, so no CTA-wide barrier sits in the
+//   particle loop; lane 0 issues the copies, every lane waits with a bounded wait.  The first two
+//   chunks of every warp are in flight while the tile is built.  A copy starts at the 16-byte
+//   boundary at or below the chunk's first element and its size is rounded up to 16 bytes, so up
+//   to 3 floats past the end of the last array are read: SoA buffers are allocated kSoaPad floats
+//   longer.
+// - On a wait that runs out, the warp waits (again bounded) for every copy it issued before it
+//   stops, so that no copy lands in shared memory after the CTA has given it up.
+// arm_only (tests of the timeout path): the barrier of the block's first chunk is armed but its copy
+// is not issued, and the waits poll `polls` times.
 // Drop-in mode (D.perm set): the particles are the sorted copy that aw_p2g made of the caller's AoS
 // arrays; the new velocities go to the caller's array through the sort permutation, no u_new tile is
 // written, and the kernel does nothing unless the caller's arrays still hash as they did then.
@@ -1290,8 +1295,10 @@ struct DropIn {
 };
 constexpr int G2P_THREADS = 256;
 constexpr int G2P_TB = 4;  // tile entries whose loads a thread issues together
-constexpr int G2P_CHUNK = 512;
-constexpr int G2P_SLOT = G2P_CHUNK + 8;  // floats per staged array: chunk + alignment head and tail
+constexpr int G2P_WARPS = G2P_THREADS / 32;
+constexpr int G2P_WCH = 64;              // particles per warp chunk (two per lane)
+constexpr int G2P_SLOT = G2P_WCH + 8;    // floats per staged array: chunk + alignment head and tail
+constexpr int G2P_STAGE_FLOATS = G2P_WARPS * 2 * 6 * G2P_SLOT;  // two stages of six arrays per warp
 
 __device__ inline void g2p_stage_chunk(const float* soa, int64_t n, uint32_t q0, uint32_t q1, float* slot,
                                        uint64_t* bar, bool issue) {
@@ -1318,7 +1325,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                                                            float* __restrict__ tn, int* err, int polls, int arm_only,
                                                            DropIn D) {
     extern __shared__ __align__(16) float sm[];
-    __shared__ __align__(8) uint64_t bar[2];
+    __shared__ __align__(8) uint64_t wbar[G2P_WARPS][2];
     __shared__ NbFaces nbr[27];
     const int b = blockIdx.x;
     const int r = L.res[b];
@@ -1326,21 +1333,24 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     if (D.perm && !sort_reusable(D.hash, true)) return;
     const uint32_t c0 = L.off[0][b];
     const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
-    const uint32_t nchunk = (p1 - p0 + G2P_CHUNK - 1) / G2P_CHUNK;
+    const uint32_t nchunk = (p1 - p0 + G2P_WCH - 1) / G2P_WCH;
     const uint32_t tb = tile_block(r);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* tw = sm;
-    float* stage = sm + tb;  // tb is a multiple of 4 floats
-    if (nchunk) {
-        if (threadIdx.x == 0) {
+    float* wstage = sm + tb + wid * 2 * 6 * G2P_SLOT;  // tb is a multiple of 4 floats
+    uint64_t* bar = wbar[wid];
+    if ((uint32_t)wid < nchunk) {  // this warp has chunks: its barriers and its first two copies
+        if (lane == 0) {
             mbar_init(&bar[0], 1);
             mbar_init(&bar[1], 1);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0)
-            for (uint32_t c = 0; c < 2 && c < nchunk; ++c) {
-                const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
-                g2p_stage_chunk(soa, n, q0, q1, stage + c * 6 * G2P_SLOT, &bar[c], !(arm_only && c == 0));
+            for (uint32_t k = 0; k < 2; ++k) {
+                const uint32_t c = wid + k * G2P_WARPS;
+                if (c >= nchunk) break;
+                const uint32_t q0 = p0 + c * G2P_WCH, q1 = min(p1, q0 + G2P_WCH);
+                g2p_stage_chunk(soa, n, q0, q1, wstage + k * 6 * G2P_SLOT, &bar[k], !(arm_only && c == 0));
             }
+        }
+        __syncwarp();
     }
     // ghosted tiles (the copies above are in flight meanwhile).  The 26 neighbours' resolutions
     // and face offsets are read once into shared memory; each thread then locates G2P_TB entries
@@ -1404,23 +1414,27 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(L.g, a, cb[a]);
-    for (uint32_t c = 0; c < nchunk; ++c) {
-        const int sl = c & 1;
-        const bool ok = mbar_wait_bounded(&bar[sl], (c >> 1) & 1u, err, polls);
-        if (!__syncthreads_and(ok)) {
-            // drain: the copies of chunks c and c + 1 may still be in flight
-            if (threadIdx.x == 0)
-                for (uint32_t k = c; k < c + 2 && k < nchunk; ++k)
-                    if (!(arm_only && k == 0)) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1u, err, polls);
-            __syncthreads();
-            return;
+    uint32_t k = 0;
+    for (uint32_t c = wid; c < nchunk; c += G2P_WARPS, ++k) {
+        const int sl = k & 1;
+        const bool ok = mbar_wait_bounded(&bar[sl], (k >> 1) & 1u, err, polls);
+        if (!__all_sync(0xffffffffu, ok)) {
+            // drain: the copies of this chunk and of the warp's next chunk may still be in flight
+            if (lane == 0)
+                for (uint32_t e = 0; e < 2; ++e) {
+                    const uint32_t ce = c + e * G2P_WARPS;
+                    if (ce < nchunk && !(arm_only && ce == 0))
+                        mbar_wait_bounded(&bar[(k + e) & 1], ((k + e) >> 1) & 1u, err, polls);
+                }
+            __syncwarp();
+            break;
         }
-        const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
-        const float* slot = stage + sl * 6 * G2P_SLOT;
+        const uint32_t q0 = p0 + c * G2P_WCH, q1 = min(p1, q0 + G2P_WCH);
+        const float* slot = wstage + sl * 6 * G2P_SLOT;
         uint32_t head[6];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) head[k] = (uint32_t)(((uintptr_t)(soa + (int64_t)k * n + q0) >> 2) & 3u);
-        for (uint32_t j = threadIdx.x; j < q1 - q0; j += blockDim.x) {
+        for (int a = 0; a < 6; ++a) head[a] = (uint32_t)(((uintptr_t)(soa + (int64_t)a * n + q0) >> 2) & 3u);
+        for (uint32_t j = lane; j < q1 - q0; j += 32) {
             const float X[3] = {slot[head[0] + j], slot[G2P_SLOT + head[1] + j], slot[2 * G2P_SLOT + head[2] + j]};
             float vout[3];
 #pragma unroll
@@ -1435,10 +1449,11 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                 for (int a = 0; a < 3; ++a) soa[(int64_t)(3 + a) * n + q0 + j] = vout[a];
             }
         }
-        __syncthreads();  // slot sl is free again
-        if (threadIdx.x == 0 && c + 2 < nchunk) {
-            const uint32_t n0 = p0 + (c + 2) * G2P_CHUNK, n1 = min(p1, n0 + G2P_CHUNK);
-            g2p_stage_chunk(soa, n, n0, n1, stage + sl * 6 * G2P_SLOT, &bar[sl], true);
+        __syncwarp();  // stage sl is free again
+        const uint32_t cn = c + 2 * G2P_WARPS;
+        if (lane == 0 && cn < nchunk) {
+            const uint32_t n0 = p0 + cn * G2P_WCH, n1 = min(p1, n0 + G2P_WCH);
+            g2p_stage_chunk(soa, n, n0, n1, wstage + sl * 6 * G2P_SLOT, &bar[sl], true);
         }
     }
 }
@@ -1456,9 +1471,20 @@ struct PointTile {
 __device__ inline PointTile point_tile(const LevelView& L, const int cb[3], int r, const float o[3], float invh,
                                        const float* __restrict__ tl, const uint32_t* __restrict__ toff,
                                        const float* __restrict__ tg, const float X[3]) {
-    int pc[3];
-    point_block(L.g, X, pc);
     PointTile T;
+    // A point farther than a margin from every side of block cb lies in cb for point_block as well:
+    // its subtraction and division err by a few ulps of the coordinate, far below the margin of
+    // 1e-4 block sizes plus 1e-6 of the coordinate's magnitude.  So the exact lookup, with its three
+    // divisions, runs only near the sides.
+    const float bs = L.g.bs;
+    bool inner = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float m = 1e-4f * bs + 1e-6f * (fabsf(o[k]) + bs), d = X[k] - o[k];
+        inner = inner && d > m && d < bs - m;
+    }
+    int pc[3] = {cb[0], cb[1], cb[2]};
+    if (!inner) point_block(L.g, X, pc);
     if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) {
         T.t = tl;
         T.r = r;
@@ -1629,7 +1655,7 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
     AW_TRY(ensure_tiles(G));
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
+    const size_t smem = ((size_t)tile_block(maxres) + G2P_STAGE_FLOATS) * sizeof(float);
     AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
     const int arm_only = G.test_copy_timeout ? 1 : 0;
@@ -2246,7 +2272,7 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
         AW_LAUNCH();
         int maxres = 0;
         for (int r : G.h_res) maxres = std::max(maxres, r);
-        const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
+        const size_t smem = ((size_t)tile_block(maxres) + G2P_STAGE_FLOATS) * sizeof(float);
         AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
         k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,
