@@ -411,6 +411,87 @@ constexpr int P2G_MAX_SLICES = 1 << 19;  // 6 * 8^3 * this stays below 2^31
 constexpr int P2G_MAX_CELLS = 16 * 16 * 16;  // cells of the largest block (base resolution <= 16)
 constexpr int P2G_NEAR_CELLS = 8 * 8 * 8;    // blocks up to this size list their near cells
 
+// The particles of one cell of b (resolution r) on the faces of component a of a coarser neighbour
+// (resolution rn = r / 2), register sums and one global atomic per face.  A cell of b lies within
+// one cell of the coarser lattice along every axis, inside one half of it, so the faces its
+// particles can reach are the same 2 x 2 x 2 for all of them: along a the faces below and above the
+// coarse cell, across it the two face rows on the cell's own side.  They are located from the fine
+// cell's centre; every weight is that of p2g_cross.
+template <bool PH>
+__device__ __forceinline__ void p2g_cross_cell(const CrossNb& N, int rn, int a, const int cc[3], const float o[3],
+                                               float h, const float* __restrict__ soa, int64_t n, uint32_t i0,
+                                               uint32_t i1, const FaceAcc& acc, const uint32_t* __restrict__ pid,
+                                               const float* __restrict__ phase) {
+    // axes a, t1, t2 picked by selects: a is not a compile-time constant here
+    const int t1 = a == 2 ? 0 : a + 1, t2 = a == 0 ? 2 : a - 1;
+    auto pick = [](const float v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); };
+    auto picki = [](const int v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); };
+    const float ina = N.invh;
+    const float oa = pick(N.o, a), o1 = pick(N.o, t1), o2 = pick(N.o, t2);
+    const float qca = (pick(o, a) + ((float)picki(cc, a) + 0.5f) * h - oa) * ina;
+    const float qc1 = (pick(o, t1) + ((float)picki(cc, t1) + 0.5f) * h - o1) * ina;
+    const float qc2 = (pick(o, t2) + ((float)picki(cc, t2) + 0.5f) * h - o2) * ina;
+    const int ia = (int)floorf(qca), j1 = (int)floorf(qc1 - 0.5f), j2 = (int)floorf(qc2 - 0.5f);
+    const float* __restrict__ pa = soa + (int64_t)a * n;
+    const float* __restrict__ p1 = soa + (int64_t)t1 * n;
+    const float* __restrict__ p2 = soa + (int64_t)t2 * n;
+    const float* __restrict__ pv = soa + (int64_t)(3 + a) * n;
+    float sw[2][2][2], sv[2][2][2], sq[2][2][2];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        sw[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
+        sv[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
+        sq[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
+    }
+    for (uint32_t i = i0; i < i1; ++i) {
+        const float qa = (pa[i] - oa) * ina, q1 = (p1[i] - o1) * ina, q2 = (p2[i] - o2) * ina;
+        const float va = pv[i];
+        const float ph = PH ? phase[pid[i]] : 0.f;
+        float A[2], B[2], Cq[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const float dA = qa - (float)(ia + k);
+            const float dB = q1 - ((float)(j1 + k) + 0.5f);
+            const float dC = q2 - ((float)(j2 + k) + 0.5f);
+            A[k] = dA * dA;
+            B[k] = dB * dB;
+            Cq[k] = dC * dC;
+        }
+#pragma unroll
+        for (int da = 0; da < 2; ++da)
+#pragma unroll
+            for (int d1 = 0; d1 < 2; ++d1)
+#pragma unroll
+                for (int d2 = 0; d2 < 2; ++d2) {
+                    const float tt = fmaxf(1.f - ((A[da] + B[d1]) + Cq[d2]), 0.f);
+                    const float w = tt * tt * tt;
+                    sw[da][d1][d2] += w;
+                    sv[da][d1][d2] += w * va;
+                    if (PH) sq[da][d1][d2] += w * ph;
+                }
+    }
+    float* mw = a == 0 ? acc.m[0] : (a == 1 ? acc.m[1] : acc.m[2]);
+    float* Pw = a == 0 ? acc.P[0] : (a == 1 ? acc.P[1] : acc.P[2]);
+    float* Qw = PH ? (a == 0 ? acc.Phi[0] : (a == 1 ? acc.Phi[1] : acc.Phi[2])) : nullptr;
+    const uint32_t ob = a == 0 ? N.off[0] : (a == 1 ? N.off[1] : N.off[2]);
+#pragma unroll
+    for (int da = 0; da < 2; ++da)
+#pragma unroll
+        for (int d1 = 0; d1 < 2; ++d1)
+#pragma unroll
+            for (int d2 = 0; d2 < 2; ++d2) {
+                const int fa = ia + da, f1 = j1 + d1, f2 = j2 + d2;
+                if (sw[da][d1][d2] == 0.f || fa < 0 || fa > rn || f1 < 0 || f1 >= rn || f2 < 0 || f2 >= rn) continue;
+                // (fa, f1, f2) along (a, t1, t2) -> face index of axis a
+                const uint32_t fi = ob + (a == 0 ? (uint32_t)(fa + (rn + 1) * (f1 + rn * f2))
+                                                 : (a == 1 ? (uint32_t)(f2 + rn * (fa + (rn + 1) * f1))
+                                                           : (uint32_t)(f1 + rn * (f2 + rn * fa))));
+                atomicAdd(&mw[fi], sw[da][d1][d2]);
+                atomicAdd(&Pw[fi], sv[da][d1][d2]);
+                if (PH && sq[da][d1][d2] != 0.f) atomicAdd(&Qw[fi], sq[da][d1][d2]);
+            }
+}
+
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
 __device__ __forceinline__ void p2g_cross_pair(const CrossNb* xn, const int* nres, uint32_t v, int d, uint32_t p0,
@@ -445,6 +526,11 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __shared__ uint32_t nl_mask[P2G_NEAR_CELLS], nl_pre[P2G_NEAR_CELLS + 1];
     __shared__ uint32_t nmask_tmp[P2G_NEAR_CELLS];
     __shared__ int ncnt_tmp[P2G_NEAR_CELLS];
+    // cells near a coarser neighbour and those directions (per-cell deposit into the coarse lattice)
+    __shared__ uint16_t cl_cell[P2G_NEAR_CELLS];
+    __shared__ uint32_t cl_mask[P2G_NEAR_CELLS];
+    __shared__ int ccount2[P2G_NEAR_CELLS / 32];
+    __shared__ int ncoarse, crossc;
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
@@ -474,6 +560,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     for (int i = threadIdx.x; i < ntile; i += blockDim.x) sm[i] = 0.f;
     if (threadIdx.x == 0) {
         cross = 0;
+        crossc = 0;
         maxcnt = 0;
     }
     __syncthreads();
@@ -485,6 +572,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         nres[d] = rn;
         if (rn && rn != r) {
             atomicOr(&cross, 1 << d);
+            if (rn < r) atomicOr(&crossc, 1 << d);
             xn[d].invh = 1.f / fcell(g, rn);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -569,40 +657,58 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                 }
                 if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
-            if (lane == 0) ccount[ch] = __popc(bal);
-            // stash this lane's result in the slot the final list will give it: first the chunk counts
-            nmask_tmp[k < P2G_NEAR_CELLS ? k : 0] = k < ncell ? cm : 0u;
-            ncnt_tmp[k < P2G_NEAR_CELLS ? k : 0] = cnt;
+            // coarser directions go to the per-cell list, finer ones to the queued pairs
+            const uint32_t cmc = cm & (uint32_t)crossc, cmf = cm & ~(uint32_t)crossc;
+            if (!cmf) cnt = 0;
+            const unsigned bal = __ballot_sync(0xffffffffu, cmf != 0);
+            const unsigned balc = __ballot_sync(0xffffffffu, cmc != 0);
+            if (lane == 0) {
+                ccount[ch] = __popc(bal);
+                ccount2[ch] = __popc(balc);
+            }
+            nmask_tmp[k] = k < ncell ? cm : 0u;  // both kinds, split again when compacting
+            ncnt_tmp[k] = cnt;
         }
         __syncthreads();
-        if (wid == 0) {  // exclusive scan of the per-chunk counts of near cells
+        if (wid < 2) {  // exclusive scans of the per-chunk counts: warp 0 finer, warp 1 coarser
+            int* cnts = wid == 0 ? ccount : ccount2;
             int carry = 0;
             const int nch = (ncell + 31) / 32;
             for (int base = 0; base < nch; base += 32) {
                 const int ch = base + lane;
-                const int v = ch < nch ? ccount[ch] : 0;
+                const int v = ch < nch ? cnts[ch] : 0;
                 int incl = v;
 #pragma unroll
                 for (int sh = 1; sh < 32; sh <<= 1) {
                     const int y = __shfl_up_sync(0xffffffffu, incl, sh);
                     if (lane >= sh) incl += y;
                 }
-                if (ch < nch) ccount[ch] = carry + incl - v;
+                if (ch < nch) cnts[ch] = carry + incl - v;
                 carry += __shfl_sync(0xffffffffu, incl, 31);
             }
-            if (lane == 0) nnear = carry;
+            if (lane == 0) {
+                if (wid == 0) nnear = carry;
+                else ncoarse = carry;
+            }
         }
         __syncthreads();
         for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
             const int k = ch * 32 + lane;
             const uint32_t cm = k < ncell ? nmask_tmp[k] : 0u;
-            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
-            if (cm) {
+            const uint32_t cmf = cm & ~(uint32_t)crossc, cmc = cm & (uint32_t)crossc;
+            const unsigned bal = __ballot_sync(0xffffffffu, cmf != 0);
+            const unsigned balc = __ballot_sync(0xffffffffu, cmc != 0);
+            const int c = k < ncell ? (int)clist[k] : 0;
+            if (cmf) {
                 const int at = ccount[ch] + __popc(bal & ((1u << lane) - 1u));
-                nl_cell[at] = clist[k];
-                nl_mask[at] = cm;
+                nl_cell[at] = (uint16_t)c;
+                nl_mask[at] = cmf;
                 nl_pre[at + 1] = ncnt_tmp[k];
+            }
+            if (cmc) {
+                const int at = ccount2[ch] + __popc(balc & ((1u << lane) - 1u));
+                cl_cell[at] = (uint16_t)c;
+                cl_mask[at] = cmc;
             }
         }
         __syncthreads();
@@ -738,6 +844,22 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                         atomicAdd(&apw[e], sv[da][d1][d2]);
                     }
                 }
+    }
+    // Per-cell deposit into coarser neighbours (blocks of up to P2G_NEAR_CELLS cells): a task is
+    // (component, cell near such a neighbour); it visits the neighbours of the cell's mask in turn.
+    if (listed && crossc) {
+        const int ncl = ncoarse;
+        const float h = fcell(g, r);
+        for (int task = threadIdx.x; task < 3 * ncl; task += blockDim.x) {
+            const int a = task / ncl, k = task - a * ncl;
+            const int c = cl_cell[k];
+            const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
+            const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+            for (uint32_t mm = cl_mask[k]; mm; mm &= mm - 1) {
+                const int d = __ffs(mm) - 1;
+                p2g_cross_cell<PH>(xn[d], nres[d], a, cc, o, h, soa, n, ca, ce, acc, pid, phase);
+            }
+        }
     }
     // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
     // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
@@ -1221,6 +1343,40 @@ __device__ inline float tile_interp(const float* __restrict__ t, int a, int r, c
     return c0 + f2 * (c1 - c0);
 }
 
+// The three components of tile_interp at one point, with the per-axis coordinates, floors and
+// fractions computed once (the same operations as three calls of tile_interp).
+__device__ __forceinline__ void tile_interp3(const float* __restrict__ t, int r, const float o[3], float invh,
+                                             const float X[3], float out[3]) {
+    const float rf = (float)r;
+    int iU[3], iV[3];
+    float fU[3], fV[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float u = (X[k] - o[k]) * invh;
+        const float su = fminf(fmaxf(u, 0.f), rf);
+        const float sv = fminf(fmaxf(u - 0.5f, -1.f), rf);
+        iU[k] = min(max((int)floorf(su), 0), r - 1);
+        iV[k] = min(max((int)floorf(sv), -1), r - 1);
+        fU[k] = su - (float)iU[k];
+        fV[k] = sv - (float)iV[k];
+    }
+    const int R1 = r + 1, R2 = r + 2, TA = (int)tile_axis(r);
+    const int s_1 = R1, s_2 = R1 * R2;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        const float fA = fU[a], f1 = fV[t1], f2 = fV[t2];
+        const float* p = t + a * TA + iU[a] + R1 * ((iV[t1] + 1) + R2 * (iV[t2] + 1));
+        const float c00 = p[0] + fA * (p[1] - p[0]);
+        const float c10 = p[s_1] + fA * (p[s_1 + 1] - p[s_1]);
+        const float c01 = p[s_2] + fA * (p[s_2 + 1] - p[s_2]);
+        const float c11 = p[s_1 + s_2] + fA * (p[s_1 + s_2 + 1] - p[s_1 + s_2]);
+        const float c0 = c00 + f1 * (c10 - c00);
+        const float c1 = c01 + f1 * (c11 - c01);
+        out[a] = c0 + f2 * (c1 - c0);
+    }
+}
+
 __device__ inline float sample_tiles(const LevelView& L, const uint32_t* __restrict__ toff, const float* __restrict__ tiles,
                                      int a, const float X[3]) {
     int cb[3];
@@ -1273,18 +1429,15 @@ __device__ inline bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, int* er
 //   FLIP blend alpha (v + u_new - u_old) + (1 - alpha) u_new equals alpha v + I(w) because the
 //   trilinear interpolation I is linear), and the u_new tile is written to `tn` for the advection
 //   that follows.  Every active block writes its u_new tile, with particles or not.
-// - The block's particles (a contiguous range of each SoA array) are staged by TMA bulk copies
-//   (cp.async.bulk, no multicast) in chunks of G2P_WCH.  Each warp runs its own two-stage pipeline
-//   over chunks w, w + 8, w + 16, ... with its own mbarriers, so no CTA-wide barrier sits in the
-//   particle loop; lane 0 issues the copies, every lane waits with a bounded wait.  The first two
-//   chunks of every warp are in flight while the tile is built.  A copy starts at the 16-byte
-//   boundary at or below the chunk's first element and its size is rounded up to 16 bytes, so up
-//   to 3 floats past the end of the last array are read: SoA buffers are allocated kSoaPad floats
-//   longer.
-// - On a wait that runs out, the warp waits (again bounded) for every copy it issued before it
-//   stops, so that no copy lands in shared memory after the CTA has given it up.
-// arm_only (tests of the timeout path): the barrier of the block's first chunk is armed but its copy
-// is not issued, and the waits poll `polls` times.
+// - The block's particles (a contiguous range of each SoA array) are staged in chunks of G2P_CHUNK
+//   by TMA bulk copies (cp.async.bulk, no multicast), two chunks in flight, each behind an mbarrier
+//   with a bounded wait.  A copy starts at the 16-byte boundary at or below the chunk's first
+//   element and its size is rounded up to 16 bytes, so up to 3 floats past the end of the last array
+//   are read: SoA buffers are allocated kSoaPad floats longer.
+// - On a wait that runs out, the CTA waits (again bounded) for every copy it issued before it
+//   returns, so that no copy lands in shared memory that another CTA may then own.
+// arm_only (tests of the timeout path): chunk 0's barrier is armed but its copy is not issued, and
+// the waits poll `polls` times.
 // Drop-in mode (D.perm set): the particles are the sorted copy that aw_p2g made of the caller's AoS
 // arrays; the new velocities go to the caller's array through the sort permutation, no u_new tile is
 // written, and the kernel does nothing unless the caller's arrays still hash as they did then.
@@ -1295,10 +1448,8 @@ struct DropIn {
 };
 constexpr int G2P_THREADS = 256;
 constexpr int G2P_TB = 4;  // tile entries whose loads a thread issues together
-constexpr int G2P_WARPS = G2P_THREADS / 32;
-constexpr int G2P_WCH = 64;              // particles per warp chunk (two per lane)
-constexpr int G2P_SLOT = G2P_WCH + 8;    // floats per staged array: chunk + alignment head and tail
-constexpr int G2P_STAGE_FLOATS = G2P_WARPS * 2 * 6 * G2P_SLOT;  // two stages of six arrays per warp
+constexpr int G2P_CHUNK = 512;
+constexpr int G2P_SLOT = G2P_CHUNK + 8;  // floats per staged array: chunk + alignment head and tail
 
 __device__ inline void g2p_stage_chunk(const float* soa, int64_t n, uint32_t q0, uint32_t q1, float* slot,
                                        uint64_t* bar, bool issue) {
@@ -1325,7 +1476,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                                                            float* __restrict__ tn, int* err, int polls, int arm_only,
                                                            DropIn D) {
     extern __shared__ __align__(16) float sm[];
-    __shared__ __align__(8) uint64_t wbar[G2P_WARPS][2];
+    __shared__ __align__(8) uint64_t bar[2];
     __shared__ NbFaces nbr[27];
     const int b = blockIdx.x;
     const int r = L.res[b];
@@ -1333,24 +1484,21 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     if (D.perm && !sort_reusable(D.hash, true)) return;
     const uint32_t c0 = L.off[0][b];
     const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
-    const uint32_t nchunk = (p1 - p0 + G2P_WCH - 1) / G2P_WCH;
+    const uint32_t nchunk = (p1 - p0 + G2P_CHUNK - 1) / G2P_CHUNK;
     const uint32_t tb = tile_block(r);
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     float* tw = sm;
-    float* wstage = sm + tb + wid * 2 * 6 * G2P_SLOT;  // tb is a multiple of 4 floats
-    uint64_t* bar = wbar[wid];
-    if ((uint32_t)wid < nchunk) {  // this warp has chunks: its barriers and its first two copies
-        if (lane == 0) {
+    float* stage = sm + tb;  // tb is a multiple of 4 floats
+    if (nchunk) {
+        if (threadIdx.x == 0) {
             mbar_init(&bar[0], 1);
             mbar_init(&bar[1], 1);
-            for (uint32_t k = 0; k < 2; ++k) {
-                const uint32_t c = wid + k * G2P_WARPS;
-                if (c >= nchunk) break;
-                const uint32_t q0 = p0 + c * G2P_WCH, q1 = min(p1, q0 + G2P_WCH);
-                g2p_stage_chunk(soa, n, q0, q1, wstage + k * 6 * G2P_SLOT, &bar[k], !(arm_only && c == 0));
-            }
         }
-        __syncwarp();
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint32_t c = 0; c < 2 && c < nchunk; ++c) {
+                const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
+                g2p_stage_chunk(soa, n, q0, q1, stage + c * 6 * G2P_SLOT, &bar[c], !(arm_only && c == 0));
+            }
     }
     // ghosted tiles (the copies above are in flight meanwhile).  The 26 neighbours' resolutions
     // and face offsets are read once into shared memory; each thread then locates G2P_TB entries
@@ -1414,32 +1562,28 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     float o[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) o[a] = forigin(L.g, a, cb[a]);
-    uint32_t k = 0;
-    for (uint32_t c = wid; c < nchunk; c += G2P_WARPS, ++k) {
-        const int sl = k & 1;
-        const bool ok = mbar_wait_bounded(&bar[sl], (k >> 1) & 1u, err, polls);
-        if (!__all_sync(0xffffffffu, ok)) {
-            // drain: the copies of this chunk and of the warp's next chunk may still be in flight
-            if (lane == 0)
-                for (uint32_t e = 0; e < 2; ++e) {
-                    const uint32_t ce = c + e * G2P_WARPS;
-                    if (ce < nchunk && !(arm_only && ce == 0))
-                        mbar_wait_bounded(&bar[(k + e) & 1], ((k + e) >> 1) & 1u, err, polls);
-                }
-            __syncwarp();
-            break;
+    for (uint32_t c = 0; c < nchunk; ++c) {
+        const int sl = c & 1;
+        const bool ok = mbar_wait_bounded(&bar[sl], (c >> 1) & 1u, err, polls);
+        if (!__syncthreads_and(ok)) {
+            // drain: the copies of chunks c and c + 1 may still be in flight
+            if (threadIdx.x == 0)
+                for (uint32_t k = c; k < c + 2 && k < nchunk; ++k)
+                    if (!(arm_only && k == 0)) mbar_wait_bounded(&bar[k & 1], (k >> 1) & 1u, err, polls);
+            __syncthreads();
+            return;
         }
-        const uint32_t q0 = p0 + c * G2P_WCH, q1 = min(p1, q0 + G2P_WCH);
-        const float* slot = wstage + sl * 6 * G2P_SLOT;
+        const uint32_t q0 = p0 + c * G2P_CHUNK, q1 = min(p1, q0 + G2P_CHUNK);
+        const float* slot = stage + sl * 6 * G2P_SLOT;
         uint32_t head[6];
 #pragma unroll
-        for (int a = 0; a < 6; ++a) head[a] = (uint32_t)(((uintptr_t)(soa + (int64_t)a * n + q0) >> 2) & 3u);
-        for (uint32_t j = lane; j < q1 - q0; j += 32) {
+        for (int k = 0; k < 6; ++k) head[k] = (uint32_t)(((uintptr_t)(soa + (int64_t)k * n + q0) >> 2) & 3u);
+        for (uint32_t j = threadIdx.x; j < q1 - q0; j += blockDim.x) {
             const float X[3] = {slot[head[0] + j], slot[G2P_SLOT + head[1] + j], slot[2 * G2P_SLOT + head[2] + j]};
             float vout[3];
+            tile_interp3(tw, r, o, invh, X, vout);
 #pragma unroll
-            for (int a = 0; a < 3; ++a)
-                vout[a] = alpha * slot[(3 + a) * G2P_SLOT + head[3 + a] + j] + tile_interp(tw, a, r, o, invh, X);
+            for (int a = 0; a < 3; ++a) vout[a] += alpha * slot[(3 + a) * G2P_SLOT + head[3 + a] + j];
             if (D.perm) {
                 float* dst = D.aos + 3 * (size_t)D.perm[q0 + j];
 #pragma unroll
@@ -1449,11 +1593,10 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                 for (int a = 0; a < 3; ++a) soa[(int64_t)(3 + a) * n + q0 + j] = vout[a];
             }
         }
-        __syncwarp();  // stage sl is free again
-        const uint32_t cn = c + 2 * G2P_WARPS;
-        if (lane == 0 && cn < nchunk) {
-            const uint32_t n0 = p0 + cn * G2P_WCH, n1 = min(p1, n0 + G2P_WCH);
-            g2p_stage_chunk(soa, n, n0, n1, wstage + sl * 6 * G2P_SLOT, &bar[sl], true);
+        __syncthreads();  // slot sl is free again
+        if (threadIdx.x == 0 && c + 2 < nchunk) {
+            const uint32_t n0 = p0 + (c + 2) * G2P_CHUNK, n1 = min(p1, n0 + G2P_CHUNK);
+            g2p_stage_chunk(soa, n, n0, n1, stage + sl * 6 * G2P_SLOT, &bar[sl], true);
         }
     }
 }
@@ -1541,23 +1684,30 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
         float x[3], k1[3], k2[3], k3[3], y[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) x[a] = soa[(int64_t)a * n + i];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) k1[a] = tile_interp(sm, a, r, o, invh, x);
+        tile_interp3(sm, r, o, invh, x, k1);
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.5f * dt * k1[a];
         {
             const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)  // shared-memory loads when the point stays in the block
-                k2[a] = T.t == sm ? tile_interp(sm, a, r, o, invh, y) : (T.t ? tile_interp(T.t, a, T.r, T.o, T.invh, y) : 0.f);
+            if (T.t == sm) {  // shared-memory loads when the point stays in the block
+                tile_interp3(sm, r, o, invh, y, k2);
+            } else if (T.t) {
+                tile_interp3(T.t, T.r, T.o, T.invh, y, k2);
+            } else {
+                k2[0] = k2[1] = k2[2] = 0.f;
+            }
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) y[a] = x[a] + 0.75f * dt * k2[a];
         {
             const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
-#pragma unroll
-            for (int a = 0; a < 3; ++a)  // shared-memory loads when the point stays in the block
-                k3[a] = T.t == sm ? tile_interp(sm, a, r, o, invh, y) : (T.t ? tile_interp(T.t, a, T.r, T.o, T.invh, y) : 0.f);
+            if (T.t == sm) {  // shared-memory loads when the point stays in the block
+                tile_interp3(sm, r, o, invh, y, k3);
+            } else if (T.t) {
+                tile_interp3(T.t, T.r, T.o, T.invh, y, k3);
+            } else {
+                k3[0] = k3[1] = k3[2] = 0.f;
+            }
         }
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -1655,7 +1805,7 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
     AW_TRY(ensure_tiles(G));
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
-    const size_t smem = ((size_t)tile_block(maxres) + G2P_STAGE_FLOATS) * sizeof(float);
+    const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
     AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
     const int arm_only = G.test_copy_timeout ? 1 : 0;
@@ -2272,7 +2422,7 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
         AW_LAUNCH();
         int maxres = 0;
         for (int r : G.h_res) maxres = std::max(maxres, r);
-        const size_t smem = ((size_t)tile_block(maxres) + G2P_STAGE_FLOATS) * sizeof(float);
+        const size_t smem = ((size_t)tile_block(maxres) + 2 * 6 * G2P_SLOT) * sizeof(float);
         AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
         k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,

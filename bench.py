@@ -333,9 +333,11 @@ def run_ours(args, ws, rank, local):
         "roofline": {"kernel": "k_p2g_own (+ k_p2g_normalize)", "bound": "hbm", "achieved": p2g_gbs, "peak": hbm,
                      "unit": "GB/s", "frac": p2g_gbs / hbm, "peak_kind": peak_kind,
                      "traffic": traffic.get("k_p2g_own"), "bytes_per_launch": p2g_bytes, "ms_per_launch": p2g_ms,
-                     "note": "bound by shared-memory float atomics (about 25 per particle), not HBM"},
-        "roofline_g2p": {"kernel": "k_build_tiles_blend + k_g2p_tile", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm,
-                         "unit": "GB/s", "frac": g2p_gbs / hbm, "traffic": traffic.get("k_g2p_tile"),
+                     "note": "HBM is the roofline; the kernel runs below it, limited by instruction issue and "
+                             "load latency (weight arithmetic of the per-cell deposit and the cross-resolution "
+                             "pairs), see profiles/k_p2g_own_dam_drop_128.md"},
+        "roofline_g2p": {"kernel": "k_g2p_fused (+ k_g2p_inactive)", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm,
+                         "unit": "GB/s", "frac": g2p_gbs / hbm, "traffic": traffic.get("k_g2p_fused"),
                          "bytes_per_launch": g2p_bytes, "ms_per_launch": g2p_ms},
         "step_breakdown_ms": {k: last[k] for k in ("ms_sort", "ms_p2g", "ms_solve", "ms_g2p", "ms_advect", "ms_other")},
         "solver": {"cycles": last["cycles"], "residual": last["residual"], "div_before": last["div_before"],
