@@ -848,16 +848,23 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // Per-cell deposit into coarser neighbours (blocks of up to P2G_NEAR_CELLS cells): a task is
     // (component, cell near such a neighbour); it visits the neighbours of the cell's mask in turn.
     if (listed && crossc) {
+        // tasks are (component, listed cell, slice of the cell's particles), as for the own particles:
+        // coarse cells hold hundreds of particles
         const int ncl = ncoarse;
         const float h = fcell(g, r);
-        for (int task = threadIdx.x; task < 3 * ncl; task += blockDim.x) {
-            const int a = task / ncl, k = task - a * ncl;
+        const int per = ncl * nsl;
+        for (int task = threadIdx.x; task < 3 * per; task += blockDim.x) {
+            const int a = task / per, rem = task - a * per;
+            const int k = rem % ncl, sl = rem / ncl;
             const int c = cl_cell[k];
-            const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
             const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+            if ((uint32_t)sl * slice >= ce - ca) continue;
+            const uint32_t i0 = ca + (uint32_t)sl * slice;
+            const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
+            const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
             for (uint32_t mm = cl_mask[k]; mm; mm &= mm - 1) {
                 const int d = __ffs(mm) - 1;
-                p2g_cross_cell<PH>(xn[d], nres[d], a, cc, o, h, soa, n, ca, ce, acc, pid, phase);
+                p2g_cross_cell<PH>(xn[d], nres[d], a, cc, o, h, soa, n, i0, i1, acc, pid, phase);
             }
         }
     }
