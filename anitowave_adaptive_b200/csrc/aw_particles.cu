@@ -411,87 +411,6 @@ constexpr int P2G_MAX_SLICES = 1 << 19;  // 6 * 8^3 * this stays below 2^31
 constexpr int P2G_MAX_CELLS = 16 * 16 * 16;  // cells of the largest block (base resolution <= 16)
 constexpr int P2G_NEAR_CELLS = 8 * 8 * 8;    // blocks up to this size list their near cells
 
-// The particles of one cell of b (resolution r) on the faces of component a of a coarser neighbour
-// (resolution rn = r / 2), register sums and one global atomic per face.  A cell of b lies within
-// one cell of the coarser lattice along every axis, inside one half of it, so the faces its
-// particles can reach are the same 2 x 2 x 2 for all of them: along a the faces below and above the
-// coarse cell, across it the two face rows on the cell's own side.  They are located from the fine
-// cell's centre; every weight is that of p2g_cross.
-template <bool PH>
-__device__ __forceinline__ void p2g_cross_cell(const CrossNb& N, int rn, int a, const int cc[3], const float o[3],
-                                               float h, const float* __restrict__ soa, int64_t n, uint32_t i0,
-                                               uint32_t i1, const FaceAcc& acc, const uint32_t* __restrict__ pid,
-                                               const float* __restrict__ phase) {
-    // axes a, t1, t2 picked by selects: a is not a compile-time constant here
-    const int t1 = a == 2 ? 0 : a + 1, t2 = a == 0 ? 2 : a - 1;
-    auto pick = [](const float v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); };
-    auto picki = [](const int v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); };
-    const float ina = N.invh;
-    const float oa = pick(N.o, a), o1 = pick(N.o, t1), o2 = pick(N.o, t2);
-    const float qca = (pick(o, a) + ((float)picki(cc, a) + 0.5f) * h - oa) * ina;
-    const float qc1 = (pick(o, t1) + ((float)picki(cc, t1) + 0.5f) * h - o1) * ina;
-    const float qc2 = (pick(o, t2) + ((float)picki(cc, t2) + 0.5f) * h - o2) * ina;
-    const int ia = (int)floorf(qca), j1 = (int)floorf(qc1 - 0.5f), j2 = (int)floorf(qc2 - 0.5f);
-    const float* __restrict__ pa = soa + (int64_t)a * n;
-    const float* __restrict__ p1 = soa + (int64_t)t1 * n;
-    const float* __restrict__ p2 = soa + (int64_t)t2 * n;
-    const float* __restrict__ pv = soa + (int64_t)(3 + a) * n;
-    float sw[2][2][2], sv[2][2][2], sq[2][2][2];
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        sw[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
-        sv[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
-        sq[e >> 2][(e >> 1) & 1][e & 1] = 0.f;
-    }
-    for (uint32_t i = i0; i < i1; ++i) {
-        const float qa = (pa[i] - oa) * ina, q1 = (p1[i] - o1) * ina, q2 = (p2[i] - o2) * ina;
-        const float va = pv[i];
-        const float ph = PH ? phase[pid[i]] : 0.f;
-        float A[2], B[2], Cq[2];
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const float dA = qa - (float)(ia + k);
-            const float dB = q1 - ((float)(j1 + k) + 0.5f);
-            const float dC = q2 - ((float)(j2 + k) + 0.5f);
-            A[k] = dA * dA;
-            B[k] = dB * dB;
-            Cq[k] = dC * dC;
-        }
-#pragma unroll
-        for (int da = 0; da < 2; ++da)
-#pragma unroll
-            for (int d1 = 0; d1 < 2; ++d1)
-#pragma unroll
-                for (int d2 = 0; d2 < 2; ++d2) {
-                    const float tt = fmaxf(1.f - ((A[da] + B[d1]) + Cq[d2]), 0.f);
-                    const float w = tt * tt * tt;
-                    sw[da][d1][d2] += w;
-                    sv[da][d1][d2] += w * va;
-                    if (PH) sq[da][d1][d2] += w * ph;
-                }
-    }
-    float* mw = a == 0 ? acc.m[0] : (a == 1 ? acc.m[1] : acc.m[2]);
-    float* Pw = a == 0 ? acc.P[0] : (a == 1 ? acc.P[1] : acc.P[2]);
-    float* Qw = PH ? (a == 0 ? acc.Phi[0] : (a == 1 ? acc.Phi[1] : acc.Phi[2])) : nullptr;
-    const uint32_t ob = a == 0 ? N.off[0] : (a == 1 ? N.off[1] : N.off[2]);
-#pragma unroll
-    for (int da = 0; da < 2; ++da)
-#pragma unroll
-        for (int d1 = 0; d1 < 2; ++d1)
-#pragma unroll
-            for (int d2 = 0; d2 < 2; ++d2) {
-                const int fa = ia + da, f1 = j1 + d1, f2 = j2 + d2;
-                if (sw[da][d1][d2] == 0.f || fa < 0 || fa > rn || f1 < 0 || f1 >= rn || f2 < 0 || f2 >= rn) continue;
-                // (fa, f1, f2) along (a, t1, t2) -> face index of axis a
-                const uint32_t fi = ob + (a == 0 ? (uint32_t)(fa + (rn + 1) * (f1 + rn * f2))
-                                                 : (a == 1 ? (uint32_t)(f2 + rn * (fa + (rn + 1) * f1))
-                                                           : (uint32_t)(f1 + rn * (f2 + rn * fa))));
-                atomicAdd(&mw[fi], sw[da][d1][d2]);
-                atomicAdd(&Pw[fi], sv[da][d1][d2]);
-                if (PH && sq[da][d1][d2] != 0.f) atomicAdd(&Qw[fi], sq[da][d1][d2]);
-            }
-}
-
 // one queued (particle, neighbour direction d) pair: the particle's weights on neighbour d's faces
 template <bool PH>
 __device__ __forceinline__ void p2g_cross_pair(const CrossNb* xn, const int* nres, uint32_t v, int d, uint32_t p0,
@@ -526,11 +445,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __shared__ uint32_t nl_mask[P2G_NEAR_CELLS], nl_pre[P2G_NEAR_CELLS + 1];
     __shared__ uint32_t nmask_tmp[P2G_NEAR_CELLS];
     __shared__ int ncnt_tmp[P2G_NEAR_CELLS];
-    // cells near a coarser neighbour and those directions (per-cell deposit into the coarse lattice)
-    __shared__ uint16_t cl_cell[P2G_NEAR_CELLS];
-    __shared__ uint32_t cl_mask[P2G_NEAR_CELLS];
-    __shared__ int ccount2[P2G_NEAR_CELLS / 32];
-    __shared__ int ncoarse, crossc;
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
@@ -560,7 +474,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     for (int i = threadIdx.x; i < ntile; i += blockDim.x) sm[i] = 0.f;
     if (threadIdx.x == 0) {
         cross = 0;
-        crossc = 0;
         maxcnt = 0;
     }
     __syncthreads();
@@ -572,7 +485,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         nres[d] = rn;
         if (rn && rn != r) {
             atomicOr(&cross, 1 << d);
-            if (rn < r) atomicOr(&crossc, 1 << d);
             xn[d].invh = 1.f / fcell(g, rn);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -657,58 +569,40 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                 }
                 if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
             }
-            // coarser directions go to the per-cell list, finer ones to the queued pairs
-            const uint32_t cmc = cm & (uint32_t)crossc, cmf = cm & ~(uint32_t)crossc;
-            if (!cmf) cnt = 0;
-            const unsigned bal = __ballot_sync(0xffffffffu, cmf != 0);
-            const unsigned balc = __ballot_sync(0xffffffffu, cmc != 0);
-            if (lane == 0) {
-                ccount[ch] = __popc(bal);
-                ccount2[ch] = __popc(balc);
-            }
-            nmask_tmp[k] = k < ncell ? cm : 0u;  // both kinds, split again when compacting
-            ncnt_tmp[k] = cnt;
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (lane == 0) ccount[ch] = __popc(bal);
+            // stash this lane's result in the slot the final list will give it: first the chunk counts
+            nmask_tmp[k < P2G_NEAR_CELLS ? k : 0] = k < ncell ? cm : 0u;
+            ncnt_tmp[k < P2G_NEAR_CELLS ? k : 0] = cnt;
         }
         __syncthreads();
-        if (wid < 2) {  // exclusive scans of the per-chunk counts: warp 0 finer, warp 1 coarser
-            int* cnts = wid == 0 ? ccount : ccount2;
+        if (wid == 0) {  // exclusive scan of the per-chunk counts of near cells
             int carry = 0;
             const int nch = (ncell + 31) / 32;
             for (int base = 0; base < nch; base += 32) {
                 const int ch = base + lane;
-                const int v = ch < nch ? cnts[ch] : 0;
+                const int v = ch < nch ? ccount[ch] : 0;
                 int incl = v;
 #pragma unroll
                 for (int sh = 1; sh < 32; sh <<= 1) {
                     const int y = __shfl_up_sync(0xffffffffu, incl, sh);
                     if (lane >= sh) incl += y;
                 }
-                if (ch < nch) cnts[ch] = carry + incl - v;
+                if (ch < nch) ccount[ch] = carry + incl - v;
                 carry += __shfl_sync(0xffffffffu, incl, 31);
             }
-            if (lane == 0) {
-                if (wid == 0) nnear = carry;
-                else ncoarse = carry;
-            }
+            if (lane == 0) nnear = carry;
         }
         __syncthreads();
         for (int ch = wid; ch < (ncell + 31) / 32; ch += nwarp) {
             const int k = ch * 32 + lane;
             const uint32_t cm = k < ncell ? nmask_tmp[k] : 0u;
-            const uint32_t cmf = cm & ~(uint32_t)crossc, cmc = cm & (uint32_t)crossc;
-            const unsigned bal = __ballot_sync(0xffffffffu, cmf != 0);
-            const unsigned balc = __ballot_sync(0xffffffffu, cmc != 0);
-            const int c = k < ncell ? (int)clist[k] : 0;
-            if (cmf) {
+            const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
+            if (cm) {
                 const int at = ccount[ch] + __popc(bal & ((1u << lane) - 1u));
-                nl_cell[at] = (uint16_t)c;
-                nl_mask[at] = cmf;
+                nl_cell[at] = clist[k];
+                nl_mask[at] = cm;
                 nl_pre[at + 1] = ncnt_tmp[k];
-            }
-            if (cmc) {
-                const int at = ccount2[ch] + __popc(balc & ((1u << lane) - 1u));
-                cl_cell[at] = (uint16_t)c;
-                cl_mask[at] = cmc;
             }
         }
         __syncthreads();
@@ -844,29 +738,6 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                         atomicAdd(&apw[e], sv[da][d1][d2]);
                     }
                 }
-    }
-    // Per-cell deposit into coarser neighbours (blocks of up to P2G_NEAR_CELLS cells): a task is
-    // (component, cell near such a neighbour); it visits the neighbours of the cell's mask in turn.
-    if (listed && crossc) {
-        // tasks are (component, listed cell, slice of the cell's particles), as for the own particles:
-        // coarse cells hold hundreds of particles
-        const int ncl = ncoarse;
-        const float h = fcell(g, r);
-        const int per = ncl * nsl;
-        for (int task = threadIdx.x; task < 3 * per; task += blockDim.x) {
-            const int a = task / per, rem = task - a * per;
-            const int k = rem % ncl, sl = rem / ncl;
-            const int c = cl_cell[k];
-            const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
-            if ((uint32_t)sl * slice >= ce - ca) continue;
-            const uint32_t i0 = ca + (uint32_t)sl * slice;
-            const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
-            const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
-            for (uint32_t mm = cl_mask[k]; mm; mm &= mm - 1) {
-                const int d = __ffs(mm) - 1;
-                p2g_cross_cell<PH>(xn[d], nres[d], a, cc, o, h, soa, n, i0, i1, acc, pid, phase);
-            }
-        }
     }
     // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
     // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
