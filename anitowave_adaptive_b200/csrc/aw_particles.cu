@@ -376,31 +376,40 @@ __device__ __forceinline__ void p2g_cross(const CrossNb& N, int rn, const float 
     for (int k = 0; k < 3; ++k) q[k] = (X[k] - N.o[k]) * N.invh;
     const float rf = (float)rn;
     if (q[0] <= -1.f || q[1] <= -1.f || q[2] <= -1.f || q[0] >= rf + 1.f || q[1] >= rf + 1.f || q[2] >= rf + 1.f) return;
+    // Per component, only the face rows inside the neighbour are visited: for a face neighbour about
+    // half of the 2 x 2 x 2 candidates, for edges and corners fewer.
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
         const int ia = (int)floorf(q[a]);
         const int j1 = (int)floorf(q[t1] - 0.5f), j2 = (int)floorf(q[t2] - 0.5f);
+        const int a0 = max(ia, 0), a1 = min(ia + 1, rn);
+        const int b0 = max(j1, 0), b1 = min(j1 + 1, rn - 1);
+        const int e0 = max(j2, 0), e1 = min(j2 + 1, rn - 1);
         const uint32_t ob = N.off[a];
-        for (int da = 0; da < 2; ++da)
-            for (int d1 = 0; d1 < 2; ++d1)
-                for (int d2 = 0; d2 < 2; ++d2) {
-                    int f[3];
-                    f[a] = ia + da;
-                    f[t1] = j1 + d1;
-                    f[t2] = j2 + d2;
-                    if (f[a] < 0 || f[a] > rn || f[t1] < 0 || f[t1] >= rn || f[t2] < 0 || f[t2] >= rn) continue;
-                    const float dA = q[a] - (float)f[a];
-                    const float dB = q[t1] - ((float)f[t1] + 0.5f);
-                    const float dC = q[t2] - ((float)f[t2] + 0.5f);
-                    const float tt = 1.f - ((dA * dA + dB * dB) + dC * dC);
+#pragma unroll 1
+        for (int fa = a0; fa <= a1; ++fa) {
+            const float dA = q[a] - (float)fa;
+#pragma unroll 1
+            for (int f1 = b0; f1 <= b1; ++f1) {
+                const float dB = q[t1] - ((float)f1 + 0.5f);
+                const float AB = dA * dA + dB * dB;
+#pragma unroll 1
+                for (int f2 = e0; f2 <= e1; ++f2) {
+                    const float dC = q[t2] - ((float)f2 + 0.5f);
+                    const float tt = 1.f - (AB + dC * dC);
                     if (tt <= 0.f) continue;
                     const float w = tt * tt * tt;
-                    const uint32_t fi = ob + fidx(a, f[0], f[1], f[2], rn);
+                    // (fa, f1, f2) along (a, t1, t2) -> the face index of axis a
+                    const uint32_t fi = ob + (a == 0 ? (uint32_t)(fa + (rn + 1) * (f1 + rn * f2))
+                                                     : (a == 1 ? (uint32_t)(f2 + rn * (fa + (rn + 1) * f1))
+                                                               : (uint32_t)(f1 + rn * (f2 + rn * fa))));
                     atomicAdd(&acc.m[a][fi], w);
                     atomicAdd(&acc.P[a][fi], w * V[a]);
                     if (PH && ph != 0.f) atomicAdd(&acc.Phi[a][fi], w * ph);
                 }
+            }
+        }
     }
 }
 
