@@ -887,13 +887,11 @@ extern "C" aw_status aw_flip_rebuild_levels(aw_flip* F, const int32_t* h_thresho
         G.allocated = true;
         return AW_OK;
     }
-    // a new layout: channels, tiles and the solver hierarchy follow it; the particles carry the state
-    if (F->solver) {
-        aw_solver_destroy(F->solver);
-        F->solver = nullptr;
-    }
+    // a new layout: channels, tiles and the solver hierarchy follow it, in the storage they had
+    // (grow-only buffers); the particles carry the state
     AW_TRY(aw_msbg_allocate(F->g, s_));
-    AW_TRY(aw_solver_create(F->g, &F->sd, &F->solver));
+    if (F->solver) AW_TRY(solver_relayout(F->solver));
+    else AW_TRY(aw_solver_create(F->g, &F->sd, &F->solver));
     AW_TRY(F->B.ensure(G));
     F->B.p_warm = false;  // cell indices changed
     if (changed) *changed = 1;

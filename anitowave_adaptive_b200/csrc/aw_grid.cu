@@ -384,21 +384,19 @@ static inline unsigned nblk(size_t n, int t = 256) { return (unsigned)((n + t - 
 aw_status level_offsets(MsbgState& G, int m, int vanish, uint32_t* d_off4, int* d_res, uint32_t tot[4], cudaStream_t s) {
     size_t nb = (size_t)G.nb;
     AW_TRY(G.scratch_u32.ensure(4 * (nb + 1)));
+    // four scanned rows of nb+1 values (the last one is the row's total), then the four totals
+    AW_TRY(G.scratch_scan.ensure(4 * (nb + 1) + 4));
     uint32_t* cnt = G.scratch_u32.p;
+    uint32_t* scan = G.scratch_scan.p;
     k_count<<<nblk(nb), 256, 0, s>>>(G.geo, G.level.p, m, vanish, cnt, d_res);
     AW_LAUNCH();
-    DBuf<uint32_t> tmp, tot_d;
-    AW_TRY(tot_d.alloc(4));
     for (int k = 0; k < 4; ++k) {
-        // scan writes nb+1 values; stage through a temporary so d_off4 rows stay nb long
-        DBuf<uint32_t> o;
-        AW_TRY(o.alloc(nb + 1));
-        AW_TRY(exclusive_scan_u32(cnt + k * nb, o.p, nb, tmp, s));
-        AW_CUDA(cudaMemcpyAsync(d_off4 + k * nb, o.p, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-        AW_CUDA(cudaMemcpyAsync(tot_d.p + k, o.p + nb, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
-        AW_CUDA(cudaStreamSynchronize(s));
+        uint32_t* o = scan + k * (nb + 1);
+        AW_TRY(exclusive_scan_u32(cnt + k * nb, o, nb, G.scratch_scan_tmp, s));
+        AW_CUDA(cudaMemcpyAsync(d_off4 + k * nb, o, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+        AW_CUDA(cudaMemcpyAsync(scan + 4 * (nb + 1) + k, o + nb, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
     }
-    AW_CUDA(cudaMemcpyAsync(tot, tot_d.p, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+    AW_CUDA(cudaMemcpyAsync(tot, scan + 4 * (nb + 1), 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     AW_CUDA(cudaStreamSynchronize(s));
     return AW_OK;
 }
@@ -566,8 +564,8 @@ extern "C" aw_status aw_msbg_allocate(aw_msbg* g, aw_stream s_) {
     size_t nb = (size_t)G.nb;
     for (int k = 0; k < 4; ++k) AW_TRY(G.off[k].ensure(nb));
     AW_TRY(G.res.ensure(nb));
-    DBuf<uint32_t> off4;
-    AW_TRY(off4.alloc(4 * nb));
+    DBuf<uint32_t>& off4 = G.scratch_off4;
+    AW_TRY(off4.ensure(4 * nb));
     AW_TRY(level_offsets(G, 0, 1, off4.p, G.res.p, G.tot, s));
     for (int k = 0; k < 4; ++k)
         AW_CUDA(cudaMemcpyAsync(G.off[k].p, off4.p + k * nb, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
@@ -593,7 +591,8 @@ extern "C" aw_status aw_msbg_allocate(aw_msbg* g, aw_stream s_) {
         for (int a = 0; a < 3; ++a) cnt[fb + a] = G.tot[1 + a];
     for (int c = 0; c < AW_NUM_CHANNELS_EXT; ++c)
         if (cnt[c]) total += ((cnt[c] + pad - 1) / pad) * pad;
-    AW_TRY(G.slab.alloc(total));
+    // grow-only: a re-layout that fits the previous slab reuses it (no free/allocate on the way)
+    AW_TRY(G.slab.ensure(total));
     AW_CUDA(cudaMemsetAsync(G.slab.p, 0, total * sizeof(float), s));
     size_t at = 0;
     for (int c = 0; c < AW_NUM_CHANNELS_EXT; ++c) {

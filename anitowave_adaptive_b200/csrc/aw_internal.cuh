@@ -220,6 +220,7 @@ struct MsbgState {
     float* ch[AW_NUM_CHANNELS_EXT] = {};    // channel pointers into the slab
     uint32_t ch_count[AW_NUM_CHANNELS_EXT] = {};
     DBuf<uint32_t> scratch_u32;
+    DBuf<uint32_t> scratch_scan, scratch_scan_tmp, scratch_off4;  // level_offsets / aw_msbg_allocate
     // ghosted face tiles (per block: 3 axes x (r+1)(r+2)^2, padded to 16 bytes)
     DBuf<uint32_t> tile_off;
     std::vector<uint32_t> h_tile_off;
@@ -255,6 +256,10 @@ aw_status levels_from_positions(MsbgState& G, const float* d_pos, int64_t si, in
 // host synchronisation).  Marks the grid unallocated.
 aw_status relevel_on_device(MsbgState& G, const float* d_pos, int64_t si, int64_t sa, int64_t n,
                             const int32_t* thresholds, int* changed, int* passes, cudaStream_t s);
+
+// Rebuilds a solver's multigrid hierarchy for the grid's new layout (after aw_msbg_allocate), in
+// the storage it already holds where the new levels fit, and sets it up with every cell fluid.
+aw_status solver_relayout(aw_solver* S);
 
 // Exclusive scan of n u32 values into out[0..n] (out[n] = total).  tmp: scan scratch.
 aw_status exclusive_scan_u32(const uint32_t* in, uint32_t* out, size_t n, DBuf<uint32_t>& tmp, cudaStream_t s);

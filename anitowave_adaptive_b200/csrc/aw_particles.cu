@@ -1646,10 +1646,10 @@ aw_status ensure_tiles(MsbgState& G) {
         acc += tile_block(G.h_res[b]);
     }
     G.tile_tot = acc;
-    AW_TRY(G.tile_off.alloc(G.nb));
+    AW_TRY(G.tile_off.ensure(G.nb));
     AW_CUDA(cudaMemcpy(G.tile_off.p, G.h_tile_off.data(), G.nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
-    AW_TRY(G.tiles_new.alloc(std::max<uint32_t>(acc, 4)));
-    AW_TRY(G.tiles_old.alloc(std::max<uint32_t>(acc, 4)));
+    AW_TRY(G.tiles_new.ensure(std::max<uint32_t>(acc, 4)));
+    AW_TRY(G.tiles_old.ensure(std::max<uint32_t>(acc, 4)));
     AW_TRY(G.err.ensure(4));
     AW_CUDA(cudaMemset(G.err.p, 0, 4 * sizeof(int)));
     return AW_OK;

@@ -1414,7 +1414,7 @@ static aw_status build_batches(MGLevel& L, const Geo& geo) {
         L.ndesc[k] = (int)desc.size();
         L.h_blocks[k] = std::move(blocks);
         if (L.ndesc[k]) {
-            AW_TRY(L.desc[k].alloc(desc.size()));
+            AW_TRY(L.desc[k].ensure(desc.size()));
             AW_CUDA(cudaMemcpy(L.desc[k].p, desc.data(), desc.size() * sizeof(int4), cudaMemcpyHostToDevice));
         }
     }
@@ -1468,7 +1468,7 @@ static aw_status build_meta(MGLevel& L, const Geo& geo, const HostLevel& h, cons
                 F(MF_COARSE_RES) = coarser->res[b];
             }
         }
-        AW_TRY(L.meta[k].alloc(mt.size()));
+        AW_TRY(L.meta[k].ensure(mt.size()));
         AW_CUDA(cudaMemcpy(L.meta[k].p, mt.data(), mt.size() * sizeof(int), cudaMemcpyHostToDevice));
     }
     return AW_OK;
@@ -1720,83 +1720,105 @@ extern "C" aw_status aw_solver_update_coefficients(aw_solver* S, aw_stream s) {
     return build_coefficients(S, (cudaStream_t)s);
 }
 
-extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_solver** out) {
-    AW_CHECK_ARG(g && d && out, "null argument");
-    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
-    AW_CHECK_ARG(d->operator_mode == AW_OPERATOR_FV || d->operator_mode == AW_OPERATOR_REFERENCE, "bad operator mode");
-    AW_CHECK_ARG(d->precision == AW_PRECISION_FP32 || d->precision == AW_PRECISION_MIXED ||
-                     d->precision == AW_PRECISION_FP32_PCG,
-                 "bad precision");
-    AW_CHECK_ARG(d->block_iterations >= 1 && d->pre_smooth >= 0 && d->post_smooth >= 0, "bad smoother settings");
-    *out = nullptr;
-    MsbgState& G = g->st;
-    {  // the stencils assume 2:1 grading between face neighbours
-        const Geo& geo = G.geo;
-        for (int b = 0; b < G.nb; ++b) {
-            if ((int)G.h_level[b] >= geo.L) continue;
-            int c[3];
-            bcoord(geo, b, c);
-            for (int a = 0; a < 3; ++a) {
-                int nc[3] = {c[0], c[1], c[2]};
-                nc[a] += 1;
-                if (!inside(geo, nc)) continue;
-                uint32_t nl = G.h_level[bidx(geo, nc[0], nc[1], nc[2])];
-                if ((int)nl < geo.L && std::abs((int)nl - (int)G.h_level[b]) > 1)
-                    return set_error(AW_ERR_INVALID_ARGUMENT,
-                                     "level map is not 2:1 graded (block %d); run aw_msbg_enforce_grading first", b);
-            }
+// The multigrid hierarchy of the grid's current layout, built into S.  Every device buffer grows
+// only: a re-layout whose levels fit the previous ones reuses their storage, so rebuilding the
+// solver after aw_flip_rebuild_levels allocates and frees nothing in the common case.
+static void reset_level(MGLevel& L) {
+    L.dense = false;
+    L.D[0] = L.D[1] = L.D[2] = 0;
+    L.H = 0.f;
+    L.half = false;
+    L.h_res.clear();
+    for (int k = 0; k < 4; ++k) L.tot[k] = 0;
+    for (int k = 0; k < 3; ++k) {
+        L.h_blocks[k].clear();
+        L.ndesc[k] = 0;
+    }
+    L.smem_smooth = L.smem_x64 = L.smem_prolong = L.smem_meta = 0;
+    L.maxres = 0;
+}
+
+// The stencils assume 2:1 grading between face neighbours.
+static aw_status check_grading(const MsbgState& G) {
+    const Geo& geo = G.geo;
+    for (int b = 0; b < G.nb; ++b) {
+        if ((int)G.h_level[b] >= geo.L) continue;
+        int c[3];
+        bcoord(geo, b, c);
+        for (int a = 0; a < 3; ++a) {
+            int nc[3] = {c[0], c[1], c[2]};
+            nc[a] += 1;
+            if (!inside(geo, nc)) continue;
+            uint32_t nl = G.h_level[bidx(geo, nc[0], nc[1], nc[2])];
+            if ((int)nl < geo.L && std::abs((int)nl - (int)G.h_level[b]) > 1)
+                return set_error(AW_ERR_INVALID_ARGUMENT,
+                                 "level map is not 2:1 graded (block %d); run aw_msbg_enforce_grading first", b);
         }
     }
-    std::unique_ptr<aw_solver> S(new aw_solver());
-    S->g = g;
-    S->d = *d;
-    const bool ref = d->operator_mode == AW_OPERATOR_REFERENCE;
+    return AW_OK;
+}
+
+static aw_status solver_build(aw_solver* S) {
+    aw_msbg* g = S->g;
+    MsbgState& G = g->st;
+    S->exact = false;
+    S->coef_dirty = true;
+    S->smem_max = S->smem_max64 = 0;
+    if (S->cycle) cudaGraphExecDestroy(S->cycle);
+    S->cycle = nullptr;
+    S->cycle_x0 = S->cycle_b0 = nullptr;
+    S->cycle_kernels = 0;
+    S->x0 = nullptr;
+    S->b0 = nullptr;
+    const bool ref = S->d.operator_mode == AW_OPERATOR_REFERENCE;
     const int nb = G.nb;
-    int M = d->mg_levels > 0 ? d->mg_levels : (ref ? G.geo.L : ilog2(G.geo.R0) + 1);
+    int M = S->d.mg_levels > 0 ? S->d.mg_levels : (ref ? G.geo.L : ilog2(G.geo.R0) + 1);
     if (!ref) M = std::min(M, ilog2(G.geo.R0) + 1);
     cudaStream_t s = 0;
-    S->lv.resize(M);
+    if (S->lv.size() < (size_t)M) S->lv.resize(M);
+    DBuf<uint32_t>& off4 = G.scratch_off4;
+    AW_TRY(off4.ensure(4 * (size_t)nb));
+    int nlev = M;
     for (int m = 0; m < M; ++m) {
         MGLevel& L = S->lv[m];
-        AW_TRY(L.res.alloc(nb));
-        DBuf<uint32_t> off4;
-        AW_TRY(off4.alloc(4 * (size_t)nb));
+        reset_level(L);
+        AW_TRY(L.res.ensure(nb));
         AW_TRY(level_offsets(G, m, ref ? 1 : 0, off4.p, L.res.p, L.tot, s));
         for (int k = 0; k < 4; ++k) {
-            AW_TRY(L.off[k].alloc(nb));
+            AW_TRY(L.off[k].ensure(nb));
             AW_CUDA(cudaMemcpy(L.off[k].p, off4.p + (size_t)k * nb, nb * sizeof(uint32_t), cudaMemcpyDeviceToDevice));
         }
         L.h_res.resize(nb);
         AW_CUDA(cudaMemcpy(L.h_res.data(), L.res.p, nb * sizeof(int), cudaMemcpyDeviceToHost));
         for (int b = 0; b < nb; ++b) L.maxres = std::max(L.maxres, L.h_res[b]);
         if (L.maxres == 0) {
-            S->lv.resize(m);
+            nlev = m;
             break;
         }
         AW_TRY(build_batches(L, G.geo));
-        AW_TRY(L.status[0].alloc(nb));
-        AW_TRY(L.status[1].alloc(nb));
-        L.half = (d->precision == AW_PRECISION_MIXED) && m >= 1 && m < M - 1 + (ref ? 0 : 1) && L.maxres > 1;
+        AW_TRY(L.status[0].ensure(nb));
+        AW_TRY(L.status[1].ensure(nb));
+        L.half = (S->d.precision == AW_PRECISION_MIXED) && m >= 1 && m < M - 1 + (ref ? 0 : 1) && L.maxres > 1;
         size_t nc = L.ncell();
-        AW_TRY(L.x.alloc(nc));
-        AW_TRY(L.b.alloc(nc));
-        AW_TRY(L.r.alloc(nc));
-        AW_TRY(L.fluid.alloc(nc + 16));  // whole 32-bit words are staged
+        AW_TRY(L.x.ensure(nc));
+        AW_TRY(L.b.ensure(nc));
+        AW_TRY(L.r.ensure(nc));
+        AW_TRY(L.fluid.ensure(nc + 16));  // whole 32-bit words are staged
         AW_CUDA(cudaMemset(L.x.p, 0, nc * sizeof(float)));
         AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
         AW_CUDA(cudaMemset(L.fluid.p, 1, nc + 16));
         if (L.half) {
-            AW_TRY(L.xh.alloc(nc));
-            AW_TRY(L.xscale.alloc(nb));
+            AW_TRY(L.xh.ensure(nc));
+            AW_TRY(L.xscale.ensure(nb));
             AW_CUDA(cudaMemset(L.xh.p, 0, nc * sizeof(__half)));
             AW_CUDA(cudaMemset(L.xscale.p, 0, nb * sizeof(float)));
         }
         for (int a = 0; a < 3; ++a) {
-            AW_TRY(L.W[a].alloc(L.nface(a)));
-            AW_TRY(L.bbar[a].alloc(L.nface(a)));
+            AW_TRY(L.W[a].ensure(L.nface(a)));
+            AW_TRY(L.bbar[a].ensure(L.nface(a)));
         }
     }
-    S->nmsbg = (int)S->lv.size();
+    S->nmsbg = nlev;
     {
         std::vector<HostLevel> hl(S->nmsbg);
         for (int m = 0; m < S->nmsbg; ++m) {
@@ -1815,47 +1837,51 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         }
     }
     // coefficients of the block-structured levels
-    AW_TRY(build_coefficients(S.get(), 0));
+    AW_TRY(build_coefficients(S, 0));
     // uniform continuation below one cell per block (FV mode)
-    if (!ref && S->nmsbg > 0 && S->lv.back().maxres == 1) {
+    size_t used = (size_t)S->nmsbg;
+    if (!ref && S->nmsbg > 0 && S->lv[S->nmsbg - 1].maxres == 1) {
         int Dd[3] = {G.geo.D[0], G.geo.D[1], G.geo.D[2]};
         float H = G.geo.bs;
         while (Dd[0] % 2 == 0 && Dd[1] % 2 == 0 && Dd[2] % 2 == 0 && (long)Dd[0] * Dd[1] * Dd[2] > 64) {
-            S->lv.emplace_back();
-            MGLevel& L = S->lv.back();
+            if (S->lv.size() <= used) S->lv.emplace_back();
+            MGLevel& L = S->lv[used++];
+            reset_level(L);
             L.dense = true;
             for (int a = 0; a < 3; ++a) L.D[a] = Dd[a] / 2;
             H *= 2.f;
             L.H = H;
             size_t nc = L.ncell();
-            AW_TRY(L.x.alloc(nc));
-            AW_TRY(L.b.alloc(nc));
-            AW_TRY(L.r.alloc(nc));
-            AW_TRY(L.fluid.alloc(nc));
+            AW_TRY(L.x.ensure(nc));
+            AW_TRY(L.b.ensure(nc));
+            AW_TRY(L.r.ensure(nc));
+            AW_TRY(L.fluid.ensure(nc));
             AW_CUDA(cudaMemset(L.x.p, 0, nc * sizeof(float)));
             AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
             for (int a = 0; a < 3; ++a) {
-                AW_TRY(L.W[a].alloc(L.nface(a)));
+                AW_TRY(L.W[a].ensure(L.nface(a)));
                 k_dense_conductance<<<nblk(L.nface(a)), 256>>>(dview(L), a, H, L.W[a].p);
                 AW_LAUNCH();
             }
             for (int a = 0; a < 3; ++a) Dd[a] /= 2;
         }
+        S->lv.resize(used);  // levels beyond the new hierarchy are released
         // the coarsest level is uniform: factorise it densely when small enough
         MGLevel& C = S->lv.back();
         size_t npos = C.dense ? C.ncell() : (size_t)nb;
         if (npos <= (size_t)EXACT_POS_CAP) {
-            AW_TRY(S->M.alloc((size_t)EXACT_CAP * EXACT_CAP));
-            AW_TRY(S->Minv.alloc((size_t)EXACT_CAP * EXACT_CAP));
-            AW_TRY(S->ex_idx.alloc(EXACT_CAP));
-            AW_TRY(S->ex_pos.alloc(npos));
-            AW_TRY(S->ex_prev.alloc(npos));
+            AW_TRY(S->M.ensure((size_t)EXACT_CAP * EXACT_CAP));
+            AW_TRY(S->Minv.ensure((size_t)EXACT_CAP * EXACT_CAP));
+            AW_TRY(S->ex_idx.ensure(EXACT_CAP));
+            AW_TRY(S->ex_pos.ensure(npos));
+            AW_TRY(S->ex_prev.ensure(npos));
             AW_CUDA(cudaMemset(S->ex_prev.p, 0xFF, npos));
-            AW_TRY(S->ex_n.alloc(1));
+            AW_TRY(S->ex_n.ensure(1));
             AW_CUDA(cudaMemset(S->ex_n.p, 0, sizeof(int)));
             S->exact = true;
         }
     }
+    S->lv.resize(used);
     {  // always opted in: static shared memory (k_smooth's per-slot state) counts against the default 48 KB too
         AW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_residual<SrcX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
@@ -1863,31 +1889,58 @@ extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_so
         AW_CUDA(cudaFuncSetAttribute(k_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
     }
     AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
-    if (d->precision == AW_PRECISION_MIXED) {
+    if (S->d.precision == AW_PRECISION_MIXED) {
         const size_t nc0 = S->lv[0].ncell();
-        AW_TRY(S->cg_r.alloc(nc0));
-        AW_TRY(S->cg_d.alloc(nc0));
-        AW_TRY(S->cg_q.alloc(nc0));
-        AW_TRY(S->cg_sc.alloc(4));
-        AW_TRY(S->cg_zero.alloc(nc0));
+        AW_TRY(S->cg_r.ensure(nc0));
+        AW_TRY(S->cg_d.ensure(nc0));
+        AW_TRY(S->cg_q.ensure(nc0));
+        AW_TRY(S->cg_sc.ensure(4));
+        AW_TRY(S->cg_zero.ensure(nc0));
         AW_CUDA(cudaMemset(S->cg_zero.p, 0, nc0 * sizeof(float)));
         AW_CUDA(cudaMemset(S->cg_d.p, 0, nc0 * sizeof(double)));
     }
-    if (d->precision == AW_PRECISION_FP32_PCG) {
+    if (S->d.precision == AW_PRECISION_FP32_PCG) {
         const size_t nc0 = S->lv[0].ncell();
-        AW_TRY(S->cg32_d.alloc(std::max<size_t>(nc0, 1)));
-        AW_TRY(S->cg32_q.alloc(std::max<size_t>(nc0, 1)));
-        AW_TRY(S->cg32_sc.alloc(4));
-        AW_TRY(S->cg_zero.alloc(std::max<size_t>(nc0, 1)));
-        AW_TRY(S->partials32.alloc(4096));
+        AW_TRY(S->cg32_d.ensure(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->cg32_q.ensure(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->cg32_sc.ensure(4));
+        AW_TRY(S->cg_zero.ensure(std::max<size_t>(nc0, 1)));
+        AW_TRY(S->partials32.ensure(4096));
         AW_CUDA(cudaMemset(S->cg_zero.p, 0, std::max<size_t>(nc0, 1) * sizeof(float)));
         AW_CUDA(cudaMemset(S->cg32_d.p, 0, std::max<size_t>(nc0, 1) * sizeof(float)));
     }
     size_t nparts = (size_t)nb + 1024;
-    AW_TRY(S->partials.alloc(nparts));
-    AW_TRY(S->norm.alloc(2));
+    AW_TRY(S->partials.ensure(nparts));
+    AW_TRY(S->norm.ensure(2));
     S->use_graph = getenv("AW_NO_GRAPH") == nullptr;
     AW_CUDA(cudaDeviceSynchronize());
+    return AW_OK;
+}
+
+namespace aw {
+aw_status solver_relayout(aw_solver* S) {
+    AW_CHECK_ARG(S && S->g && S->g->st.allocated, "grid not allocated");
+    AW_TRY(check_grading(S->g->st));
+    AW_TRY(solver_build(S));
+    return aw_solver_setup(S, nullptr, 0);
+}
+}  // namespace aw
+
+extern "C" aw_status aw_solver_create(aw_msbg* g, const aw_solver_desc* d, aw_solver** out) {
+    AW_CHECK_ARG(g && d && out, "null argument");
+    AW_CHECK_ARG(g->st.allocated, "grid not allocated");
+    AW_CHECK_ARG(d->operator_mode == AW_OPERATOR_FV || d->operator_mode == AW_OPERATOR_REFERENCE, "bad operator mode");
+    AW_CHECK_ARG(d->precision == AW_PRECISION_FP32 || d->precision == AW_PRECISION_MIXED ||
+                     d->precision == AW_PRECISION_FP32_PCG,
+                 "bad precision");
+    AW_CHECK_ARG(d->block_iterations >= 1 && d->pre_smooth >= 0 && d->post_smooth >= 0, "bad smoother settings");
+    *out = nullptr;
+    MsbgState& G = g->st;
+    AW_TRY(check_grading(G));
+    std::unique_ptr<aw_solver> S(new aw_solver());
+    S->g = g;
+    S->d = *d;
+    AW_TRY(solver_build(S.get()));
     *out = S.release();
     // default setup: every cell fluid
     return aw_solver_setup(*out, nullptr, 0);

@@ -517,7 +517,8 @@ def resample_bench(g, aw, dims=(256, 256, 256), reps=10, warmup=3):
 def rebuild_bench(steps=20, warmup=3):
     """dam_drop_128 with the level map re-derived from the particles after every FLIP step
     (aw_flip_rebuild_levels): host wall time of the rebuild when the map is unchanged (map, grading
-    and comparison on the device, one read-back) and when it changed (new layout and solver)."""
+    and comparison on the device, one read-back) and when it changed (new layout; channels, tiles
+    and solver hierarchy rebuilt in the storage they hold), and of the FLIP step that follows each."""
     import torch
     import anitowave_adaptive_b200 as aw
     from anitowave_adaptive_b200 import scenes
@@ -527,19 +528,24 @@ def rebuild_bench(steps=20, warmup=3):
                 max_cycles=100)
     for _ in range(warmup):
         F.step()
-    same, new = [], []
+    same, new, step_same, step_new = [], [], [], []
+    changed = False
     for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         F.step()
         torch.cuda.synchronize()
+        (step_new if changed else step_same).append(1e3 * (time.perf_counter() - t0))
         t0 = time.perf_counter()
         changed = F.rebuild_levels(S.thresholds)
         dt = 1e3 * (time.perf_counter() - t0)
         (new if changed else same).append(dt)
     F.close()
     g.close()
+    med = lambda v: float(np.median(v)) if v else None  # noqa: E731
     return {"workload": WORKLOAD, "steps": steps, "layout_changes": len(new),
-            "ms_unchanged": float(np.median(same)) if same else None,
-            "ms_changed": float(np.median(new)) if new else None}
+            "ms_unchanged": med(same), "ms_changed": med(new),
+            "ms_step_after_unchanged": med(step_same), "ms_step_after_changed": med(step_new)}
 
 
 def two_phase_bench(steps=10, warmup=3, rho=(1.0, 3.0)):
