@@ -569,11 +569,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                 for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
                     const int d = __ffs(mm) - 1;
                     const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                    const int reach = nres[d] < r ? 2 : 1;
+                    const float reach = nres[d] < r ? 2.f : 0.5f;
                     bool nr = true;
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
-                        nr = nr && (dd[a] == 0 || (dd[a] < 0 ? cc[a] <= reach : cc[a] >= r - 1 - reach));
+                        nr = nr && (dd[a] == 0 || (dd[a] < 0 ? (float)cc[a] < reach + 0.5f
+                                                             : (float)cc[a] > (float)(r - 1) - reach - 0.5f));
                     if (nr) cm |= 1u << d;
                 }
                 if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
@@ -752,10 +753,12 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
     // at a time, one pair per lane, instead of one divergent pass per neighbour direction.
     // Blocks of up to 8^3 cells visit only the particles of cells near a side that faces a
-    // neighbour at another resolution, and test only those directions.  A cell qualifies for
-    // direction d when, on every axis d crosses, it lies within reach + 1 cells of that side
-    // (reach: two of b's cells towards a coarser neighbour, one towards a finer; the extra cell
-    // covers the rounding between a particle's key cell and its position in cell units).
+    // neighbour at another resolution, and test only those directions.  The reach is one of the
+    // neighbour's cells: two of b's cells towards a coarser neighbour, half of one towards a finer
+    // (its faces across the side sit half a fine cell in).  A cell qualifies for direction d when,
+    // on every axis d crosses, its particles can lie within reach of that side; the half-cell margin
+    // covers the rounding between a particle's key cell and its position in cell units.  A particle
+    // that the exact test drops by rounding has weight (1 - d^2)^3 with d^2 within 1e-7 of 1.
     const int nn = listed ? nnear : 0;
     const uint32_t T = listed ? (xmask ? nl_pre[nn] : 0u) : p1 - p0;
     const uint32_t Ls = (T + 31) / 32;
@@ -782,13 +785,14 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
 #pragma unroll
             for (int k = 0; k < 3; ++k) q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
         }
-        // neighbours at another resolution within reach (up to two of b's cells for a coarser one)
+        // neighbours at another resolution within reach (two of b's cells for a coarser one, half a
+        // cell for a finer one)
         uint32_t near = 0;
         if (valid) {
             for (uint32_t mm = dirs; mm; mm &= mm - 1) {
                 const int d = __ffs(mm) - 1;
                 const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                const float reach = nres[d] < r ? 2.f : 1.f;
+                const float reach = nres[d] < r ? 2.f : 0.5f;
                 bool nr = true;
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
