@@ -345,12 +345,13 @@ __global__ void k_cell_count(const uint32_t* __restrict__ cstart, uint32_t nc, f
 // absolute rounding error is amplified by u = P/m on the low-mass faces at the fluid's edge.)
 //
 // The flush adds every nonzero tile entry into each copy of that physical face held by a block of
-// b's resolution (a face on a block boundary has one copy per side).  Faces of
-// neighbours at another resolution are at other positions: particles within reach of such a
-// neighbour add their weights in the neighbour's own lattice with global float atomics.  Those
-// (particle, neighbour) pairs are queued per warp and run one pair per lane, so a warp does not
-// pass over every neighbour direction with most lanes idle.  A second kernel normalises
-// u = P / m.  The face arrays must start at zero.
+// b's resolution (a face on a block boundary has one copy per side).  Faces of neighbours at
+// another resolution are at other positions.  Those of a coarser neighbour (half b's resolution)
+// lie in a second, coarse tile around b, filled by per-cell register sums like the own tile and
+// flushed the same way.  Particles within reach of a finer neighbour add their weights in the
+// neighbour's own lattice with global float atomics; those (particle, neighbour) pairs are queued
+// per warp and run one pair per lane, so a warp does not pass over every neighbour direction with
+// most lanes idle.  A second kernel normalises u = P / m.  The face arrays must start at zero.
 // ------------------------------------------------------------------------------------------------
 __device__ inline int floordiv(int a, int b) { return a >= 0 ? a / b : -((-a + b - 1) / b); }
 
@@ -436,6 +437,54 @@ __device__ __forceinline__ void p2g_cross_pair(const CrossNb* xn, const int* nre
     p2g_cross<PH>(xn[d], nres[d], X, V, ph, acc);
 }
 
+// Adds every nonzero entry of a ghosted face tile of resolution rr around block cb (faces [0, rr]
+// along the axis, [-1, rr] across) into each copy of that face held by a block of resolution rr: a
+// face on a plane between two blocks along its axis has one copy per side.
+template <bool PH>
+__device__ __forceinline__ void p2g_flush_tile(const LevelView& L, const int cb[3], int rr, const float* tm,
+                                               const float* tp, const float* tq, const FaceAcc& acc) {
+    const Geo& g = L.g;
+    const int R1 = rr + 1, R2 = rr + 2;
+    const int TA = (int)tile_axis(rr);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
+            const float mv = tm[a * TA + rem];
+            if (mv == 0.f) continue;
+            const float pv = tp[a * TA + rem];
+            const float qv2 = PH ? tq[a * TA + rem] : 0.f;
+            const int iA = rem % R1;
+            const int i1 = (rem / R1) % R2 - 1;
+            const int i2 = rem / (R1 * R2) - 1;
+            const int B1 = cb[t1] + floordiv(i1, rr), B2 = cb[t2] + floordiv(i2, rr);
+            const int l1 = i1 - (B1 - cb[t1]) * rr, l2 = i2 - (B2 - cb[t2]) * rr;
+            const int nA = (iA == 0 || iA == rr) ? 2 : 1;
+            for (int k = 0; k < nA; ++k) {
+                int A, lA;
+                if (iA == 0) { A = cb[a] - 1 + k; lA = k == 0 ? rr : 0; }
+                else if (iA == rr) { A = cb[a] + k; lA = k == 0 ? rr : 0; }
+                else { A = cb[a]; lA = iA; }
+                int nc[3];
+                nc[a] = A;
+                nc[t1] = B1;
+                nc[t2] = B2;
+                if (!inside(g, nc)) continue;
+                const int nb = bidx(g, nc[0], nc[1], nc[2]);
+                if (L.res[nb] != rr) continue;
+                int f[3];
+                f[a] = lA;
+                f[t1] = l1;
+                f[t2] = l2;
+                const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], rr);
+                atomicAdd(&acc.m[a][fi], mv);
+                atomicAdd(&acc.P[a][fi], pv);
+                if (PH && qv2 != 0.f) atomicAdd(&acc.Phi[a][fi], qv2);
+            }
+        }
+    }
+}
+
 template <bool PH>
 __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
@@ -444,11 +493,11 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ CrossNb xn[27];
-    __shared__ int cross;
+    __shared__ int cross, coarse;
     __shared__ uint32_t maxcnt;
-    __shared__ int ccount[P2G_MAX_CELLS / 32];
-    __shared__ uint16_t clist[P2G_MAX_CELLS];
-    __shared__ int nonempty, nnear;
+    __shared__ int ccount[P2G_MAX_CELLS / 32], cocount[P2G_MAX_CELLS / 32];
+    __shared__ uint16_t clist[P2G_MAX_CELLS], colist[P2G_MAX_CELLS];
+    __shared__ int nonempty, nnear, ncoarse;
     // near-cell list of the cross-resolution pass (blocks of at most P2G_NEAR_CELLS cells)
     __shared__ uint16_t nl_cell[P2G_NEAR_CELLS];
     __shared__ uint32_t nl_mask[P2G_NEAR_CELLS], nl_pre[P2G_NEAR_CELLS + 1];
@@ -467,22 +516,35 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     bcoord(g, b, cb);
     const int R1 = r + 1, R2 = r + 2;
     const int TA = (int)tile_axis(r);
-    float* am = sm;           // 3 TA mass
-    float* ap = sm + 3 * TA;  // 3 TA momentum
-    float* aq = sm + 6 * TA;  // 3 TA phase (PH)
+    // The coarse tile: the faces of the lattice of half b's resolution around b, with the same
+    // ghost rows (faces [0, r/2] along the axis, [-1, r/2] across); its entries outside b hold the
+    // deposits into coarser neighbours.
+    const int rc = r >> 1;
+    const int TAc = rc ? (int)tile_axis(rc) : 0;
+    constexpr int NV = PH ? 3 : 2;  // mass, momentum (, phase) per face
+    float* am = sm;                   // 3 TA mass
+    float* ap = sm + 3 * TA;          // 3 TA momentum
+    float* aq = sm + 6 * TA;          // 3 TA phase (PH)
+    float* cm = sm + 3 * NV * TA;     // 3 TAc mass of the coarse tile
+    float* cp = cm + 3 * TAc;         // 3 TAc momentum
+    float* cq = cm + 6 * TAc;         // 3 TAc phase (PH)
     // Blocks of one or two cells per edge hold thousands of particles on a tile of 18 or 48 faces
-    // per axis: each warp then deposits into a private copy of the tile, and the copies are summed
+    // per axis: each warp then deposits into a private copy of the tiles, and the copies are summed
     // before the flush, so that warps do not contend for the same few addresses.
-    const int TW = (PH ? 9 : 6) * TA;
+    const int TW = 3 * NV * (TA + TAc);
     const bool priv = r <= 2 && (int)(blockDim.x >> 5) * TW <= smem_floats;
     const int ntile = priv ? (int)(blockDim.x >> 5) * TW : TW;
     float* tw = priv ? sm + (threadIdx.x >> 5) * TW : sm;
     float* amw = tw;
     float* apw = tw + 3 * TA;
     float* aqw = tw + 6 * TA;
+    float* cmw = tw + 3 * NV * TA;
+    float* cpw = cmw + 3 * TAc;
+    float* cqw = cmw + 6 * TAc;
     for (int i = threadIdx.x; i < ntile; i += blockDim.x) sm[i] = 0.f;
     if (threadIdx.x == 0) {
         cross = 0;
+        coarse = 0;
         maxcnt = 0;
     }
     __syncthreads();
@@ -492,7 +554,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         const int nb = inside(g, nc) ? bidx(g, nc[0], nc[1], nc[2]) : -1;
         const int rn = nb >= 0 ? L.res[nb] : 0;
         nres[d] = rn;
-        if (rn && rn != r) {
+        if (rn && 2 * rn == r) atomicOr(&coarse, 1 << d);
+        if (rn && rn != r && 2 * rn != r) {  // finer (or, in a map that is not 2:1 graded, coarser still)
             atomicOr(&cross, 1 << d);
             xn[d].invh = 1.f / fcell(g, rn);
 #pragma unroll
@@ -503,7 +566,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         }
     }
     __syncthreads();
-    const int xmask = cross;
+    const int xmask = cross;    // finer neighbours: (particle, neighbour) pairs
+    const int cmask = coarse;   // neighbours at half b's resolution: the coarse tile
     const float h = fcell(g, r);
     const float invh = 1.f / h;
     float o[3];
@@ -520,37 +584,71 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     // The block's non-empty cells, in cell order: tasks run over these only, so that lanes do not
     // idle on the air cells of a surface block.
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    // A cell is listed for the coarse tile too when it lies within two of b's cells (one coarse
+    // cell, the reach there) of a side towards a coarser neighbour, on every axis that neighbour's
+    // direction crosses.
+    auto coarse_near = [&](int c) {
+        const int cc[3] = {c % r, (c / r) % r, c / (r * r)};
+        for (uint32_t mm = (uint32_t)cmask; mm; mm &= mm - 1) {
+            const int d = __ffs(mm) - 1;
+            const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
+            bool nr = true;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) nr = nr && (dd[k] == 0 || (dd[k] < 0 ? cc[k] <= 1 : cc[k] >= r - 2));
+            if (nr) return true;
+        }
+        return false;
+    };
     const int nchunk = (nc3 + 31) / 32;
     for (int ch = wid; ch < nchunk; ch += nwarp) {
         const int c = ch * 32 + lane;
         const uint32_t cnt = c < nc3 ? cs[c0 + c + 1] - cs[c0 + c] : 0u;
         if (cnt > 0) atomicMax(&maxcnt, cnt);
         const unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
-        if (lane == 0) ccount[ch] = __popc(m);
+        const unsigned mc = __ballot_sync(0xffffffffu, cnt > 0 && cmask && coarse_near(c));
+        if (lane == 0) {
+            ccount[ch] = __popc(m);
+            cocount[ch] = __popc(mc);
+        }
     }
     __syncthreads();
-    if (wid == 0) {  // exclusive scan of the per-chunk counts
-        int carry = 0;
+    if (wid == 0) {  // exclusive scans of the per-chunk counts
+        int carry = 0, carry2 = 0;
         for (int base = 0; base < nchunk; base += 32) {
             const int ch = base + lane;
             const int v = ch < nchunk ? ccount[ch] : 0;
-            int incl = v;
+            const int v2 = ch < nchunk ? cocount[ch] : 0;
+            int incl = v, incl2 = v2;
 #pragma unroll
             for (int sh = 1; sh < 32; sh <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, incl, sh);
-                if (lane >= sh) incl += y;
+                const int y2 = __shfl_up_sync(0xffffffffu, incl2, sh);
+                if (lane >= sh) {
+                    incl += y;
+                    incl2 += y2;
+                }
             }
-            if (ch < nchunk) ccount[ch] = carry + incl - v;
+            if (ch < nchunk) {
+                ccount[ch] = carry + incl - v;
+                cocount[ch] = carry2 + incl2 - v2;
+            }
             carry += __shfl_sync(0xffffffffu, incl, 31);
+            carry2 += __shfl_sync(0xffffffffu, incl2, 31);
         }
-        if (lane == 0) nonempty = carry;
+        if (lane == 0) {
+            nonempty = carry;
+            ncoarse = carry2;
+        }
     }
     __syncthreads();
     for (int ch = wid; ch < nchunk; ch += nwarp) {
         const int c = ch * 32 + lane;
         const bool ne = c < nc3 && cs[c0 + c + 1] > cs[c0 + c];
+        const bool cn = ne && cmask && coarse_near(c);
         const unsigned m = __ballot_sync(0xffffffffu, ne);
+        const unsigned mc = __ballot_sync(0xffffffffu, cn);
         if (ne) clist[ccount[ch] + __popc(m & ((1u << lane) - 1u))] = (uint16_t)c;
+        if (cn) colist[cocount[ch] + __popc(mc & ((1u << lane) - 1u))] = (uint16_t)c;
     }
     __syncthreads();
     const int ncell = nonempty;
@@ -569,7 +667,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                 for (uint32_t mm = (uint32_t)xmask; mm; mm &= mm - 1) {
                     const int d = __ffs(mm) - 1;
                     const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                    const float reach = nres[d] < r ? 2.f : 0.5f;
+                    const float reach = (float)r / (float)nres[d];
                     bool nr = true;
 #pragma unroll
                     for (int a = 0; a < 3; ++a)
@@ -749,16 +847,110 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                     }
                 }
     }
-    // Cross-resolution pairs: lanes of a warp take particles a 32nd of the range apart, and the
-    // (particle, neighbour) pairs bound for another resolution wait in a per-warp queue and run 32
-    // at a time, one pair per lane, instead of one divergent pass per neighbour direction.
-    // Blocks of up to 8^3 cells visit only the particles of cells near a side that faces a
-    // neighbour at another resolution, and test only those directions.  The reach is one of the
-    // neighbour's cells: two of b's cells towards a coarser neighbour, half of one towards a finer
-    // (its faces across the side sit half a fine cell in).  A cell qualifies for direction d when,
-    // on every axis d crosses, its particles can lie within reach of that side; the half-cell margin
-    // covers the rounding between a particle's key cell and its position in cell units.  A particle
-    // that the exact test drops by rounding has weight (1 - d^2)^3 with d^2 within 1e-7 of 1.
+    // Coarser neighbours.  A coarser neighbour's lattice continues the lattice of half b's
+    // resolution anchored at b's origin (every block spans the same length), so its faces within
+    // reach of b's particles are entries of the coarse tile outside b.  One of b's cells lies inside
+    // half of one coarse cell along every axis, so the faces its particles can reach in that lattice
+    // are the same 2 x 2 x 2 for all of them: along a the faces below and above the coarse cell,
+    // across it the two face rows on the cell's own side.  A task (kind, listed cell, slice) sums
+    // their weights in registers as the own tasks do and adds the sums of the candidates that belong
+    // to a coarser neighbour into the coarse tile.
+    const int nco = ncoarse;
+    const int ntask_c = NK * nco * nsl;
+    const float invhc = 0.5f * invh;
+    for (int task = threadIdx.x; task < ntask_c; task += blockDim.x) {
+        const int kind = task / (nco * nsl);
+        const int rem = task - kind * nco * nsl;
+        const bool qpass = PH && kind >= 3;
+        const int a = qpass ? kind - 3 : kind;
+        const int c = colist[rem % nco], sl = rem / nco;
+        const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+        if ((uint32_t)sl * slice >= ce - ca) continue;
+        const uint32_t i0 = ca + (uint32_t)sl * slice;
+        const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
+        const int t1 = a == 2 ? 0 : a + 1, t2 = a == 0 ? 2 : a - 1;
+        const int cx = c % r, cy = (c / r) % r, cz = c / (r * r);
+        const int ka = a == 0 ? cx : (a == 1 ? cy : cz);
+        const int k1 = a == 0 ? cy : (a == 1 ? cz : cx);
+        const int k2 = a == 0 ? cz : (a == 1 ? cx : cy);
+        // candidates (ia + da, j1 + d1, j2 + d2): coarse face index along a, coarse cell rows across
+        const int ia = ka >> 1, j1 = ((k1 + 1) >> 1) - 1, j2 = ((k2 + 1) >> 1) - 1;
+        // the candidates that lie in a coarser neighbour; a face on a plane between two blocks
+        // along a belongs to both
+        uint32_t live = 0;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int fa = ia + (e >> 2), f1 = j1 + ((e >> 1) & 1), f2 = j2 + (e & 1);
+            const int s1 = f1 < 0 ? -1 : (f1 >= rc ? 1 : 0), s2 = f2 < 0 ? -1 : (f2 >= rc ? 1 : 0);
+            const int sa0 = fa == 0 ? -1 : 0, sa1 = fa == rc ? 1 : 0;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                const int sa = q ? sa1 : sa0;
+                int dxyz[3];
+                dxyz[a] = sa;
+                dxyz[t1] = s1;
+                dxyz[t2] = s2;
+                const int d = (dxyz[0] + 1) + 3 * (dxyz[1] + 1) + 9 * (dxyz[2] + 1);
+                if ((sa | s1 | s2) != 0 && ((cmask >> d) & 1)) live |= 1u << e;
+            }
+        }
+        if (!live) continue;
+        const float oa = a == 0 ? o[0] : (a == 1 ? o[1] : o[2]);
+        const float o1 = t1 == 0 ? o[0] : (t1 == 1 ? o[1] : o[2]);
+        const float o2 = t2 == 0 ? o[0] : (t2 == 1 ? o[1] : o[2]);
+        const float fa0 = (float)ia, f10 = (float)j1 + 0.5f, f20 = (float)j2 + 0.5f;
+        float sw[8], sv[8];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            sw[e] = 0.f;
+            sv[e] = 0.f;
+        }
+        for (uint32_t i = i0; i < i1; ++i) {
+            float val;
+            if (qpass) {
+                val = phase[pid[i]];
+                if (val == 0.f) continue;
+            } else {
+                val = soa[(int64_t)(3 + a) * n + i];
+            }
+            const float dA = (soa[(int64_t)a * n + i] - oa) * invhc - fa0;
+            const float dB = (soa[(int64_t)t1 * n + i] - o1) * invhc - f10;
+            const float dC = (soa[(int64_t)t2 * n + i] - o2) * invhc - f20;
+            const float A[2] = {dA * dA, (dA - 1.f) * (dA - 1.f)};
+            const float B[2] = {dB * dB, (dB - 1.f) * (dB - 1.f)};
+            const float C[2] = {dC * dC, (dC - 1.f) * (dC - 1.f)};
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                float t = fmaxf(1.f - ((A[e >> 2] + B[(e >> 1) & 1]) + C[e & 1]), 0.f);
+                t = t * t * t;
+                sw[e] += t;
+                sv[e] += t * val;
+            }
+        }
+        const int Rc1 = rc + 1, Rc2 = rc + 2;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            if (!((live >> e) & 1) || sw[e] == 0.f) continue;
+            const int ei = a * TAc + (ia + (e >> 2)) + Rc1 * ((j1 + ((e >> 1) & 1) + 1) + Rc2 * (j2 + (e & 1) + 1));
+            if (qpass) {
+                atomicAdd(&cqw[ei], sv[e]);
+            } else {
+                atomicAdd(&cmw[ei], sw[e]);
+                atomicAdd(&cpw[ei], sv[e]);
+            }
+        }
+    }
+    // Finer neighbours: lanes of a warp take particles a 32nd of the range apart, and the
+    // (particle, neighbour) pairs bound for a finer neighbour wait in a per-warp queue and run 32 at
+    // a time, one pair per lane, with global atomics, instead of one divergent pass per neighbour
+    // direction.  Blocks of up to 8^3 cells visit only the particles of cells near a side that faces
+    // such a neighbour, and test only those directions.  The reach is one of the neighbour's cells:
+    // half of one of b's cells (its faces across the side sit half a fine cell in; a map that is not
+    // 2:1 graded sends a neighbour of a quarter of b's resolution here too, with a reach of four of
+    // b's cells).  A cell qualifies for direction d when, on every axis d crosses, its particles can
+    // lie within reach of that side; the half-cell margin covers the rounding between a particle's
+    // key cell and its position in cell units.  A particle that the exact test drops by rounding has
+    // weight (1 - d^2)^3 with d^2 within 1e-7 of 1.
     const int nn = listed ? nnear : 0;
     const uint32_t T = listed ? (xmask ? nl_pre[nn] : 0u) : p1 - p0;
     const uint32_t Ls = (T + 31) / 32;
@@ -785,14 +977,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
 #pragma unroll
             for (int k = 0; k < 3; ++k) q[k] = (soa[(int64_t)k * n + sidx] - o[k]) * invh;
         }
-        // neighbours at another resolution within reach (two of b's cells for a coarser one, half a
-        // cell for a finer one)
+        // queued neighbours within reach (half a cell for a finer one)
         uint32_t near = 0;
         if (valid) {
             for (uint32_t mm = dirs; mm; mm &= mm - 1) {
                 const int d = __ffs(mm) - 1;
                 const int dd[3] = {d % 3 - 1, (d / 3) % 3 - 1, d / 9 - 1};
-                const float reach = nres[d] < r ? 2.f : 0.5f;
+                const float reach = (float)r / (float)nres[d];
                 bool nr = true;
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
@@ -838,44 +1029,10 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         }
         __syncthreads();
     }
-    // flush: every nonzero tile entry into each same-resolution copy of its face
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
-        for (int rem = threadIdx.x; rem < TA; rem += blockDim.x) {
-            const float mv = am[a * TA + rem];
-            if (mv == 0.f) continue;
-            const float pv = ap[a * TA + rem];
-            const float qv2 = PH ? aq[a * TA + rem] : 0.f;
-            const int iA = rem % R1;
-            const int i1 = (rem / R1) % R2 - 1;
-            const int i2 = rem / (R1 * R2) - 1;
-            const int B1 = cb[t1] + floordiv(i1, r), B2 = cb[t2] + floordiv(i2, r);
-            const int l1 = i1 - (B1 - cb[t1]) * r, l2 = i2 - (B2 - cb[t2]) * r;
-            const int nA = (iA == 0 || iA == r) ? 2 : 1;
-            for (int k = 0; k < nA; ++k) {
-                int A, lA;
-                if (iA == 0) { A = cb[a] - 1 + k; lA = k == 0 ? r : 0; }
-                else if (iA == r) { A = cb[a] + k; lA = k == 0 ? r : 0; }
-                else { A = cb[a]; lA = iA; }
-                int nc[3];
-                nc[a] = A;
-                nc[t1] = B1;
-                nc[t2] = B2;
-                if (!inside(g, nc)) continue;
-                const int nb = bidx(g, nc[0], nc[1], nc[2]);
-                if (L.res[nb] != r) continue;
-                int f[3];
-                f[a] = lA;
-                f[t1] = l1;
-                f[t2] = l2;
-                const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], r);
-                atomicAdd(&acc.m[a][fi], mv);
-                atomicAdd(&acc.P[a][fi], pv);
-                if (PH && qv2 != 0.f) atomicAdd(&acc.Phi[a][fi], qv2);
-            }
-        }
-    }
+    // flush: every nonzero entry of the own tile into each copy of its face held by a block of b's
+    // resolution, and of the coarse tile into each copy held by a block of half b's resolution
+    p2g_flush_tile<PH>(L, cb, r, am, ap, aq, acc);
+    if (cmask) p2g_flush_tile<PH>(L, cb, rc, cm, cp, cq, acc);
 }
 
 // u = P / m where m > 1e-6, else 0 (normalizeVelocity, P2G.cuh:139-171), over the three axes
@@ -948,8 +1105,9 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     // tile of 18 faces per axis, and more threads on it contend more (the 4-level dam_drop2_256
     // takes 2.96 ms with 512 against 2.85 ms with 256).
     const int nthreads = minres >= 2 ? P2G_THREADS : 256;
-    const size_t smem_f = std::max((size_t)NVt * tile_axis(maxres),
-                                   minres <= 2 ? (size_t)(nthreads / 32) * NVt * tile_axis(std::min(maxres, 2)) : 0);
+    // own tile and coarse tile (half the resolution) of one block
+    auto tiles = [&](int r) { return (size_t)NVt * (tile_axis(r) + (r >= 2 ? tile_axis(r / 2) : 0u)); };
+    const size_t smem_f = std::max(tiles(maxres), minres <= 2 ? (size_t)(nthreads / 32) * tiles(std::min(maxres, 2)) : 0);
     const size_t smem = smem_f * sizeof(float);
     if (n > 0) {
         if (ph) {
