@@ -739,11 +739,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     constexpr int NK = PH ? 6 : 3;
     const int ntask = NK * ncell * nsl;
     for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
-        const int kind = task / (ncell * nsl);
-        const int rem = task - kind * ncell * nsl;
+        // neighbouring threads take the kinds of one cell (they read the same particles, so one
+        // warp-wide load touches a third as many sectors), then neighbouring cells
+        const int kind = task % NK;
+        const int rem = task / NK;
         const bool qpass = PH && kind >= 3;
         const int a = qpass ? kind - 3 : kind;
-        const int c = clist[rem % ncell], sl = rem / ncell;  // neighbouring threads take neighbouring cells
+        const int c = clist[rem % ncell], sl = rem / ncell;
         const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
         if ((uint32_t)sl * slice >= ce - ca) continue;
         const uint32_t i0 = ca + (uint32_t)sl * slice;
@@ -859,8 +861,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     const int ntask_c = NK * nco * nsl;
     const float invhc = 0.5f * invh;
     for (int task = threadIdx.x; task < ntask_c; task += blockDim.x) {
-        const int kind = task / (nco * nsl);
-        const int rem = task - kind * nco * nsl;
+        const int kind = task % NK;
+        const int rem = task / NK;
         const bool qpass = PH && kind >= 3;
         const int a = qpass ? kind - 3 : kind;
         const int c = colist[rem % nco], sl = rem / nco;
