@@ -439,11 +439,12 @@ __device__ __forceinline__ void p2g_cross_pair(const CrossNb* xn, const int* nre
 
 // Adds every nonzero entry of a ghosted face tile of resolution rr around block cb (faces [0, rr]
 // along the axis, [-1, rr] across) into each copy of that face held by a block of resolution rr: a
-// face on a plane between two blocks along its axis has one copy per side.
+// face on a plane between two blocks along its axis has one copy per side.  nres / noff: the
+// resolution (0 outside the domain or inactive) and face offsets of the 27 blocks around cb,
+// direction d = (dx + 1) + 3 (dy + 1) + 9 (dz + 1).
 template <bool PH>
-__device__ __forceinline__ void p2g_flush_tile(const LevelView& L, const int cb[3], int rr, const float* tm,
+__device__ __forceinline__ void p2g_flush_tile(const int* nres, const uint32_t (*noff)[3], int rr, const float* tm,
                                                const float* tp, const float* tq, const FaceAcc& acc) {
-    const Geo& g = L.g;
     const int R1 = rr + 1, R2 = rr + 2;
     const int TA = (int)tile_axis(rr);
 #pragma unroll
@@ -457,26 +458,25 @@ __device__ __forceinline__ void p2g_flush_tile(const LevelView& L, const int cb[
             const int iA = rem % R1;
             const int i1 = (rem / R1) % R2 - 1;
             const int i2 = rem / (R1 * R2) - 1;
-            const int B1 = cb[t1] + floordiv(i1, rr), B2 = cb[t2] + floordiv(i2, rr);
-            const int l1 = i1 - (B1 - cb[t1]) * rr, l2 = i2 - (B2 - cb[t2]) * rr;
+            const int s1 = i1 < 0 ? -1 : (i1 >= rr ? 1 : 0), s2 = i2 < 0 ? -1 : (i2 >= rr ? 1 : 0);
+            const int l1 = i1 - s1 * rr, l2 = i2 - s2 * rr;
             const int nA = (iA == 0 || iA == rr) ? 2 : 1;
             for (int k = 0; k < nA; ++k) {
-                int A, lA;
-                if (iA == 0) { A = cb[a] - 1 + k; lA = k == 0 ? rr : 0; }
-                else if (iA == rr) { A = cb[a] + k; lA = k == 0 ? rr : 0; }
-                else { A = cb[a]; lA = iA; }
-                int nc[3];
-                nc[a] = A;
-                nc[t1] = B1;
-                nc[t2] = B2;
-                if (!inside(g, nc)) continue;
-                const int nb = bidx(g, nc[0], nc[1], nc[2]);
-                if (L.res[nb] != rr) continue;
+                int sA, lA;
+                if (iA == 0) { sA = k - 1; lA = k == 0 ? rr : 0; }
+                else if (iA == rr) { sA = k; lA = k == 0 ? rr : 0; }
+                else { sA = 0; lA = iA; }
+                int sd[3];
+                sd[a] = sA;
+                sd[t1] = s1;
+                sd[t2] = s2;
+                const int d = (sd[0] + 1) + 3 * (sd[1] + 1) + 9 * (sd[2] + 1);
+                if (nres[d] != rr) continue;
                 int f[3];
                 f[a] = lA;
                 f[t1] = l1;
                 f[t2] = l2;
-                const uint32_t fi = L.off[1 + a][nb] + fidx(a, f[0], f[1], f[2], rr);
+                const uint32_t fi = noff[d][a] + fidx(a, f[0], f[1], f[2], rr);
                 atomicAdd(&acc.m[a][fi], mv);
                 atomicAdd(&acc.P[a][fi], pv);
                 if (PH && qv2 != 0.f) atomicAdd(&acc.Phi[a][fi], qv2);
@@ -492,12 +492,14 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                                                  int smem_floats) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
+    __shared__ uint32_t noff[27][3];
     __shared__ CrossNb xn[27];
     __shared__ int cross, coarse;
     __shared__ uint32_t maxcnt;
     __shared__ int ccount[P2G_MAX_CELLS / 32], cocount[P2G_MAX_CELLS / 32];
     __shared__ uint16_t clist[P2G_MAX_CELLS], colist[P2G_MAX_CELLS];
     __shared__ int nonempty, nnear, ncoarse;
+    __shared__ int tctr[2];  // next own / coarse task to hand out
     // near-cell list of the cross-resolution pass (blocks of at most P2G_NEAR_CELLS cells)
     __shared__ uint16_t nl_cell[P2G_NEAR_CELLS];
     __shared__ uint32_t nl_mask[P2G_NEAR_CELLS], nl_pre[P2G_NEAR_CELLS + 1];
@@ -546,6 +548,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         cross = 0;
         coarse = 0;
         maxcnt = 0;
+        tctr[0] = 0;
+        tctr[1] = 0;
     }
     __syncthreads();
     if (threadIdx.x < 27) {
@@ -554,6 +558,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         const int nb = inside(g, nc) ? bidx(g, nc[0], nc[1], nc[2]) : -1;
         const int rn = nb >= 0 ? L.res[nb] : 0;
         nres[d] = rn;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) noff[d][k] = rn ? L.off[1 + k][nb] : 0u;
         if (rn && 2 * rn == r) atomicOr(&coarse, 1 << d);
         if (rn && rn != r && 2 * rn != r) {  // finer (or, in a map that is not 2:1 graded, coarser still)
             atomicOr(&cross, 1 << d);
@@ -738,7 +744,15 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     const uint32_t slice = nsl ? (mc + nsl - 1) / nsl : 0;
     constexpr int NK = PH ? 6 : 3;
     const int ntask = NK * ncell * nsl;
-    for (int task = threadIdx.x; task < ntask; task += blockDim.x) {
+    // Warps take 32 tasks at a time from a shared counter, so that warps whose tasks hold fewer
+    // particles take more of them.
+    for (;;) {
+        int tb = 0;
+        if (lane == 0) tb = atomicAdd(&tctr[0], 32);
+        tb = __shfl_sync(0xffffffffu, tb, 0);
+        if (tb >= ntask) break;
+        const int task = tb + lane;
+        if (task >= ntask) continue;
         // neighbouring threads take the kinds of one cell (they read the same particles, so one
         // warp-wide load touches a third as many sectors), then neighbouring cells
         const int kind = task % NK;
@@ -860,7 +874,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     const int nco = ncoarse;
     const int ntask_c = NK * nco * nsl;
     const float invhc = 0.5f * invh;
-    for (int task = threadIdx.x; task < ntask_c; task += blockDim.x) {
+    for (;;) {
+        int tb = 0;
+        if (lane == 0) tb = atomicAdd(&tctr[1], 32);
+        tb = __shfl_sync(0xffffffffu, tb, 0);
+        if (tb >= ntask_c) break;
+        const int task = tb + lane;
+        if (task >= ntask_c) continue;
         const int kind = task % NK;
         const int rem = task / NK;
         const bool qpass = PH && kind >= 3;
@@ -1033,8 +1053,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     }
     // flush: every nonzero entry of the own tile into each copy of its face held by a block of b's
     // resolution, and of the coarse tile into each copy held by a block of half b's resolution
-    p2g_flush_tile<PH>(L, cb, r, am, ap, aq, acc);
-    if (cmask) p2g_flush_tile<PH>(L, cb, rc, cm, cp, cq, acc);
+    p2g_flush_tile<PH>(nres, noff, r, am, ap, aq, acc);
+    if (cmask) p2g_flush_tile<PH>(nres, noff, rc, cm, cp, cq, acc);
 }
 
 // u = P / m where m > 1e-6, else 0 (normalizeVelocity, P2G.cuh:139-171), over the three axes
