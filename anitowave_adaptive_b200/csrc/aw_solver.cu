@@ -1149,13 +1149,49 @@ __global__ void k_dense_fluid(DenseView K, int from_msbg, LevelView F, const uin
     fc[t] = f;
 }
 
-__global__ void k_dense_conductance(DenseView K, int a, float H, float* W) {
+// 1/rho on the faces of axis a of a uniform level: the mean of the four faces it covers on the next
+// finer level, either the last block-structured level (one cell per block; a face is read from the
+// block above it along a, else from the block below, else taken as 1 when neither is active) or the
+// previous uniform level.
+__global__ void k_dense_bbar(DenseView K, int a, int from_msbg, LevelView F, const float* __restrict__ fb, DenseView Fd,
+                             float* __restrict__ bc) {
+    const int n = (K.D[0] + (a == 0)) * (K.D[1] + (a == 1)) * (K.D[2] + (a == 2));
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int dx = K.D[0] + (a == 0), dy = K.D[1] + (a == 1);
+    const int f[3] = {t % dx, (t / dx) % dy, t / (dx * dy)};
+    const int t1 = (a + 1) % 3, t2 = (a + 2) % 3;
+    float sum = 0.f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        int q[3];
+        q[a] = 2 * f[a];
+        q[t1] = 2 * f[t1] + (d & 1);
+        q[t2] = 2 * f[t2] + (d >> 1);
+        float v = 1.f;
+        if (from_msbg) {
+            int lo[3] = {q[0], q[1], q[2]};
+            lo[a] -= 1;
+            const int bh = inside(F.g, q) ? bidx(F.g, q[0], q[1], q[2]) : -1;
+            const int bl = inside(F.g, lo) ? bidx(F.g, lo[0], lo[1], lo[2]) : -1;
+            if (bh >= 0 && F.res[bh]) v = fb[F.off[1 + a][bh]];           // its low face
+            else if (bl >= 0 && F.res[bl]) v = fb[F.off[1 + a][bl] + 1];  // its high face
+        } else {
+            v = fb[dfidx(Fd, a, q[0], q[1], q[2])];
+        }
+        sum += v;
+    }
+    bc[t] = 0.25f * sum;
+}
+
+// conductance W = H * bbar on a uniform level, 0 on the domain walls
+__global__ void k_dense_conductance(DenseView K, int a, float H, const float* __restrict__ bbar, float* W) {
     int n = (K.D[0] + (a == 0)) * (K.D[1] + (a == 1)) * (K.D[2] + (a == 2));
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     int dx = K.D[0] + (a == 0), dy = K.D[1] + (a == 1);
     int f[3] = {t % dx, (t / dx) % dy, t / (dx * dy)};
-    W[t] = (f[a] == 0 || f[a] == K.D[a]) ? 0.f : H;
+    W[t] = (f[a] == 0 || f[a] == K.D[a]) ? 0.f : H * bbar[t];
 }
 
 // ------------------------------- coarsest FP64 dense solve ------------------------------------
@@ -1711,6 +1747,20 @@ static aw_status build_coefficients(aw_solver* S, cudaStream_t s) {
             }
         }
     }
+    // uniform levels below one cell per block (FV mode): 1/rho averaged down face by face, so that
+    // their operator follows the density of the finer levels
+    for (int m = S->nmsbg; m < (int)S->lv.size(); ++m) {
+        MGLevel& L = S->lv[m];
+        const MGLevel& P = S->lv[m - 1];
+        const bool from_msbg = m == S->nmsbg;
+        for (int a = 0; a < 3; ++a) {
+            k_dense_bbar<<<nblk(L.nface(a)), 256, 0, s>>>(dview(L), a, from_msbg ? 1 : 0, lview(S, m - 1),
+                                                           P.bbar[a].p, dview(P), L.bbar[a].p);
+            AW_LAUNCH();
+            k_dense_conductance<<<nblk(L.nface(a)), 256, 0, s>>>(dview(L), a, L.H, L.bbar[a].p, L.W[a].p);
+            AW_LAUNCH();
+        }
+    }
     return AW_OK;
 }
 
@@ -1836,8 +1886,6 @@ static aw_status solver_build(aw_solver* S) {
             S->smem_max64 = std::max(S->smem_max64, L.smem_x64);
         }
     }
-    // coefficients of the block-structured levels
-    AW_TRY(build_coefficients(S, 0));
     // uniform continuation below one cell per block (FV mode)
     size_t used = (size_t)S->nmsbg;
     if (!ref && S->nmsbg > 0 && S->lv[S->nmsbg - 1].maxres == 1) {
@@ -1860,8 +1908,7 @@ static aw_status solver_build(aw_solver* S) {
             AW_CUDA(cudaMemset(L.b.p, 0, nc * sizeof(float)));
             for (int a = 0; a < 3; ++a) {
                 AW_TRY(L.W[a].ensure(L.nface(a)));
-                k_dense_conductance<<<nblk(L.nface(a)), 256>>>(dview(L), a, H, L.W[a].p);
-                AW_LAUNCH();
+                AW_TRY(L.bbar[a].ensure(L.nface(a)));
             }
             for (int a = 0; a < 3; ++a) Dd[a] /= 2;
         }
@@ -1882,6 +1929,8 @@ static aw_status solver_build(aw_solver* S) {
         }
     }
     S->lv.resize(used);
+    // coefficients of every level
+    AW_TRY(build_coefficients(S, 0));
     {  // always opted in: static shared memory (k_smooth's per-slot state) counts against the default 48 KB too
         AW_CUDA(cudaFuncSetAttribute(k_smooth, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
         AW_CUDA(cudaFuncSetAttribute(k_residual<SrcX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
