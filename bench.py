@@ -334,8 +334,8 @@ def run_ours(args, ws, rank, local):
                      "unit": "GB/s", "frac": p2g_gbs / hbm, "peak_kind": peak_kind,
                      "traffic": traffic.get("k_p2g_own"), "bytes_per_launch": p2g_bytes, "ms_per_launch": p2g_ms,
                      "note": "HBM is the roofline; the kernel runs below it, limited by instruction issue and "
-                             "load latency (weight arithmetic of the per-cell deposit and the cross-resolution "
-                             "pairs), see profiles/k_p2g_own_dam_drop_128.md"},
+                             "particle-load latency in the per-cell register deposits (own and coarse tiles), "
+                             "see profiles/k_p2g_own_dam_drop_128.md"},
         "roofline_g2p": {"kernel": "k_g2p_fused (+ k_g2p_inactive)", "bound": "hbm", "achieved": g2p_gbs, "peak": hbm,
                          "unit": "GB/s", "frac": g2p_gbs / hbm, "traffic": traffic.get("k_g2p_fused"),
                          "bytes_per_launch": g2p_bytes, "ms_per_launch": g2p_ms},
