@@ -514,6 +514,8 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
     if (p0 == p1) return;
     const Geo& g = L.g;
+    // the block's cell starts in the sorted array, after the tiles (smem_floats floats)
+    uint32_t* cst = reinterpret_cast<uint32_t*>(sm + smem_floats);
     int cb[3];
     bcoord(g, b, cb);
     const int R1 = r + 1, R2 = r + 2;
@@ -608,7 +610,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     const int nchunk = (nc3 + 31) / 32;
     for (int ch = wid; ch < nchunk; ch += nwarp) {
         const int c = ch * 32 + lane;
-        const uint32_t cnt = c < nc3 ? cs[c0 + c + 1] - cs[c0 + c] : 0u;
+        uint32_t cnt = 0;
+        if (c < nc3) {
+            const uint32_t a0 = cs[c0 + c], a1 = cs[c0 + c + 1];
+            cst[c] = a0;
+            if (c == nc3 - 1) cst[nc3] = a1;
+            cnt = a1 - a0;
+        }
         if (cnt > 0) atomicMax(&maxcnt, cnt);
         const unsigned m = __ballot_sync(0xffffffffu, cnt > 0);
         const unsigned mc = __ballot_sync(0xffffffffu, cnt > 0 && cmask && coarse_near(c));
@@ -649,7 +657,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __syncthreads();
     for (int ch = wid; ch < nchunk; ch += nwarp) {
         const int c = ch * 32 + lane;
-        const bool ne = c < nc3 && cs[c0 + c + 1] > cs[c0 + c];
+        const bool ne = c < nc3 && cst[c + 1] > cst[c];
         const bool cn = ne && cmask && coarse_near(c);
         const unsigned m = __ballot_sync(0xffffffffu, ne);
         const unsigned mc = __ballot_sync(0xffffffffu, cn);
@@ -681,7 +689,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                                                              : (float)cc[a] > (float)(r - 1) - reach - 0.5f));
                     if (nr) cm |= 1u << d;
                 }
-                if (cm) cnt = (int)(cs[c0 + c + 1] - cs[c0 + c]);
+                if (cm) cnt = (int)(cst[c + 1] - cst[c]);
             }
             const unsigned bal = __ballot_sync(0xffffffffu, cm != 0);
             if (lane == 0) ccount[ch] = __popc(bal);
@@ -760,7 +768,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         const bool qpass = PH && kind >= 3;
         const int a = qpass ? kind - 3 : kind;
         const int c = clist[rem % ncell], sl = rem / ncell;
-        const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+        const uint32_t ca = cst[c], ce = cst[c + 1];
         if ((uint32_t)sl * slice >= ce - ca) continue;
         const uint32_t i0 = ca + (uint32_t)sl * slice;
         const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
@@ -886,7 +894,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
         const bool qpass = PH && kind >= 3;
         const int a = qpass ? kind - 3 : kind;
         const int c = colist[rem % nco], sl = rem / nco;
-        const uint32_t ca = cs[c0 + c], ce = cs[c0 + c + 1];
+        const uint32_t ca = cst[c], ce = cst[c + 1];
         if ((uint32_t)sl * slice >= ce - ca) continue;
         const uint32_t i0 = ca + (uint32_t)sl * slice;
         const uint32_t i1 = ce - i0 > slice ? i0 + slice : ce;
@@ -990,7 +998,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
                 if (nl_pre[mid] <= f) lo = mid;
                 else hi = mid - 1;
             }
-            v = cs[c0 + nl_cell[lo]] - p0 + (f - nl_pre[lo]);
+            v = cst[nl_cell[lo]] - p0 + (f - nl_pre[lo]);
             dirs = nl_mask[lo];
         }
         float q[3];
@@ -1130,7 +1138,8 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
     // own tile and coarse tile (half the resolution) of one block
     auto tiles = [&](int r) { return (size_t)NVt * (tile_axis(r) + (r >= 2 ? tile_axis(r / 2) : 0u)); };
     const size_t smem_f = std::max(tiles(maxres), minres <= 2 ? (size_t)(nthreads / 32) * tiles(std::min(maxres, 2)) : 0);
-    const size_t smem = smem_f * sizeof(float);
+    // then the cell starts of the largest block
+    const size_t smem = (smem_f + (((size_t)maxres * maxres * maxres + 1 + 3) & ~(size_t)3)) * sizeof(float);
     if (n > 0) {
         if (ph) {
             // always opted in: the pair queues' static shared memory counts against the default 48 KB too
