@@ -94,6 +94,7 @@ struct aw_solver {
     const void* cycle_b0 = nullptr;
     unsigned long long cycle_kernels = 0;
     bool use_graph = true;
+    bool use_pdl = true;  // V-cycle kernels as programmatic dependent launches
     double* h_norm = nullptr;  // pinned host word for the per-iteration residual norm
     ~aw_solver() {
         if (cycle) cudaGraphExecDestroy(cycle);
@@ -197,6 +198,13 @@ __device__ inline void cp_async8(void* s, const void* g) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_addr(s)), "l"(g) : "memory");
 }
 __device__ inline void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+// Programmatic dependent launch: the V-cycle's kernels are launched so that each may start while its
+// predecessor drains.  A kernel reads what its predecessor wrote only after pdl_wait() (which returns
+// once the predecessor grid has completed and its memory is visible; at once for a kernel launched
+// without the attribute), and lets its successor start with pdl_trigger() once its own main work is
+// issued.  Descriptors and slot metadata (fixed at solver build) are staged before the wait.
+__device__ inline void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ inline void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
 
 // Sources of x for staging: FP32 (copied asynchronously), FP16 + per-block scale (decoded in
 // registers), FP64 (copied asynchronously).
@@ -492,9 +500,11 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
     constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
     SlotImage<float, R> S(smraw, d.y);
     const int G = S.G;
+    if (status) pdl_wait();  // the activation flags come from the previous sweep
     stage_meta<R>(S.meta, G, B, d.x, status);
     const int* sb = S.meta + MF_BLOCK * G;
     if (!__syncthreads_or(threadIdx.x < G && sb[threadIdx.x] >= 0)) return;
+    pdl_wait();
     for (int t = threadIdx.x; t < G; t += NT) {
         Z.smr[t] = 0;
         Z.sdone[t] = 0;
@@ -577,6 +587,7 @@ __device__ inline void smooth_body(int4 d, unsigned char* smraw, SmoothShared& Z
         if (!__syncthreads_or(more)) break;
     }
     __syncthreads();
+    pdl_trigger();
     store_slots<R>(x, sb, S.meta + MF_OFF * G, G, S.xs, Z.sdone);  // sdone reused as per-slot |x| max
     if (!status_next) return;
     for (int t = threadIdx.x; t < G; t += NT) {
@@ -618,8 +629,10 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
     SlotImage<T, R> S(smraw, d.y);
     const int G = S.G;
     stage_meta<R>(S.meta, G, B, d.x, nullptr);
+    pdl_wait();
     stage_data<R>(S, x, bvec, W, check_fluid ? fluid : nullptr);
     __syncthreads();
+    pdl_trigger();
     double acc = 0.0;
 #pragma unroll
     for (int t0 = 0; t0 < GM * n3; t0 += NT) {
@@ -678,6 +691,8 @@ __device__ inline void restrict_body(int4 d, unsigned char* smraw, const float* 
     const int G = d.y;
     int* meta = (int*)smraw;
     stage_meta<R>(meta, G, B, d.x, nullptr);
+    pdl_wait();
+    pdl_trigger();
     const MetaView S{meta, G};
 #pragma unroll
     for (int base = 0; base < GM * n3; base += K * NT) {
@@ -741,6 +756,8 @@ __device__ inline void prolong_body(int4 d, unsigned char* smraw, int* smax, con
     float* xs = (float*)smraw;
     int* meta = (int*)(xs + (xf.f ? 0 : G * Gm::X3));
     stage_meta<R>(meta, G, B, d.x, nullptr);
+    pdl_wait();
+    pdl_trigger();
     const MetaView S{meta, G};
 #pragma unroll
     for (int base = 0; base < GM * n3; base += K * NT) {
@@ -960,6 +977,7 @@ __device__ inline float dense_Ax(const DenseArgs& A, const float* x, int i, int 
 }
 
 __global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ b, int col, float omega) {
+    pdl_wait();
     const DenseView& d = A.d;
     int n = d.D[0] * d.D[1] * d.D[2];
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -973,6 +991,7 @@ __global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ 
 }
 
 __global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const float* __restrict__ b, float* r) {
+    pdl_wait();
     const DenseView& d = A.d;
     int n = d.D[0] * d.D[1] * d.D[2];
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -985,6 +1004,7 @@ __global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const
 // restriction into a dense level from the one-cell-per-block MSBG level (first) or a dense level
 __global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_c, float* __restrict__ bc, int from_msbg,
                                  LevelView F, DenseView Fd, const float* __restrict__ rf) {
+    pdl_wait();
     int n = K.D[0] * K.D[1] * K.D[2];
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
@@ -1006,6 +1026,7 @@ __global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_
 
 __global__ void k_dense_prolong(DenseView K, const float* __restrict__ xc, int to_msbg, LevelView F, XStore xf_msbg,
                                 DenseView Fd, float* __restrict__ xf, const uint8_t* __restrict__ fluid_f) {
+    pdl_wait();
     int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (to_msbg) {
         if (t >= F.g.nb) return;
@@ -1368,6 +1389,7 @@ __global__ void __launch_bounds__(512) k_coarse_factor(Uniform U, int* pos_of, i
 // x = Minv b on the fluid cells of the coarsest level (FP64 accumulation)
 __global__ void k_coarse_apply(Uniform U, const int* __restrict__ idx, const int* __restrict__ ex_n,
                                const double* __restrict__ Minv, const float* __restrict__ b, float* __restrict__ x) {
+    pdl_wait();
     const int n = ex_n[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         double s = 0.0;
@@ -1529,6 +1551,26 @@ static Uniform uniform_of(aw_solver* S, int m) {
     return U;
 }
 
+// A V-cycle kernel launch, as a programmatic dependent of the kernel before it in the stream (the
+// kernels call pdl_wait before reading what it wrote).
+template <typename... KArgs, typename... Args>
+static aw_status launch_dep(const aw_solver* S, void (*k)(KArgs...), unsigned grid, unsigned block, size_t smem,
+                            cudaStream_t s, Args&&... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = S->use_pdl ? 1 : 0;
+    AW_CUDA(cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...));
+    AW_LAUNCH();
+    return AW_OK;
+}
+
 static aw_status zero_x(aw_solver* S, int m, cudaStream_t s) {
     MGLevel& L = S->lv[m];
     if (L.half) {
@@ -1554,8 +1596,8 @@ static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t 
         size_t n = L.ncell();
         for (int it = 0; it < iterations; ++it)
             for (int k = 0; k < 2; ++k) {
-                k_dense_smooth<<<nblk(n), 256, 0, s>>>(A, L.x.p, L.b.p, rev ? 1 - k : k, S->d.omega);
-                AW_LAUNCH();
+                AW_TRY(launch_dep(S, k_dense_smooth, nblk(n), 256, 0, s, A, L.x.p, (const float*)L.b.p, rev ? 1 - k : k,
+                                  S->d.omega));
             }
         return AW_OK;
     }
@@ -1572,10 +1614,9 @@ static aw_status smooth_level(aw_solver* S, int m, int iterations, cudaStream_t 
         for (int k = 0; k < 2; ++k) {
             const int rb = rev ? 1 - k : k;
             if (!L.ndesc[rb]) continue;
-            k_smooth<<<L.ndesc[rb], 256, L.smem_smooth, s>>>(V, x, bptr(S, m), coef(L), L.fluid.p, batch(L, rb),
-                                                              act ? L.status[cur].p : nullptr,
-                                                              act ? L.status[cur ^ 1].p : nullptr, P);
-            AW_LAUNCH();
+            AW_TRY(launch_dep(S, k_smooth, (unsigned)L.ndesc[rb], 256, L.smem_smooth, s, V, x, bptr(S, m), coef(L),
+                              (const uint8_t*)L.fluid.p, batch(L, rb),
+                              (const uint8_t*)(act ? L.status[cur].p : nullptr), act ? L.status[cur ^ 1].p : nullptr, P));
         }
         cur ^= 1;
     }
@@ -1587,15 +1628,13 @@ static aw_status residual_level(aw_solver* S, int m, double* part, cudaStream_t 
     const int cf = fv(S) ? 1 : 0;
     if (L.dense) {
         DenseArgs A{dview(L), {L.W[0].p, L.W[1].p, L.W[2].p}, L.fluid.p};
-        k_dense_residual<<<nblk(L.ncell()), 256, 0, s>>>(A, L.x.p, L.b.p, L.r.p);
-        AW_LAUNCH();
-        return AW_OK;
+        return launch_dep(S, k_dense_residual, nblk(L.ncell()), 256, 0, s, A, (const float*)L.x.p, (const float*)L.b.p,
+                          L.r.p);
     }
     XStore x = xstore(S, m);
     if (L.ndesc[2]) {
-        k_residual<SrcX><<<L.ndesc[2], 256, L.smem_smooth, s>>>(SrcX{x}, bptr(S, m), coef(L), L.fluid.p, batch(L, 2), cf,
-                                                                 L.r.p, nullptr, part);
-        AW_LAUNCH();
+        AW_TRY(launch_dep(S, k_residual<SrcX>, (unsigned)L.ndesc[2], 256, L.smem_smooth, s, SrcX{x}, bptr(S, m), coef(L),
+                          (const uint8_t*)L.fluid.p, batch(L, 2), cf, L.r.p, (double*)nullptr, part));
     }
     return AW_OK;
 }
@@ -1607,13 +1646,12 @@ static aw_status restrict_level(aw_solver* S, int m, cudaStream_t s) {
     if (K.dense) {
         LevelView Fv = F.dense ? LevelView{} : lview(S, m);
         if (F.dense) Fv.g = S->g->st.geo;
-        k_dense_restrict<<<nblk(K.ncell()), 256, 0, s>>>(dview(K), K.fluid.p, K.b.p, F.dense ? 0 : 1, Fv, dview(F), F.r.p);
-        AW_LAUNCH();
-        return AW_OK;
+        return launch_dep(S, k_dense_restrict, nblk(K.ncell()), 256, 0, s, dview(K), (const uint8_t*)K.fluid.p, K.b.p,
+                          F.dense ? 0 : 1, Fv, dview(F), (const float*)F.r.p);
     }
     if (K.ndesc[2]) {
-        k_restrict<<<K.ndesc[2], 256, K.smem_meta, s>>>(F.r.p, K.b.p, K.fluid.p, cf, batch(K, 2));
-        AW_LAUNCH();
+        AW_TRY(launch_dep(S, k_restrict, (unsigned)K.ndesc[2], 256, K.smem_meta, s, (const float*)F.r.p, K.b.p,
+                          (const uint8_t*)K.fluid.p, cf, batch(K, 2)));
     }
     return AW_OK;
 }
@@ -1628,14 +1666,12 @@ static aw_status prolong_level(aw_solver* S, int m, cudaStream_t s) {
         size_t n = F.dense ? F.ncell() : (size_t)S->g->st.nb;
         XStore xf = F.dense ? XStore{} : xstore(S, m);
         AW_CHECK_ARG(F.dense || xf.f, "FP16 storage on the one-cell MSBG level is not supported");
-        k_dense_prolong<<<nblk(n), 256, 0, s>>>(dview(K), K.x.p, F.dense ? 0 : 1, Fv, xf, dview(F), F.x.p, F.fluid.p);
-        AW_LAUNCH();
-        return AW_OK;
+        return launch_dep(S, k_dense_prolong, nblk(n), 256, 0, s, dview(K), (const float*)K.x.p, F.dense ? 0 : 1, Fv, xf,
+                          dview(F), F.x.p, (const uint8_t*)F.fluid.p);
     }
     if (F.ndesc[2]) {
-        k_prolong<<<F.ndesc[2], 256, F.half ? F.smem_prolong : F.smem_meta, s>>>(xstore(S, m), xstore(S, m + 1), F.fluid.p,
-                                                                                 cf, batch(F, 2));
-        AW_LAUNCH();
+        AW_TRY(launch_dep(S, k_prolong, (unsigned)F.ndesc[2], 256, F.half ? F.smem_prolong : F.smem_meta, s, xstore(S, m),
+                          xstore(S, m + 1), (const uint8_t*)F.fluid.p, cf, batch(F, 2)));
     }
     return AW_OK;
 }
@@ -1645,9 +1681,8 @@ static aw_status coarsest(aw_solver* S, int m, cudaStream_t s) {
     if (fv(S) && S->exact) {
         Uniform U = uniform_of(S, m);
         float* x = L.dense ? L.x.p : (m == 0 && S->x0 ? S->x0 : L.x.p);
-        k_coarse_apply<<<4, 128, 0, s>>>(U, S->ex_idx.p, S->ex_n.p, S->Minv.p, bptr(S, m), x);
-        AW_LAUNCH();
-        return AW_OK;
+        return launch_dep(S, k_coarse_apply, 4, 128, 0, s, U, (const int*)S->ex_idx.p, (const int*)S->ex_n.p,
+                          (const double*)S->Minv.p, bptr(S, m), x);
     }
     return smooth_level(S, m, S->d.coarsest_iterations, s);
 }
@@ -1962,6 +1997,7 @@ static aw_status solver_build(aw_solver* S) {
     AW_TRY(S->partials.ensure(nparts));
     AW_TRY(S->norm.ensure(2));
     S->use_graph = getenv("AW_NO_GRAPH") == nullptr;
+    S->use_pdl = getenv("AW_NO_PDL") == nullptr;
     AW_CUDA(cudaDeviceSynchronize());
     return AW_OK;
 }
