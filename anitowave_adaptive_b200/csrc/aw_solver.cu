@@ -812,6 +812,7 @@ __global__ void __launch_bounds__(NT) k_prolong(XStore xf, XStore xc, const uint
 // dot(a, b) over fluid cells (b is FP64, or FP32 when bf is given), per-CTA partial sums
 __global__ void k_dot64(const double* __restrict__ a, const double* __restrict__ b, const float* __restrict__ bf,
                         const uint8_t* __restrict__ fluid, size_t n, double* __restrict__ part) {
+    pdl_wait();
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
         if (fluid[i]) acc += a[i] * (bf ? (double)bf[i] : b[i]);
@@ -828,6 +829,7 @@ __global__ void k_dot64(const double* __restrict__ a, const double* __restrict__
 // z (FP32 V-cycle output) -> search direction d = z + beta d, beta = rho / rho_old (0 when first)
 __global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__ z, const uint8_t* __restrict__ fluid,
                                const double* __restrict__ sc, int first, size_t n) {
+    pdl_wait();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double beta = first ? 0.0 : sc[0] / sc[1];
@@ -839,6 +841,7 @@ __global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__
 __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, float* __restrict__ rf,
                             const double* __restrict__ d, const double* __restrict__ qn, const double* __restrict__ sc,
                             const uint8_t* __restrict__ fluid, size_t n, double* __restrict__ part) {
+    pdl_wait();
     const double dq = -sc[2];
     const double alpha = dq != 0.0 ? sc[0] / dq : 0.0;
     double acc = 0.0;
@@ -859,7 +862,8 @@ __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, floa
         if (threadIdx.x == 0) part[blockIdx.x] = t;
     }
 }
-__global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
+__global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) {
+    pdl_wait(); sc[dst] = sc[src]; }
 
 // ---- conjugate gradients with every vector and scalar in FP32 (AW_PRECISION_FP32_PCG) ----------
 // The same V-cycle preconditioner as the mixed form, without its FP64 residual, direction and
@@ -881,6 +885,7 @@ __device__ inline float block_sum_f(float v, float* red) {
 }
 __global__ void k_dot32(const float* __restrict__ a, const float* __restrict__ b, const uint8_t* __restrict__ fluid,
                         size_t n, float* __restrict__ part) {
+    pdl_wait();
     __shared__ float red[32];
     float acc = 0.f;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
@@ -889,6 +894,7 @@ __global__ void k_dot32(const float* __restrict__ a, const float* __restrict__ b
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 __global__ void k_reduce_sum32(const float* __restrict__ part, int n, float* out) {
+    pdl_wait();
     __shared__ float red[32];
     float acc = 0.f;
     for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
@@ -897,6 +903,7 @@ __global__ void k_reduce_sum32(const float* __restrict__ part, int n, float* out
 }
 __global__ void k_cg_direction32(float* __restrict__ d, const float* __restrict__ z, const uint8_t* __restrict__ fluid,
                                  const float* __restrict__ sc, int first, size_t n) {
+    pdl_wait();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float beta = first ? 0.f : sc[0] / sc[1];
@@ -906,6 +913,7 @@ __global__ void k_cg_direction32(float* __restrict__ d, const float* __restrict_
 __global__ void k_cg_update32(float* __restrict__ p, float* __restrict__ r, const float* __restrict__ d,
                               const float* __restrict__ qn, const float* __restrict__ sc,
                               const uint8_t* __restrict__ fluid, size_t n, float* __restrict__ part) {
+    pdl_wait();
     __shared__ float red[32];
     const float dq = -sc[2];
     const float alpha = dq != 0.f ? sc[0] / dq : 0.f;
@@ -919,7 +927,8 @@ __global__ void k_cg_update32(float* __restrict__ p, float* __restrict__ r, cons
     const float t = block_sum_f(acc, red);
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
-__global__ void k_copy_scalar32(float* __restrict__ sc, int dst, int src) { sc[dst] = sc[src]; }
+__global__ void k_copy_scalar32(float* __restrict__ sc, int dst, int src) {
+    pdl_wait(); sc[dst] = sc[src]; }
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -927,6 +936,7 @@ __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, s
 }
 
 __global__ void k_reduce_sum(const double* __restrict__ part, int n, double* out) {
+    pdl_wait();
     __shared__ double red[32];
     double acc = 0.0;
     for (int i = threadIdx.x; i < n; i += blockDim.x) acc += part[i];
@@ -2281,24 +2291,24 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
             st = zero_x(S, 0, s);
             if (st == AW_OK) st = run_vcycle(S, s);
             if (st != AW_OK) break;
-            k_dot32<<<ndot, 256, 0, s>>>(L0.b.p, L0.x.p, L0.fluid.p, nc, S->partials32.p);
-            if ((st = launch_err("k_dot32")) != AW_OK) break;
-            k_reduce_sum32<<<1, 256, 0, s>>>(S->partials32.p, (int)ndot, sc + 0);
-            if ((st = launch_err("k_reduce_sum32")) != AW_OK) break;
-            k_cg_direction32<<<nblk(nc), 256, 0, s>>>(S->cg32_d.p, L0.x.p, L0.fluid.p, sc, restart ? 1 : 0, nc);
-            if ((st = launch_err("k_cg_direction32")) != AW_OK) break;
-            k_residual<SrcX><<<L0.ndesc[2], 256, L0.smem_smooth, s>>>(SrcX{xd}, S->cg_zero.p, coef(L0), L0.fluid.p,
-                                                                       batch(L0, 2), cf, S->cg32_q.p, nullptr, nullptr);
-            if ((st = launch_err("k_residual (A d)")) != AW_OK) break;
-            k_dot32<<<ndot, 256, 0, s>>>(S->cg32_d.p, S->cg32_q.p, L0.fluid.p, nc, S->partials32.p);
-            if ((st = launch_err("k_dot32")) != AW_OK) break;
-            k_reduce_sum32<<<1, 256, 0, s>>>(S->partials32.p, (int)ndot, sc + 2);
-            if ((st = launch_err("k_reduce_sum32")) != AW_OK) break;
-            k_cg_update32<<<ndot, 256, 0, s>>>(p, L0.b.p, S->cg32_d.p, S->cg32_q.p, sc, L0.fluid.p, nc,
-                                               S->partials32.p);
-            if ((st = launch_err("k_cg_update32")) != AW_OK) break;
-            k_copy_scalar32<<<1, 1, 0, s>>>(sc, 1, 0);
-            if ((st = launch_err("k_copy_scalar32")) != AW_OK) break;
+            // the kernels of one iteration as programmatic dependents of one another
+            if ((st = launch_dep(S, k_dot32, ndot, 256, 0, s, L0.b.p, L0.x.p, L0.fluid.p, nc, S->partials32.p)) != AW_OK) break;
+            if ((st = launch_dep(S, k_reduce_sum32, 1, 256, 0, s, S->partials32.p, (int)ndot, sc + 0)) != AW_OK) break;
+            if ((st = launch_dep(S, k_cg_direction32, nblk(nc), 256, 0, s, S->cg32_d.p, L0.x.p, L0.fluid.p, sc,
+                                 restart ? 1 : 0, nc)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_residual<SrcX>, (unsigned)L0.ndesc[2], 256, L0.smem_smooth, s, SrcX{xd},
+                                 S->cg_zero.p, coef(L0), L0.fluid.p, batch(L0, 2), cf, S->cg32_q.p, (double*)nullptr,
+                                 (double*)nullptr)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_dot32, ndot, 256, 0, s, S->cg32_d.p, S->cg32_q.p, L0.fluid.p, nc,
+                                 S->partials32.p)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_reduce_sum32, 1, 256, 0, s, S->partials32.p, (int)ndot, sc + 2)) != AW_OK) break;
+            if ((st = launch_dep(S, k_cg_update32, ndot, 256, 0, s, p, L0.b.p, S->cg32_d.p, S->cg32_q.p, sc, L0.fluid.p,
+                                 nc, S->partials32.p)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_copy_scalar32, 1, 1, 0, s, sc, 1, 0)) != AW_OK) break;
             ++it;
             restart = false;
             st = read_norm32(&rn);
@@ -2355,26 +2365,28 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
             if (st == AW_OK) st = run_vcycle(S, s);
             if (st != AW_OK) break;
             // rho = r . z ; d = z + (rho / rho_old) d
-            k_dot64<<<ndot, 256, 0, s>>>(S->cg_r.p, nullptr, L0.x.p, L0.fluid.p, nc, S->partials.p);
-            if ((st = launch_err("k_dot64")) != AW_OK) break;
-            k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, ndot, sc + 0);
-            if ((st = launch_err("k_reduce_sum")) != AW_OK) break;
-            k_cg_direction<<<nblk(nc), 256, 0, s>>>(S->cg_d.p, L0.x.p, L0.fluid.p, sc, restart ? 1 : 0, nc);
-            if ((st = launch_err("k_cg_direction")) != AW_OK) break;
+            // the kernels of one iteration as programmatic dependents of one another
+            if ((st = launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_r.p, (const double*)nullptr, L0.x.p, L0.fluid.p, nc,
+                                 S->partials.p)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 0)) != AW_OK) break;
+            if ((st = launch_dep(S, k_cg_direction, nblk(nc), 256, 0, s, S->cg_d.p, L0.x.p, L0.fluid.p, sc,
+                                 restart ? 1 : 0, nc)) != AW_OK)
+                break;
             // qn = -A d ; sc[2] = d . qn
-            k_residual<SrcD><<<L0.ndesc[2], 256, L0.smem_x64, s>>>(SrcD{S->cg_d.p}, S->cg_zero.p, coef(L0), L0.fluid.p,
-                                                                    batch(L0, 2), cf, nullptr, S->cg_q.p, nullptr);
-            if ((st = launch_err("k_residual64 (A d)")) != AW_OK) break;
-            k_dot64<<<ndot, 256, 0, s>>>(S->cg_d.p, S->cg_q.p, nullptr, L0.fluid.p, nc, S->partials.p);
-            if ((st = launch_err("k_dot64")) != AW_OK) break;
-            k_reduce_sum<<<1, 256, 0, s>>>(S->partials.p, ndot, sc + 2);
-            if ((st = launch_err("k_reduce_sum")) != AW_OK) break;
+            if ((st = launch_dep(S, k_residual<SrcD>, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p},
+                                 S->cg_zero.p, coef(L0), L0.fluid.p, batch(L0, 2), cf, (float*)nullptr, S->cg_q.p,
+                                 (double*)nullptr)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_d.p, S->cg_q.p, (const float*)nullptr, L0.fluid.p, nc,
+                                 S->partials.p)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 2)) != AW_OK) break;
             // p += alpha d ; r -= alpha A d ; FP32 copy of r for the next V-cycle ; rho_old = rho
-            k_cg_update<<<ndot, 256, 0, s>>>(p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, L0.fluid.p, nc,
-                                             S->partials.p);
-            if ((st = launch_err("k_cg_update")) != AW_OK) break;
-            k_copy_scalar<<<1, 1, 0, s>>>(sc, 1, 0);
-            if ((st = launch_err("k_copy_scalar")) != AW_OK) break;
+            if ((st = launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc,
+                                 L0.fluid.p, nc, S->partials.p)) != AW_OK)
+                break;
+            if ((st = launch_dep(S, k_copy_scalar, 1, 1, 0, s, sc, 1, 0)) != AW_OK) break;
             ++it;
             restart = false;
             st = read_norm(S, ndot, s, &rn);  // ||r|| from k_cg_update's partial sums
