@@ -93,13 +93,24 @@ struct aw_solver {
     const void* cycle_x0 = nullptr;
     const void* cycle_b0 = nullptr;
     unsigned long long cycle_kernels = 0;
+    // the mixed-precision CG iterations as one graph with a device-side while loop, per pressure
+    // array; cgst = {iterations, restart flag, iteration limit}, cgprm = {||b||, tolerance}
+    cudaGraphExec_t cgloop = nullptr;
+    const void* cgloop_p = nullptr;
+    unsigned long long cgloop_kernels = 0;
+    bool use_devloop = true;
+    aw::DBuf<int> cgst;
+    aw::DBuf<double> cgprm;
     bool use_graph = true;
     bool use_pdl = true;  // V-cycle kernels as programmatic dependent launches
     double* h_norm = nullptr;  // pinned host word for the per-iteration residual norm
+    double* h_cg = nullptr;    // pinned host words of the device-loop state
     ~aw_solver() {
         if (cycle) cudaGraphExecDestroy(cycle);
+        if (cgloop) cudaGraphExecDestroy(cgloop);
         if (cap) cudaStreamDestroy(cap);
         if (h_norm) cudaFreeHost(h_norm);
+        if (h_cg) cudaFreeHost(h_cg);
     }
 };
 
@@ -827,11 +838,13 @@ __global__ void k_dot64(const double* __restrict__ a, const double* __restrict__
     }
 }
 // z (FP32 V-cycle output) -> search direction d = z + beta d, beta = rho / rho_old (0 when first)
+// first_dev (when given) holds the restart flag on the device
 __global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__ z, const uint8_t* __restrict__ fluid,
-                               const double* __restrict__ sc, int first, size_t n) {
+                               const double* __restrict__ sc, int first, const int* first_dev, size_t n) {
     pdl_wait();
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    if (first_dev) first = *first_dev;
     const double beta = first ? 0.0 : sc[0] / sc[1];
     d[i] = fluid[i] ? (double)z[i] + beta * d[i] : 0.0;
 }
@@ -862,8 +875,25 @@ __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, floa
         if (threadIdx.x == 0) part[blockIdx.x] = t;
     }
 }
+// End of one CG iteration inside the device-side loop: count it, clear the restart flag, and run the
+// loop body again while the residual (||r||^2 in norm2) is finite, at or above the tolerance and the
+// iteration limit is not reached.  st = {iterations, restart, limit}, prm = {||b||, tolerance}.
+__global__ void k_cg_check(cudaGraphConditionalHandle h, const double* __restrict__ norm2,
+                           const double* __restrict__ prm, int* st) {
+    const double rel = sqrt(norm2[0]) / prm[0];
+    const int it = st[0] + 1;
+    st[0] = it;
+    st[1] = 0;
+    cudaGraphSetConditional(h, (rel == rel && rel >= prm[1] && it < st[2]) ? 1u : 0u);
+}
+__global__ void k_fill_zero(float* __restrict__ x, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) x[i] = 0.f;
+}
 __global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) {
-    pdl_wait(); sc[dst] = sc[src]; }
+    pdl_wait();
+    sc[dst] = sc[src];
+}
 
 // ---- conjugate gradients with every vector and scalar in FP32 (AW_PRECISION_FP32_PCG) ----------
 // The same V-cycle preconditioner as the mixed form, without its FP64 residual, direction and
@@ -928,7 +958,9 @@ __global__ void k_cg_update32(float* __restrict__ p, float* __restrict__ r, cons
     if (threadIdx.x == 0) part[blockIdx.x] = t;
 }
 __global__ void k_copy_scalar32(float* __restrict__ sc, int dst, int src) {
-    pdl_wait(); sc[dst] = sc[src]; }
+    pdl_wait();
+    sc[dst] = sc[src];
+}
 
 __global__ void k_accum64(double* __restrict__ p, const float* __restrict__ e, size_t n) {
     size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1862,6 +1894,9 @@ static aw_status solver_build(aw_solver* S) {
     if (S->cycle) cudaGraphExecDestroy(S->cycle);
     S->cycle = nullptr;
     S->cycle_x0 = S->cycle_b0 = nullptr;
+    if (S->cgloop) cudaGraphExecDestroy(S->cgloop);
+    S->cgloop = nullptr;
+    S->cgloop_p = nullptr;
     S->cycle_kernels = 0;
     S->x0 = nullptr;
     S->b0 = nullptr;
@@ -2008,6 +2043,7 @@ static aw_status solver_build(aw_solver* S) {
     AW_TRY(S->norm.ensure(2));
     S->use_graph = getenv("AW_NO_GRAPH") == nullptr;
     S->use_pdl = getenv("AW_NO_PDL") == nullptr;
+    S->use_devloop = getenv("AW_NO_DEVLOOP") == nullptr;
     AW_CUDA(cudaDeviceSynchronize());
     return AW_OK;
 }
@@ -2187,6 +2223,82 @@ static aw_status read_norm(aw_solver* S, int nparts, cudaStream_t s, double* out
     return AW_OK;
 }
 
+// Mixed-precision CG iterations on the device until the recursive residual falls below the
+// tolerance, turns NaN or the iteration limit is reached: one graph whose while node repeats the
+// iteration (V-cycle preconditioner, the two dot products, the direction, A d and the update) and
+// a check kernel that sets the loop condition, so no host round trip separates iterations.  The
+// kernels and their order are those of the host-driven loop, so the results are identical.  The
+// graph is built per pressure array.  Returns false (state unchanged) when the device cannot
+// build such a graph; the caller then keeps the host loop.
+static aw_status cg_body(aw_solver* S, double* p, unsigned ndot, cudaStream_t s, cudaGraphConditionalHandle h) {
+    MGLevel& L0 = S->lv[0];
+    const size_t nc = L0.ncell();
+    const int cf = fv(S) ? 1 : 0;
+    double* sc = S->cg_sc.p;
+    k_fill_zero<<<nblk(nc), 256, 0, s>>>(L0.x.p, nc);
+    AW_LAUNCH();
+    AW_TRY(vcycle(S, 0, s));
+    AW_TRY(launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_r.p, (const double*)nullptr, L0.x.p, L0.fluid.p, nc,
+                      S->partials.p));
+    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 0));
+    AW_TRY(launch_dep(S, k_cg_direction, nblk(nc), 256, 0, s, S->cg_d.p, L0.x.p, L0.fluid.p, sc, 0,
+                      (const int*)(S->cgst.p + 1), nc));
+    AW_TRY(launch_dep(S, k_residual<SrcD>, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p}, S->cg_zero.p,
+                      coef(L0), L0.fluid.p, batch(L0, 2), cf, (float*)nullptr, S->cg_q.p, (double*)nullptr));
+    AW_TRY(launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_d.p, S->cg_q.p, (const float*)nullptr, L0.fluid.p, nc,
+                      S->partials.p));
+    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 2));
+    AW_TRY(launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, L0.fluid.p, nc,
+                      S->partials.p));
+    AW_TRY(launch_dep(S, k_copy_scalar, 1, 1, 0, s, sc, 1, 0));
+    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, S->norm.p));
+    k_cg_check<<<1, 1, 0, s>>>(h, S->norm.p, S->cgprm.p, S->cgst.p);
+    AW_LAUNCH();
+    return AW_OK;
+}
+
+static bool cg_devloop_build(aw_solver* S, double* p, unsigned ndot) {
+    if (S->cgloop) {
+        cudaGraphExecDestroy(S->cgloop);
+        S->cgloop = nullptr;
+    }
+    if (S->cgst.ensure(4) != AW_OK || S->cgprm.ensure(2) != AW_OK) return false;
+    if (!S->cap && cudaStreamCreateWithFlags(&S->cap, cudaStreamNonBlocking) != cudaSuccess) return false;
+    cudaGraph_t g = nullptr;
+    if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+    bool ok = false;
+    cudaGraphConditionalHandle h;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t node;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) == cudaSuccess) {
+            cudaGraph_t body = cp.conditional.phGraph_out[0];
+            const unsigned long long l0 = g_launches;
+            if (cudaStreamBeginCaptureToGraph(S->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal) ==
+                cudaSuccess) {
+                const aw_status st = cg_body(S, p, ndot, S->cap, h);
+                cudaGraph_t out = nullptr;
+                const cudaError_t e = cudaStreamEndCapture(S->cap, &out);
+                S->cgloop_kernels = g_launches - l0;
+                g_launches = l0;
+                ok = st == AW_OK && e == cudaSuccess && cudaGraphInstantiate(&S->cgloop, g, 0) == cudaSuccess;
+            }
+        }
+    }
+    cudaGraphDestroy(g);
+    if (!ok) {
+        S->cgloop = nullptr;
+        cudaGetLastError();
+        return false;
+    }
+    S->cgloop_p = p;
+    return true;
+}
+
 extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t* cycles, double* final_rel,
                               aw_stream s_) {
     AW_CHECK_ARG(S && d_b && d_p, "null argument");
@@ -2360,6 +2472,30 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
                 st = set_error(AW_ERR_NOT_CONVERGED, "relative residual %.3e after %d iterations", rel, it);
                 break;
             }
+            if (S->use_graph && S->use_devloop && S->cgloop_p != (const void*)p && !cg_devloop_build(S, p, ndot))
+                S->use_devloop = false;  // no such graph on this device: the host loop below
+            if (S->use_graph && S->use_devloop) {
+                // iterations on the device until the recursive residual converges, turns NaN or the
+                // limit is reached; then one read-back of ||r||^2 and the iteration count
+                const int st0[4] = {it, restart ? 1 : 0, S->d.max_cycles, 0};
+                const double prm[2] = {bn, S->d.tolerance};
+                if (!S->h_cg) AW_CUDA(cudaHostAlloc((void**)&S->h_cg, 4 * sizeof(double), cudaHostAllocDefault));
+                memcpy(S->h_cg, st0, sizeof st0);
+                memcpy(S->h_cg + 2, prm, sizeof prm);
+                AW_CUDA(cudaMemcpyAsync(S->cgst.p, S->h_cg, sizeof st0, cudaMemcpyHostToDevice, s));
+                AW_CUDA(cudaMemcpyAsync(S->cgprm.p, S->h_cg + 2, sizeof prm, cudaMemcpyHostToDevice, s));
+                AW_CUDA(cudaGraphLaunch(S->cgloop, s));
+                AW_CUDA(cudaMemcpyAsync(S->h_cg, S->norm.p, sizeof(double), cudaMemcpyDeviceToHost, s));
+                AW_CUDA(cudaMemcpyAsync(S->h_cg + 1, S->cgst.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+                AW_CUDA(cudaStreamSynchronize(s));
+                int it1 = 0;
+                memcpy(&it1, S->h_cg + 1, sizeof(int));
+                g_launches += S->cgloop_kernels * (unsigned long long)(it1 - it);
+                it = it1;
+                rn = std::sqrt(S->h_cg[0]);
+                restart = false;
+                continue;
+            }
             // z = V(r): one V-cycle on the FP32 copy of r (in L0.b), from zero
             st = zero_x(S, 0, s);
             if (st == AW_OK) st = run_vcycle(S, s);
@@ -2371,7 +2507,7 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
                 break;
             if ((st = launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 0)) != AW_OK) break;
             if ((st = launch_dep(S, k_cg_direction, nblk(nc), 256, 0, s, S->cg_d.p, L0.x.p, L0.fluid.p, sc,
-                                 restart ? 1 : 0, nc)) != AW_OK)
+                                 restart ? 1 : 0, (const int*)nullptr, nc)) != AW_OK)
                 break;
             // qn = -A d ; sc[2] = d . qn
             if ((st = launch_dep(S, k_residual<SrcD>, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p},
