@@ -2430,7 +2430,8 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
         // corrections), with the residual, the search direction and the pressure accumulation in
         // FP64 and the FP64 coarsest solve inside the V-cycle.  A stand-alone V-cycle iteration
         // stalls or diverges on free-surface domains with four levels; as a preconditioner the same
-        // cycle converges on every configuration.  One host read (||r||) per iteration.
+        // cycle converges on every configuration.  The iterations run in a device-side loop
+        // (cg_devloop_build) when the device can build it, else with one host read (||r||) each.
         double* p = (double*)d_p;
         double* sc = S->cg_sc.p;
         // reductions over the level-0 cells: 8 CTAs per SM, grid-stride
