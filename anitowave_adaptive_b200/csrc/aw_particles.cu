@@ -64,35 +64,38 @@ __global__ void k_keys(LevelView L, PArr pos, int64_t n, uint32_t invalid, uint3
 }
 
 // ------------------------------------------------------------------------------------------------
-// Stable LSD radix sort of (key, index) pairs, 10-bit digits.  Each pass: per-tile digit
-// histograms -> one exclusive scan over (digit, tile) -> scatter in which one warp walks its tile
-// in order and ranks equal digits with __match_any_sync, so equal keys keep their input order.
+// Stable LSD radix sort of (key, index) pairs, digits of up to 11 bits (as few passes as the key
+// range allows, the digit width spread evenly over them: 20-bit keys take two 10-bit passes, 22-bit
+// keys two 11-bit passes).  Each pass: per-tile digit histograms -> one exclusive scan over (digit,
+// tile) -> scatter in which one warp walks its tile in order and ranks equal digits with
+// __match_any_sync, so equal keys keep their input order.
 // ------------------------------------------------------------------------------------------------
-constexpr int RADIX_BITS = 10, RADIX_BINS = 1 << RADIX_BITS, RADIX_TILE = 2048;
+constexpr int RADIX_MAX_BITS = 11, RADIX_MAX_BINS = 1 << RADIX_MAX_BITS, RADIX_TILE = 2048;
 
-__global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift,
+__global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift, int bins,
                                                     uint32_t* __restrict__ hist, uint32_t ntiles) {
-    __shared__ uint32_t h[RADIX_BINS];
-    for (int i = threadIdx.x; i < RADIX_BINS; i += blockDim.x) h[i] = 0;
+    __shared__ uint32_t h[RADIX_MAX_BINS];
+    for (int i = threadIdx.x; i < bins; i += blockDim.x) h[i] = 0;
     __syncthreads();
     const int64_t base = (int64_t)blockIdx.x * RADIX_TILE;
     for (int i = threadIdx.x; i < RADIX_TILE; i += blockDim.x) {
         int64_t j = base + i;
-        if (j < n) atomicAdd(&h[(keys[j] >> shift) & (RADIX_BINS - 1)], 1u);
+        if (j < n) atomicAdd(&h[(keys[j] >> shift) & (uint32_t)(bins - 1)], 1u);
     }
     __syncthreads();
-    for (int d = threadIdx.x; d < RADIX_BINS; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
+    for (int d = threadIdx.x; d < bins; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
 }
 
 __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                        uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
-                                                       int shift, const uint32_t* __restrict__ offs, uint32_t ntiles) {
-    extern __shared__ uint32_t cnt[];  // RADIX_BINS per warp
+                                                       int shift, int bins, const uint32_t* __restrict__ offs,
+                                                       uint32_t ntiles) {
+    extern __shared__ uint32_t cnt[];  // bins per warp
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t tile = blockIdx.x * (blockDim.x >> 5) + w;
-    uint32_t* c = cnt + w * RADIX_BINS;
+    uint32_t* c = cnt + w * bins;
     if (tile >= ntiles) return;
-    for (int d = lane; d < RADIX_BINS; d += 32) c[d] = offs[(size_t)d * ntiles + tile];
+    for (int d = lane; d < bins; d += 32) c[d] = offs[(size_t)d * ntiles + tile];
     __syncwarp();
     const int64_t base = (int64_t)tile * RADIX_TILE;
     const unsigned lt = (1u << lane) - 1u;
@@ -103,9 +106,9 @@ __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restric
         if (valid) {
             key = kin[j];
             val = vin ? vin[j] : (uint32_t)j;
-            dig = (key >> shift) & (RADIX_BINS - 1);
+            dig = (key >> shift) & (uint32_t)(bins - 1);
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, valid ? dig : (uint32_t)(RADIX_BINS + lane));
+        const unsigned peers = __match_any_sync(0xffffffffu, valid ? dig : (uint32_t)(bins + lane));
         const uint32_t pos = valid ? c[dig] + __popc(peers & lt) : 0u;
         __syncwarp();
         if (valid && (__ffs(peers) - 1) == lane) c[dig] += __popc(peers);
@@ -122,23 +125,25 @@ static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* val
                                   uint32_t** sorted_vals, cudaStream_t s) {
     int bits = 1;
     while (bits < 32 && (maxkey >> bits)) ++bits;
-    const int passes = (bits + RADIX_BITS - 1) / RADIX_BITS;
+    const int passes = (bits + RADIX_MAX_BITS - 1) / RADIX_MAX_BITS;
+    const int digit = (bits + passes - 1) / passes;
+    const int bins = 1 << digit;
     const uint32_t ntiles = (uint32_t)((n + RADIX_TILE - 1) / RADIX_TILE);
-    const size_t nh = (size_t)RADIX_BINS * ntiles;
+    const size_t nh = (size_t)bins * ntiles;
     AW_TRY(hist.ensure(nh));
     AW_TRY(scan_out.ensure(nh + 1));
     uint32_t *kin = keys, *kout = keys2, *vin = nullptr, *vout = vals;
     const int wpb = 8;
     for (int p = 0; p < passes; ++p) {
-        const int shift = p * RADIX_BITS;
-        k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, hist.p, ntiles);
+        const int shift = p * digit;
+        k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, bins, hist.p, ntiles);
         AW_LAUNCH();
         AW_TRY(exclusive_scan_u32(hist.p, scan_out.p, nh, tmp, s));
-        const size_t ssm = (size_t)wpb * RADIX_BINS * sizeof(uint32_t);
+        const size_t ssm = (size_t)wpb * bins * sizeof(uint32_t);
         if (ssm > 48 * 1024)
             AW_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
         k_radix_scatter<<<(ntiles + wpb - 1) / wpb, 32 * wpb, ssm, s>>>(
-            kin, vin, kout, vout, n, shift, scan_out.p, ntiles);
+            kin, vin, kout, vout, n, shift, bins, scan_out.p, ntiles);
         AW_LAUNCH();
         std::swap(kin, kout);
         vin = vout;
