@@ -70,17 +70,26 @@ __global__ void k_keys(LevelView L, PArr pos, int64_t n, uint32_t invalid, uint3
 // tile) -> scatter in which one warp walks its tile in order and ranks equal digits with
 // __match_any_sync, so equal keys keep their input order.
 // ------------------------------------------------------------------------------------------------
-constexpr int RADIX_MAX_BITS = 11, RADIX_MAX_BINS = 1 << RADIX_MAX_BITS, RADIX_TILE = 2048;
+constexpr int RADIX_MAX_BITS = 11, RADIX_MAX_BINS = 1 << RADIX_MAX_BITS;
 
 __global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__ keys, int64_t n, int shift, int bins,
-                                                    uint32_t* __restrict__ hist, uint32_t ntiles) {
+                                                    int tile, uint32_t* __restrict__ hist, uint32_t ntiles) {
     __shared__ uint32_t h[RADIX_MAX_BINS];
     for (int i = threadIdx.x; i < bins; i += blockDim.x) h[i] = 0;
     __syncthreads();
-    const int64_t base = (int64_t)blockIdx.x * RADIX_TILE;
-    for (int i = threadIdx.x; i < RADIX_TILE; i += blockDim.x) {
-        int64_t j = base + i;
-        if (j < n) atomicAdd(&h[(keys[j] >> shift) & (uint32_t)(bins - 1)], 1u);
+    // keys arrive nearly sorted (runs of equal digits, thousands long in crowded cells): a warp whose
+    // 32 keys share one digit adds once, so shared-memory atomics do not queue on one address
+    const int64_t base = (int64_t)blockIdx.x * tile;
+    for (int i = threadIdx.x; i < tile; i += blockDim.x) {
+        const int64_t j = base + i;
+        const bool valid = j < n;
+        const uint32_t dig = valid ? (keys[j] >> shift) & (uint32_t)(bins - 1) : 0xFFFFFFFFu;
+        const uint32_t d0 = __shfl_sync(0xffffffffu, dig, 0);
+        if (__all_sync(0xffffffffu, dig == d0)) {
+            if ((threadIdx.x & 31) == 0 && valid) atomicAdd(&h[dig], 32u);
+        } else if (valid) {
+            atomicAdd(&h[dig], 1u);
+        }
     }
     __syncthreads();
     for (int d = threadIdx.x; d < bins; d += blockDim.x) hist[(size_t)d * ntiles + blockIdx.x] = h[d];
@@ -88,18 +97,18 @@ __global__ void __launch_bounds__(256) k_radix_hist(const uint32_t* __restrict__
 
 __global__ void __launch_bounds__(256) k_radix_scatter(const uint32_t* __restrict__ kin, const uint32_t* __restrict__ vin,
                                                        uint32_t* __restrict__ kout, uint32_t* __restrict__ vout, int64_t n,
-                                                       int shift, int bins, const uint32_t* __restrict__ offs,
+                                                       int shift, int bins, int tile, const uint32_t* __restrict__ offs,
                                                        uint32_t ntiles) {
     extern __shared__ uint32_t cnt[];  // bins per warp
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const uint32_t tile = blockIdx.x * (blockDim.x >> 5) + w;
+    const uint32_t t = blockIdx.x * (blockDim.x >> 5) + w;
     uint32_t* c = cnt + w * bins;
-    if (tile >= ntiles) return;
-    for (int d = lane; d < bins; d += 32) c[d] = offs[(size_t)d * ntiles + tile];
+    if (t >= ntiles) return;
+    for (int d = lane; d < bins; d += 32) c[d] = offs[(size_t)d * ntiles + t];
     __syncwarp();
-    const int64_t base = (int64_t)tile * RADIX_TILE;
+    const int64_t base = (int64_t)t * tile;
     const unsigned lt = (1u << lane) - 1u;
-    for (int ch = 0; ch < RADIX_TILE; ch += 32) {
+    for (int ch = 0; ch < tile; ch += 32) {
         const int64_t j = base + ch + lane;
         const bool valid = j < n;
         uint32_t key = 0, val = 0, dig = 0;
@@ -128,7 +137,11 @@ static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* val
     const int passes = (bits + RADIX_MAX_BITS - 1) / RADIX_MAX_BITS;
     const int digit = (bits + passes - 1) / passes;
     const int bins = 1 << digit;
-    const uint32_t ntiles = (uint32_t)((n + RADIX_TILE - 1) / RADIX_TILE);
+    // tiles of 2048 keys, longer for large arrays (down to about 4096 tiles, one wave of warps), so
+    // that the (digit, tile) table and its scan stay small
+    int tile = 2048;
+    while (tile < 16384 && n / (2 * (int64_t)tile) >= 4096) tile *= 2;
+    const uint32_t ntiles = (uint32_t)((n + tile - 1) / tile);
     const size_t nh = (size_t)bins * ntiles;
     AW_TRY(hist.ensure(nh));
     AW_TRY(scan_out.ensure(nh + 1));
@@ -136,14 +149,14 @@ static aw_status radix_sort_pairs(uint32_t* keys, uint32_t* keys2, uint32_t* val
     const int wpb = 8;
     for (int p = 0; p < passes; ++p) {
         const int shift = p * digit;
-        k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, bins, hist.p, ntiles);
+        k_radix_hist<<<ntiles, 256, 0, s>>>(kin, n, shift, bins, tile, hist.p, ntiles);
         AW_LAUNCH();
         AW_TRY(exclusive_scan_u32(hist.p, scan_out.p, nh, tmp, s));
         const size_t ssm = (size_t)wpb * bins * sizeof(uint32_t);
         if (ssm > 48 * 1024)
             AW_CUDA(cudaFuncSetAttribute(k_radix_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
         k_radix_scatter<<<(ntiles + wpb - 1) / wpb, 32 * wpb, ssm, s>>>(
-            kin, vin, kout, vout, n, shift, bins, scan_out.p, ntiles);
+            kin, vin, kout, vout, n, shift, bins, tile, scan_out.p, ntiles);
         AW_LAUNCH();
         std::swap(kin, kout);
         vin = vout;
