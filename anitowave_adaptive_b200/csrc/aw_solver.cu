@@ -161,7 +161,7 @@ struct Coef3 {
 
 // ------------------------------------------------------------------------------------------------
 // Batched block kernels.  A CTA serves `count` blocks ("slots") of one resolution r, listed
-// contiguously: 1 block of 8^3 or 16^3 cells, 4 of 4^3, 32 of 2^3, 256 of 1^3.  Every slot keeps
+// contiguously: 1 block of 8^3 or 16^3 cells, 4 of 4^3, 32 of 2^3, 64 of 1^3.  Every slot keeps
 // its block and a one-cell halo in shared memory; slots never interact (same colour = no shared
 // faces), so each slot's arithmetic, early exit and activation are exactly those of a CTA that
 // owns one block.
@@ -190,7 +190,7 @@ enum {
 // 3 = coarser neighbour (parent cell), 4 = finer neighbour (mean of the 4 touching cells).
 enum { NB_NONE = 0, NB_SAME = 2, NB_COARSE = 3, NB_FINE = 4 };
 
-// Every thread of a batched CTA only ever touches cells of one slot (G * r^3 == 256, or G == 1).
+// Every thread of a batched CTA only ever touches cells of one slot (G * r^3 <= 256, or G == 1).
 // Reduce a per-thread non-negative value over the threads of each slot: shuffle within aligned
 // groups of min(r^3, 32) lanes, then one shared atomicMax per group.
 __device__ inline void slot_max(int* dst, int n3, float v) {
@@ -1476,7 +1476,11 @@ static XStore xstore(aw_solver* S, int m) {
 }
 static const float* bptr(aw_solver* S, int m) { return (m == 0 && S->b0) ? S->b0 : S->lv[m].b.p; }
 static Coef3 coef(const MGLevel& L) { return Coef3{{L.W[0].p, L.W[1].p, L.W[2].p}}; }
-static int slots_per_cta(int r) { return std::max(1, std::min(256, 256 / (r * r * r))); }
+// Slots per CTA.  One-cell blocks take 64 slots (a quarter of the threads), not 256: a level's
+// slot image is sized for its largest group, and 256 one-cell slots (70 KB in FP32, 98 KB in FP64)
+// held every CTA of the level to 3 (or 2) per SM.  At 64 the image stays under 18 KB (25 KB in FP64)
+// and 6 CTAs fit per SM (poisson_256 to 1e-6: 8.05 to 5.90 ms; dam_drop_128 solve 2.08 to 1.85 ms).
+static int slots_per_cta(int r) { return r == 1 ? 64 : std::max(1, std::min(256, 256 / (r * r * r))); }
 
 // Build the CTA batches of one block-structured level from its per-block resolutions.
 static aw_status build_batches(MGLevel& L, const Geo& geo) {
