@@ -103,6 +103,7 @@ struct aw_solver {
     aw::DBuf<double> cgprm;
     bool use_graph = true;
     bool use_pdl = true;  // V-cycle kernels as programmatic dependent launches
+    int tail = 0;         // first level of the uniform tail run as one k_dense_tail launch (0: none)
     double* h_norm = nullptr;  // pinned host word for the per-iteration residual norm
     double* h_cg = nullptr;    // pinned host words of the device-loop state
     ~aw_solver() {
@@ -161,7 +162,7 @@ struct Coef3 {
 
 // ------------------------------------------------------------------------------------------------
 // Batched block kernels.  A CTA serves `count` blocks ("slots") of one resolution r, listed
-// contiguously: 1 block of 8^3 or 16^3 cells, 4 of 4^3, 32 of 2^3, 64 of 1^3.  Every slot keeps
+// contiguously: 1 block of 8^3 or 16^3 cells, 4 of 4^3, 16 of 2^3, 64 of 1^3.  Every slot keeps
 // its block and a one-cell halo in shared memory; slots never interact (same colour = no shared
 // faces), so each slot's arithmetic, early exit and activation are exactly those of a CTA that
 // owns one block.
@@ -630,13 +631,39 @@ __global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_smooth(LevelView L
 #undef AW_SMOOTH
 }
 
+// r = b - A x of cell i of slot sl from the staged slot image (0 on air cells when check_fluid)
+template <int R, class T>
+__device__ __forceinline__ T residual_cell(const SlotImage<T, R>& S, int sl, int i, int check_fluid) {
+    using Gm = Geom<R>;
+    constexpr int n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
+    T rv = T(0);
+    const float* bs = S.fs + sl * Gm::FS;
+    if (!check_fluid || S.fluid(sl, i)) {
+        const int cx = i % R, cy = (i / R) % R, cz = i / Gm::rr;
+        const float* Ws = bs + n3;
+        const T wW = Ws[fidx(0, cx, cy, cz, R)];
+        const T wE = Ws[fidx(0, cx + 1, cy, cz, R)];
+        const T wS = Ws[nf + fidx(1, cx, cy, cz, R)];
+        const T wN = Ws[nf + fidx(1, cx, cy + 1, cz, R)];
+        const T wB = Ws[2 * nf + fidx(2, cx, cy, cz, R)];
+        const T wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, R)];
+        const T diag = -(wW + wE + wS + wN + wB + wT);
+        const T* xs = S.xs + sl * Gm::X3;
+        const int q = xi3(cx, cy, cz, R2);
+        const T Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
+                     wB * xs[q - sz] + wT * xs[q + sz];
+        rv = (T)bs[i] - Ax;
+    }
+    return rv;
+}
+
 template <int R, class Src>
 __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred, const Src& x, const float* __restrict__ bvec,
                                      const Coef3& W, const uint8_t* __restrict__ fluid, const Batch& B, int check_fluid,
                                      float* __restrict__ rout, double* __restrict__ rout64, double* __restrict__ part) {
     using T = typename Src::T;
     using Gm = Geom<R>;
-    constexpr int GM = Gm::GMAX, n3 = Gm::n3, nf = Gm::nf, R2 = Gm::R2, sy = R2, sz = R2 * R2;
+    constexpr int GM = Gm::GMAX, n3 = Gm::n3;
     SlotImage<T, R> S(smraw, d.y);
     const int G = S.G;
     stage_meta<R>(S.meta, G, B, d.x, nullptr);
@@ -649,24 +676,7 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
     for (int t0 = 0; t0 < GM * n3; t0 += NT) {
         const int t = t0 + threadIdx.x, sl = t / n3, i = t % n3;
         if (sl >= G) continue;
-        T rv = T(0);
-        const float* bs = S.fs + sl * Gm::FS;
-        if (!check_fluid || S.fluid(sl, i)) {
-            const int cx = i % R, cy = (i / R) % R, cz = i / Gm::rr;
-            const float* Ws = bs + n3;
-            const T wW = Ws[fidx(0, cx, cy, cz, R)];
-            const T wE = Ws[fidx(0, cx + 1, cy, cz, R)];
-            const T wS = Ws[nf + fidx(1, cx, cy, cz, R)];
-            const T wN = Ws[nf + fidx(1, cx, cy + 1, cz, R)];
-            const T wB = Ws[2 * nf + fidx(2, cx, cy, cz, R)];
-            const T wT = Ws[2 * nf + fidx(2, cx, cy, cz + 1, R)];
-            const T diag = -(wW + wE + wS + wN + wB + wT);
-            const T* xs = S.xs + sl * Gm::X3;
-            const int q = xi3(cx, cy, cz, R2);
-            const T Ax = diag * xs[q] + wW * xs[q - 1] + wE * xs[q + 1] + wS * xs[q - sy] + wN * xs[q + sy] +
-                         wB * xs[q - sz] + wT * xs[q + sz];
-            rv = (T)bs[i] - Ax;
-        }
+        const T rv = residual_cell<R>(S, sl, i, check_fluid);
         if (rout) rout[S.off(0, sl) + i] = (float)rv;
         if (rout64) rout64[S.off(0, sl) + i] = (double)rv;
         acc += (double)rv * (double)rv;
@@ -1018,39 +1028,30 @@ __device__ inline float dense_Ax(const DenseArgs& A, const float* x, int i, int 
            diag * x[didx(d, i, j, k)];
 }
 
-__global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ b, int col, float omega) {
-    pdl_wait();
+// Per-cell values of the uniform-level kernels (the caller stores them), shared by the
+// one-launch-per-step kernels below and by k_dense_tail, so both forms do the same arithmetic in
+// the same order.  Each returns false where the kernel leaves the cell unchanged.
+__device__ inline bool dense_smooth_value(const DenseArgs& A, const float* x, const float* __restrict__ b, int t,
+                                          int col, float omega, float* out) {
     const DenseView& d = A.d;
-    int n = d.D[0] * d.D[1] * d.D[2];
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
-    if (((i + j + k) & 1) != col || !A.fluid[t]) return;
+    const int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
+    if (((i + j + k) & 1) != col || !A.fluid[t]) return false;
     float diag;
-    float ax = dense_Ax(A, x, i, j, k, &diag);
-    if (fabsf(diag) < 1e-30f) return;
-    x[t] += omega * __fdividef(b[t] - ax, diag);
+    const float ax = dense_Ax(A, x, i, j, k, &diag);
+    if (fabsf(diag) < 1e-30f) return false;
+    *out = x[t] + omega * __fdividef(b[t] - ax, diag);
+    return true;
 }
-
-__global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const float* __restrict__ b, float* r) {
-    pdl_wait();
+__device__ inline float dense_residual_value(const DenseArgs& A, const float* x, const float* __restrict__ b, int t) {
     const DenseView& d = A.d;
-    int n = d.D[0] * d.D[1] * d.D[2];
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
+    const int i = t % d.D[0], j = (t / d.D[0]) % d.D[1], k = t / (d.D[0] * d.D[1]);
     float diag;
-    r[t] = A.fluid[t] ? b[t] - dense_Ax(A, x, i, j, k, &diag) : 0.f;
+    return A.fluid[t] ? b[t] - dense_Ax(A, x, i, j, k, &diag) : 0.f;
 }
-
-// restriction into a dense level from the one-cell-per-block MSBG level (first) or a dense level
-__global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_c, float* __restrict__ bc, int from_msbg,
-                                 LevelView F, DenseView Fd, const float* __restrict__ rf) {
-    pdl_wait();
-    int n = K.D[0] * K.D[1] * K.D[2];
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    int i = t % K.D[0], j = (t / K.D[0]) % K.D[1], k = t / (K.D[0] * K.D[1]);
+// restriction into a dense level from the one-cell-per-block MSBG level (from_msbg) or a dense level
+__device__ inline float dense_restrict_value(const DenseView& K, const uint8_t* __restrict__ fluid_c, int from_msbg,
+                                             const LevelView& F, const DenseView& Fd, const float* rf, int t) {
+    const int i = t % K.D[0], j = (t / K.D[0]) % K.D[1], k = t / (K.D[0] * K.D[1]);
     float s = 0.f;
     for (int dz = 0; dz < 2; ++dz)
         for (int dy = 0; dy < 2; ++dy)
@@ -1063,28 +1064,64 @@ __global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_
                     s += rf[didx(Fd, ci, cj, ck)];
                 }
             }
-    bc[t] = fluid_c[t] ? s : 0.f;
+    return fluid_c[t] ? s : 0.f;
+}
+// x_f + x_c[parent] on fluid cells: t is a block of the one-cell MSBG level (to_msbg, *at = its
+// cell) or a dense cell (*at = t)
+__device__ inline bool dense_prolong_value(const DenseView& K, const float* xc, int to_msbg, const LevelView& F,
+                                           const float* xf_msbg, const DenseView& Fd, const float* xf,
+                                           const uint8_t* __restrict__ fluid_f, int t, uint32_t* at, float* out) {
+    if (to_msbg) {
+        if (!F.res[t]) return false;
+        const uint32_t ci = F.off[0][t];
+        if (!fluid_f[ci]) return false;
+        int c[3];
+        bcoord(F.g, t, c);
+        *at = ci;
+        *out = xf_msbg[ci] + xc[didx(K, c[0] >> 1, c[1] >> 1, c[2] >> 1)];
+        return true;
+    }
+    if (!fluid_f[t]) return false;
+    const int i = t % Fd.D[0], j = (t / Fd.D[0]) % Fd.D[1], k = t / (Fd.D[0] * Fd.D[1]);
+    *at = (uint32_t)t;
+    *out = xf[t] + xc[didx(K, i >> 1, j >> 1, k >> 1)];
+    return true;
+}
+
+__global__ void k_dense_smooth(DenseArgs A, float* x, const float* __restrict__ b, int col, float omega) {
+    pdl_wait();
+    const DenseView& d = A.d;
+    const int n = d.D[0] * d.D[1] * d.D[2];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    float v;
+    if (t < n && dense_smooth_value(A, x, b, t, col, omega, &v)) x[t] = v;
+}
+
+__global__ void k_dense_residual(DenseArgs A, const float* __restrict__ x, const float* __restrict__ b, float* r) {
+    pdl_wait();
+    const DenseView& d = A.d;
+    const int n = d.D[0] * d.D[1] * d.D[2];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) r[t] = dense_residual_value(A, x, b, t);
+}
+
+__global__ void k_dense_restrict(DenseView K, const uint8_t* __restrict__ fluid_c, float* __restrict__ bc, int from_msbg,
+                                 LevelView F, DenseView Fd, const float* __restrict__ rf) {
+    pdl_wait();
+    const int n = K.D[0] * K.D[1] * K.D[2];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) bc[t] = dense_restrict_value(K, fluid_c, from_msbg, F, Fd, rf, t);
 }
 
 __global__ void k_dense_prolong(DenseView K, const float* __restrict__ xc, int to_msbg, LevelView F, XStore xf_msbg,
                                 DenseView Fd, float* __restrict__ xf, const uint8_t* __restrict__ fluid_f) {
     pdl_wait();
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (to_msbg) {
-        if (t >= F.g.nb) return;
-        if (!F.res[t]) return;
-        uint32_t ci = F.off[0][t];
-        if (!fluid_f[ci]) return;
-        int c[3];
-        bcoord(F.g, t, c);
-        xf_msbg.f[ci] += xc[didx(K, c[0] >> 1, c[1] >> 1, c[2] >> 1)];
-    } else {
-        int n = Fd.D[0] * Fd.D[1] * Fd.D[2];
-        if (t >= n) return;
-        if (!fluid_f[t]) return;
-        int i = t % Fd.D[0], j = (t / Fd.D[0]) % Fd.D[1], k = t / (Fd.D[0] * Fd.D[1]);
-        xf[t] += xc[didx(K, i >> 1, j >> 1, k >> 1)];
-    }
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = to_msbg ? F.g.nb : Fd.D[0] * Fd.D[1] * Fd.D[2];
+    uint32_t at;
+    float v;
+    if (t < n && dense_prolong_value(K, xc, to_msbg, F, xf_msbg.f, Fd, xf, fluid_f, t, &at, &v))
+        (to_msbg ? xf_msbg.f : xf)[at] = v;
 }
 
 // ------------------------------- hierarchy setup kernels --------------------------------------
@@ -1429,15 +1466,158 @@ __global__ void __launch_bounds__(512) k_coarse_factor(Uniform U, int* pos_of, i
 }
 
 // x = Minv b on the fluid cells of the coarsest level (FP64 accumulation)
+// row i of x = Minv b over the n fluid cells of the coarsest level
+__device__ inline void coarse_apply_row(const Uniform& U, const int* __restrict__ idx, int n,
+                                        const double* __restrict__ Minv, const float* b, float* x, int i) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s += Minv[(size_t)i * n + j] * (double)b[uni_cell(U, idx[j])];
+    x[uni_cell(U, idx[i])] = (float)s;
+}
 __global__ void k_coarse_apply(Uniform U, const int* __restrict__ idx, const int* __restrict__ ex_n,
                                const double* __restrict__ Minv, const float* __restrict__ b, float* __restrict__ x) {
     pdl_wait();
     const int n = ex_n[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        double s = 0.0;
-        for (int j = 0; j < n; ++j) s += Minv[(size_t)i * n + j] * (double)b[uni_cell(U, idx[j])];
-        x[uni_cell(U, idx[i])] = (float)s;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        coarse_apply_row(U, idx, n, Minv, b, x, i);
+}
+
+// The uniform tail of an FV V-cycle in one CTA: the restriction from the level above the tail (the
+// last MSBG level, one cell per block, or a larger uniform level) into the first tail level, the
+// V-cycle over the tail levels down to the coarsest solve and back, and the prolongation into the
+// level above.  Tail levels hold at most TAIL_MAX_CELLS cells, so as separate launches (about 14 on
+// a 512/64-cell tail) each step costs a launch's latency rather than its work; here the steps are
+// separated by CTA barriers instead.  (A 4096-cell level measured slower in one CTA than as
+// launches, so larger uniform levels keep their own launches.)
+// Every step applies the per-cell value functions of the separate kernels in the same order, so the
+// results are bit-identical to the launch-per-step form.  The CTA reads and writes the levels in
+// global memory; __syncthreads orders one step's writes before the next step's reads.  Within a
+// step a thread computes the values of up to TAIL_K cells before it stores any of them, so their
+// loads are in flight together (a store between them could alias the next cell's loads).
+constexpr int TAIL_THREADS = 1024;
+constexpr int TAIL_K = 4;             // cells per thread whose loads are issued together
+constexpr int TAIL_MAX = 4;           // uniform levels the fused tail handles
+constexpr int TAIL_MAX_CELLS = 512;   // largest uniform level it handles
+struct TailLevel {
+    DenseArgs A;
+    float* x;
+    float* b;
+    float* r;
+};
+struct DenseTail {
+    TailLevel lv[TAIL_MAX];
+    int n;                    // uniform levels, lv[n - 1] the coarsest
+    int from_msbg;            // the level above is the last MSBG level (F), else a uniform level (Fd)
+    LevelView F;
+    DenseView Fd;
+    const float* rf;          // its residual
+    float* xf;                // its x (FP32)
+    const uint8_t* fluid_f;   // its fluid flags
+    int sweeps, coarsest_iters, exact;
+    float omega;
+    Uniform U;                // exact coarsest solve
+    const int* idx;
+    const int* ex_n;
+    const double* Minv;
+};
+__device__ inline int tail_cells(const TailLevel& L) { return L.A.d.D[0] * L.A.d.D[1] * L.A.d.D[2]; }
+// One step over n items: value(t, &at, &v) says whether item t writes v at index at; then store.
+template <class V, class S>
+__device__ __forceinline__ void tail_step(int n, V value, S store) {
+    for (int t0 = threadIdx.x; t0 < n; t0 += TAIL_K * blockDim.x) {
+        float v[TAIL_K];
+        uint32_t at[TAIL_K];
+        bool w[TAIL_K];
+#pragma unroll
+        for (int k = 0; k < TAIL_K; ++k) {
+            const int t = t0 + k * (int)blockDim.x;
+            w[k] = t < n && value(t, &at[k], &v[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < TAIL_K; ++k)
+            if (w[k]) store(at[k], v[k]);
     }
+    __syncthreads();
+}
+__device__ inline void tail_smooth(const TailLevel& L, int iters, int rev, float omega) {
+    const int n = tail_cells(L);
+    for (int it = 0; it < iters; ++it)
+        for (int k = 0; k < 2; ++k) {
+            const int col = rev ? 1 - k : k;
+            tail_step(
+                n,
+                [&](int t, uint32_t* at, float* v) {
+                    *at = (uint32_t)t;
+                    return dense_smooth_value(L.A, L.x, L.b, t, col, omega, v);
+                },
+                [&](uint32_t at, float v) { L.x[at] = v; });
+        }
+}
+__global__ void __launch_bounds__(TAIL_THREADS) k_dense_tail(DenseTail T) {
+    pdl_wait();
+    {  // restriction from the level above; the first tail level's x starts at zero
+        const TailLevel& C = T.lv[0];
+        tail_step(
+            tail_cells(C),
+            [&](int t, uint32_t* at, float* v) {
+                *at = (uint32_t)t;
+                *v = dense_restrict_value(C.A.d, C.A.fluid, T.from_msbg, T.F, T.Fd, T.rf, t);
+                return true;
+            },
+            [&](uint32_t at, float v) {
+                C.b[at] = v;
+                C.x[at] = 0.f;
+            });
+    }
+    for (int m = 0; m + 1 < T.n; ++m) {
+        const TailLevel& L = T.lv[m];
+        const TailLevel& K = T.lv[m + 1];
+        tail_smooth(L, T.sweeps, 0, T.omega);
+        tail_step(
+            tail_cells(L),
+            [&](int t, uint32_t* at, float* v) {
+                *at = (uint32_t)t;
+                *v = dense_residual_value(L.A, L.x, L.b, t);
+                return true;
+            },
+            [&](uint32_t at, float v) { L.r[at] = v; });
+        tail_step(
+            tail_cells(K),
+            [&](int t, uint32_t* at, float* v) {
+                *at = (uint32_t)t;
+                *v = dense_restrict_value(K.A.d, K.A.fluid, 0, T.F, L.A.d, L.r, t);
+                return true;
+            },
+            [&](uint32_t at, float v) {
+                K.b[at] = v;
+                K.x[at] = 0.f;
+            });
+    }
+    const TailLevel& C = T.lv[T.n - 1];
+    if (T.exact) {
+        const int n = T.ex_n[0];
+        for (int i = threadIdx.x; i < n; i += blockDim.x) coarse_apply_row(T.U, T.idx, n, T.Minv, C.b, C.x, i);
+        __syncthreads();
+    } else {
+        tail_smooth(C, T.coarsest_iters, 0, T.omega);
+    }
+    for (int m = T.n - 2; m >= 0; --m) {
+        const TailLevel& L = T.lv[m];
+        const TailLevel& K = T.lv[m + 1];
+        tail_step(
+            tail_cells(L),
+            [&](int t, uint32_t* at, float* v) {
+                return dense_prolong_value(K.A.d, K.x, 0, T.F, nullptr, L.A.d, L.x, L.A.fluid, t, at, v);
+            },
+            [&](uint32_t at, float v) { L.x[at] = v; });
+        tail_smooth(L, T.sweeps, 1, T.omega);
+    }
+    const TailLevel& L0 = T.lv[0];
+    tail_step(
+        T.from_msbg ? T.F.g.nb : T.Fd.D[0] * T.Fd.D[1] * T.Fd.D[2],
+        [&](int t, uint32_t* at, float* v) {
+            return dense_prolong_value(L0.A.d, L0.x, T.from_msbg, T.F, T.xf, T.Fd, T.xf, T.fluid_f, t, at, v);
+        },
+        [&](uint32_t at, float v) { T.xf[at] = v; });
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1479,8 +1659,12 @@ static Coef3 coef(const MGLevel& L) { return Coef3{{L.W[0].p, L.W[1].p, L.W[2].p
 // Slots per CTA.  One-cell blocks take 64 slots (a quarter of the threads), not 256: a level's
 // slot image is sized for its largest group, and 256 one-cell slots (70 KB in FP32, 98 KB in FP64)
 // held every CTA of the level to 3 (or 2) per SM.  At 64 the image stays under 18 KB (25 KB in FP64)
-// and 6 CTAs fit per SM (poisson_256 to 1e-6: 8.05 to 5.90 ms; dam_drop_128 solve 2.08 to 1.85 ms).
-static int slots_per_cta(int r) { return r == 1 ? 64 : std::max(1, std::min(256, 256 / (r * r * r))); }
+// and 6 CTAs fit per SM (poisson_256 to 1e-6: 8.05 to 5.90 ms; dam_drop_128 solve 2.08 to 1.86 ms).
+// Blocks of 2^3 cells take 16 slots (half the threads) rather than 32: more, shorter CTAs on the
+// small levels (dam_drop_128 solve 1.86 to 1.76 ms).
+static int slots_per_cta(int r) {
+    return r == 1 ? 64 : (r == 2 ? 16 : std::max(1, std::min(256, 256 / (r * r * r))));
+}
 
 // Build the CTA batches of one block-structured level from its per-block resolutions.
 static aw_status build_batches(MGLevel& L, const Geo& geo) {
@@ -1733,12 +1917,53 @@ static aw_status coarsest(aw_solver* S, int m, cudaStream_t s) {
     return smooth_level(S, m, S->d.coarsest_iterations, s);
 }
 
+// The uniform levels below level m (the last MSBG level or a uniform one) as one launch
+// (k_dense_tail): restriction into them, their V-cycle and the prolongation back into m.
+static aw_status dense_tail(aw_solver* S, int m, cudaStream_t s) {
+    const int last = (int)S->lv.size() - 1;
+    MGLevel& F = S->lv[m];
+    DenseTail T{};
+    T.n = last - m;
+    T.from_msbg = F.dense ? 0 : 1;
+    for (int j = 0; j < T.n; ++j) {
+        MGLevel& L = S->lv[m + 1 + j];
+        T.lv[j].A = DenseArgs{dview(L), {L.W[0].p, L.W[1].p, L.W[2].p}, L.fluid.p};
+        T.lv[j].x = L.x.p;
+        T.lv[j].b = L.b.p;
+        T.lv[j].r = L.r.p;
+    }
+    if (F.dense) {
+        T.Fd = dview(F);
+        T.xf = F.x.p;
+    } else {
+        T.F = lview(S, m);
+        T.xf = xstore(S, m).f;
+    }
+    T.rf = F.r.p;
+    T.fluid_f = F.fluid.p;
+    T.sweeps = S->d.dense_sweeps;
+    T.coarsest_iters = S->d.coarsest_iterations;
+    T.exact = S->exact ? 1 : 0;
+    T.omega = S->d.omega;
+    if (S->exact) {
+        T.U = uniform_of(S, last);
+        T.idx = S->ex_idx.p;
+        T.ex_n = S->ex_n.p;
+        T.Minv = S->Minv.p;
+    }
+    return launch_dep(S, k_dense_tail, 1, TAIL_THREADS, 0, s, T);
+}
+
 static aw_status vcycle(aw_solver* S, int m, cudaStream_t s) {
     const int last = (int)S->lv.size() - 1;
     if (m == last) return coarsest(S, m, s);
     MGLevel& L = S->lv[m];
     AW_TRY(smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.pre_smooth, s));
     AW_TRY(residual_level(S, m, nullptr, s));
+    if (S->tail && m + 1 == S->tail) {
+        AW_TRY(dense_tail(S, m, s));
+        return smooth_level(S, m, L.dense ? S->d.dense_sweeps : S->d.post_smooth, s, true);
+    }
     AW_TRY(restrict_level(S, m, s));
     AW_TRY(zero_x(S, m + 1, s));
     AW_TRY(vcycle(S, m + 1, s));
@@ -2048,6 +2273,19 @@ static aw_status solver_build(aw_solver* S) {
     S->use_graph = getenv("AW_NO_GRAPH") == nullptr;
     S->use_pdl = getenv("AW_NO_PDL") == nullptr;
     S->use_devloop = getenv("AW_NO_DEVLOOP") == nullptr;
+    // the uniform tail as one launch (FV mode): the uniform levels from the first one of at most
+    // TAIL_MAX_CELLS cells down, at most TAIL_MAX of them, below a level that stores x in FP32
+    // (AW_NO_DENSE_TAIL keeps one launch per step)
+    S->tail = 0;
+    if (!ref && S->nmsbg > 0 && getenv("AW_NO_DENSE_TAIL") == nullptr) {
+        const int nl = (int)S->lv.size();
+        int j = S->nmsbg;
+        while (j < nl && S->lv[j].ncell() > (size_t)TAIL_MAX_CELLS) ++j;
+        bool ok = j < nl && nl - j <= TAIL_MAX && !S->lv[j - 1].half;
+        for (int k = j; ok && k < nl; ++k) ok = S->lv[k].dense && S->lv[k].ncell() <= (size_t)TAIL_MAX_CELLS;
+        if (ok) S->tail = j;
+    }
+
     AW_CUDA(cudaDeviceSynchronize());
     return AW_OK;
 }
