@@ -736,7 +736,7 @@ aw_status flip_step_soa(MsbgState& G, aw_solver* solver, const aw_flip_desc& d, 
     AW_TRY(g2p_sorted(G, soa_out, n, G.pw.cell_start.p, d.alpha, un, uo, s));
     if (ev) AW_CUDA(cudaEventRecord(ev[6], s));
     // 8. RK3 advection through the u_new tiles built for G2P
-    AW_TRY(advect_sorted(G, soa_out, n, G.pw.cell_start.p, d.dt, s));
+    AW_TRY(advect_sorted(G, soa_out, n, G.pw.cell_start.p, d.dt, un, s));
     if (ev) AW_CUDA(cudaEventRecord(ev[7], s));
     if (st) {
         if (ev) AW_CUDA(cudaEventSynchronize(ev[7]));

@@ -226,6 +226,8 @@ struct MsbgState {
     std::vector<uint32_t> h_tile_off;
     uint32_t tile_tot = 0;
     DBuf<float> tiles_new, tiles_old;
+    // per block: holds particles (written by P2G), and its u_new tile was written by this step's G2P
+    DBuf<uint8_t> blk_busy, tile_ok;
     DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for
@@ -289,8 +291,10 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
 aw_status build_tiles(MsbgState& G, const float* u[3], float* tiles, cudaStream_t s);
 aw_status ensure_tiles(MsbgState& G);
 aw_status advect_tiles(MsbgState& G, float* pos, int pos_soa, int64_t n, float dt, const float* tiles, cudaStream_t s);
-// RK3 of cell-sorted SoA particles through G.tiles_new (built for G2P), one CTA per block
-aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, cudaStream_t s);
+// RK3 of cell-sorted SoA particles through G.tiles_new (built for G2P), one CTA per block; un: the
+// face arrays, sampled where G2P wrote no tile (G.tile_ok)
+aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, const float* un[3],
+                        cudaStream_t s);
 aw_status check_device_errors(MsbgState& G, cudaStream_t s);
 aw_status sort_core_soa(MsbgState& G, const float* soa_pos, int64_t n, cudaStream_t s);
 aw_status gather_soa(MsbgState& G, const float* in_soa, int64_t n, float* out_soa, const uint32_t* ids_in,

@@ -507,7 +507,7 @@ template <bool PH>
 __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
                                                  const uint32_t* __restrict__ pid, const float* __restrict__ phase,
-                                                 int smem_floats) {
+                                                 int smem_floats, uint8_t* __restrict__ occ) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ uint32_t noff[27][3];
@@ -527,9 +527,13 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
     const int b = blockIdx.x;
     const int r = L.res[b];
-    if (!r) return;
+    if (!r) {
+        if (threadIdx.x == 0) occ[b] = 0;
+        return;
+    }
     const uint32_t c0 = L.off[0][b];
     const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
+    if (threadIdx.x == 0) occ[b] = p1 > p0 ? 1 : 0;  // read by G2P: blocks around it skip their tiles
     if (p0 == p1) return;
     const Geo& g = L.g;
     // the block's cell starts in the sorted array, after the tiles (smem_floats floats)
@@ -1146,6 +1150,7 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             maxres = std::max(maxres, r);
             minres = std::min(minres, r);
         }
+    AW_TRY(G.blk_busy.ensure(std::max(G.nb, 1)));
     const int NVt = ph ? 9 : 6;
     // the largest tile, or one private tile per warp for blocks of at most two cells per edge
     // 512-thread CTAs: the aw_p2g call takes 0.43 ms on the 3-level dam_drop_128 against 0.48 ms
@@ -1163,11 +1168,11 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             // always opted in: the pair queues' static shared memory counts against the default 48 KB too
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase,
-                                                           (int)smem_f);
+                                                           (int)smem_f, G.blk_busy.p);
         } else {
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr,
-                                                            (int)smem_f);
+                                                            (int)smem_f, G.blk_busy.p);
         }
         AW_LAUNCH();
     }
@@ -1572,7 +1577,8 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                                                            const uint32_t* __restrict__ cs, float alpha, Field3 un,
                                                            Field3 uo, const uint32_t* __restrict__ toff,
                                                            float* __restrict__ tn, int* err, int polls, int arm_only,
-                                                           DropIn D) {
+                                                           DropIn D, const uint8_t* __restrict__ occ,
+                                                           uint8_t* __restrict__ tile_ok) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ NbFaces nbr[27];
@@ -1583,6 +1589,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     const uint32_t c0 = L.off[0][b];
     const uint32_t p0 = cs[c0], p1 = cs[c0 + (uint32_t)(r * r * r)];
     const uint32_t nchunk = (p1 - p0 + G2P_CHUNK - 1) / G2P_CHUNK;
+    if (!tn && !nchunk) return;  // no particles and no u_new tile to write
     const uint32_t tb = tile_block(r);
     float* tw = sm;
     float* stage = sm + tb;  // tb is a multiple of 4 floats
@@ -1603,6 +1610,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
     // and issues their loads together.
     int cb[3];
     bcoord(L.g, b, cb);
+    int busy = 0;
     if (threadIdx.x < 27) {
         const int d = threadIdx.x;
         const int nc[3] = {cb[0] + d % 3 - 1, cb[1] + (d / 3) % 3 - 1, cb[2] + d / 9 - 1};
@@ -1611,8 +1619,17 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
         nbr[d].r = rn;
 #pragma unroll
         for (int k = 0; k < 3; ++k) nbr[d].off[k] = rn ? L.off[1 + k][nb] : 0u;
+        busy = occ && nb >= 0 && occ[nb];
     }
-    __syncthreads();
+    // No particle in this block or its 26 neighbours (occ, from this step's P2G): nothing here to
+    // interpolate for, and a stage point of the advection reaches this block only from a particle more
+    // than a block away; tile_ok[b] = 0 sends such a point to the face arrays instead of the tile.
+    // (A block with particles of its own never returns here, so no bulk copy is left in flight.)
+    if (!__syncthreads_or(busy) && occ) {
+        if (threadIdx.x == 0) tile_ok[b] = 0;
+        return;
+    }
+    if (tile_ok && threadIdx.x == 0) tile_ok[b] = 1;
     {
         const int R1 = r + 1, R2 = r + 2;
         const int TA = (int)tile_axis(r);
@@ -1705,6 +1722,7 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
 // point, not once per component.
 struct PointTile {
     const float* t;  // tile of the block holding the point (nullptr: inactive block, velocity 0)
+    int b;           // that block
     int r;
     float o[3];
     float invh;
@@ -1728,6 +1746,7 @@ __device__ inline PointTile point_tile(const LevelView& L, const int cb[3], int 
     if (!inner) point_block(L.g, X, pc);
     if (pc[0] == cb[0] && pc[1] == cb[1] && pc[2] == cb[2]) {
         T.t = tl;
+        T.b = -1;
         T.r = r;
 #pragma unroll
         for (int k = 0; k < 3; ++k) T.o[k] = o[k];
@@ -1735,6 +1754,7 @@ __device__ inline PointTile point_tile(const LevelView& L, const int cb[3], int 
         return T;
     }
     const int b2 = bidx(L.g, pc[0], pc[1], pc[2]);
+    T.b = b2;
     T.r = L.res[b2];
     T.t = T.r ? tg + toff[b2] : nullptr;
     T.invh = T.r ? 1.f / fcell(L.g, T.r) : 0.f;
@@ -1743,10 +1763,17 @@ __device__ inline PointTile point_tile(const LevelView& L, const int cb[3], int 
     return T;
 }
 
-__global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restrict__ soa, int64_t n,
+// The MAC sample of u_new at X from the face arrays (the rare stage point that lands in a block whose
+// tile G2P did not write); not inlined, so the common path keeps its registers.
+__device__ __noinline__ void sample_faces3(const LevelView& L, const Field3& un, const float X[3], float out[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) out[a] = sample_comp(L, un.c[a], a, X);
+}
+
+__global__ void __launch_bounds__(256, 4) k_advect_tile(LevelView L, float* __restrict__ soa, int64_t n,
                                                      const uint32_t* __restrict__ cs, float dt,
                                                      const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
-                                                     int* err, DropIn D) {
+                                                     int* err, DropIn D, const uint8_t* __restrict__ tile_ok, Field3 un) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
     const int b = blockIdx.x;
@@ -1789,6 +1816,8 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
             const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
             if (T.t == sm) {  // shared-memory loads when the point stays in the block
                 tile_interp3(sm, r, o, invh, y, k2);
+            } else if (T.t && tile_ok && !tile_ok[T.b]) {  // no tile written this step: the face arrays
+                sample_faces3(L, un, y, k2);
             } else if (T.t) {
                 tile_interp3(T.t, T.r, T.o, T.invh, y, k2);
             } else {
@@ -1801,6 +1830,8 @@ __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restr
             const PointTile T = point_tile(L, cb, r, o, invh, sm, toff, tn_g, y);
             if (T.t == sm) {  // shared-memory loads when the point stays in the block
                 tile_interp3(sm, r, o, invh, y, k3);
+            } else if (T.t && tile_ok && !tile_ok[T.b]) {  // no tile written this step: the face arrays
+                sample_faces3(L, un, y, k3);
             } else if (T.t) {
                 tile_interp3(T.t, T.r, T.o, T.invh, y, k3);
             } else {
@@ -1861,6 +1892,7 @@ aw_status ensure_tiles(MsbgState& G) {
     AW_CUDA(cudaMemcpy(G.tile_off.p, G.h_tile_off.data(), G.nb * sizeof(uint32_t), cudaMemcpyHostToDevice));
     AW_TRY(G.tiles_new.ensure(std::max<uint32_t>(acc, 4)));
     AW_TRY(G.tiles_old.ensure(std::max<uint32_t>(acc, 4)));
+    AW_TRY(G.tile_ok.ensure(std::max(G.nb, 1)));
     AW_TRY(G.err.ensure(4));
     AW_CUDA(cudaMemset(G.err.p, 0, 4 * sizeof(int)));
     return AW_OK;
@@ -1910,7 +1942,8 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
     const int polls = arm_only ? 1 << 10 : 1 << 20;
     G.test_copy_timeout = false;
     k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), soa, n, cs, alpha, fa, fb, G.tile_off.p, G.tiles_new.p,
-                                                 G.err.p + 1, polls, arm_only, DropIn{nullptr, nullptr, nullptr});
+                                                 G.err.p + 1, polls, arm_only, DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p,
+                                                 G.blk_busy.p ? G.tile_ok.p : nullptr);
     AW_LAUNCH();
     k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
     AW_LAUNCH();
@@ -1972,7 +2005,8 @@ __global__ void k_sample_tiles(LevelView L, PArr pts, int64_t n, const uint32_t*
     for (int a = 0; a < 3; ++a) out[3 * i + a] = sample_tiles(L, toff, tiles, a, X);
 }
 
-aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, cudaStream_t s) {
+aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, float dt, const float* un[3],
+                        cudaStream_t s) {
     if (n <= 0) return AW_OK;
     int maxres = 0;
     for (int r : G.h_res) maxres = std::max(maxres, r);
@@ -1980,7 +2014,8 @@ aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs,
     if (smem > 48 * 1024)
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1,
-                                          DropIn{nullptr, nullptr, nullptr});
+                                          DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p ? G.tile_ok.p : nullptr,
+                                          Field3{{un[0], un[1], un[2]}});
     AW_LAUNCH();
     return AW_OK;
 }
@@ -2524,7 +2559,8 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
         AW_CUDA(cudaFuncSetAttribute(k_g2p_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
         k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,
-                                                     nullptr, G.err.p + 1, 1 << 20, 0, DropIn{W.sorted, d_vel, W.hash.p});
+                                                     nullptr, G.err.p + 1, 1 << 20, 0, DropIn{W.sorted, d_vel, W.hash.p},
+                                                     nullptr, nullptr);
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_vel, W.hash.p, 0, alpha);
         AW_LAUNCH();
@@ -2561,7 +2597,7 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
         const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, dt, G.tile_off.p, G.tiles_new.p,
-                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p});
+                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p}, nullptr, Field3{});
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_pos, W.hash.p, 1, 0.f);
         AW_LAUNCH();

@@ -46,6 +46,7 @@ struct MGLevel {
     DBuf<int4> desc[3];
     std::vector<int> h_blocks[3];  // block of every slot, batch order
     DBuf<int> meta[3];             // slot metadata (NMETA fields x slots, field-major)
+    DBuf<int> blk[3];              // block of every slot, batch order, on the device
     int ndesc[3] = {0, 0, 0};
     // dynamic shared memory of the batched kernels on this level
     size_t smem_smooth = 0, smem_x64 = 0, smem_prolong = 0, smem_meta = 0;
@@ -657,7 +658,9 @@ __device__ __forceinline__ T residual_cell(const SlotImage<T, R>& S, int sl, int
     return rv;
 }
 
-template <int R, class Src>
+// DOTX: the per-CTA partial sums are of x . r instead of r . r (with a zero right-hand side, the
+// d . (-A d) of a conjugate-gradient step, taken while d is staged)
+template <int R, class Src, bool DOTX = false>
 __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred, const Src& x, const float* __restrict__ bvec,
                                      const Coef3& W, const uint8_t* __restrict__ fluid, const Batch& B, int check_fluid,
                                      float* __restrict__ rout, double* __restrict__ rout64, double* __restrict__ part) {
@@ -679,7 +682,8 @@ __device__ inline void residual_body(int4 d, unsigned char* smraw, double* dred,
         const T rv = residual_cell<R>(S, sl, i, check_fluid);
         if (rout) rout[S.off(0, sl) + i] = (float)rv;
         if (rout64) rout64[S.off(0, sl) + i] = (double)rv;
-        acc += (double)rv * (double)rv;
+        if (DOTX) acc += (double)S.xs[sl * Gm::X3 + xi3(i % R, (i / R) % R, i / Gm::rr, Gm::R2)] * (double)rv;
+        else acc += (double)rv * (double)rv;
     }
     if (part) {
         double tsum = block_sum(acc, dred);
@@ -702,6 +706,19 @@ __global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_residual(Src x, co
 #define AW_RESID(R) residual_body<R>(d, smraw, dred, x, bvec, W, fluid, B, check_fluid, rout, rout64, part)
     AW_SWITCH_RES(d.z, AW_RESID)
 #undef AW_RESID
+}
+
+// qn = -A d in FP64 and the per-CTA partial sums of d . qn (the mixed-precision CG step), in one pass
+__global__ void __launch_bounds__(NT, AW_BLOCK_CTAS_PER_SM) k_apply_dot(SrcD x, const float* __restrict__ zero, Coef3 W,
+                                                                  const uint8_t* __restrict__ fluid, Batch B,
+                                                                  int check_fluid, double* __restrict__ qn,
+                                                                  double* __restrict__ part) {
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double dred[32];
+    const int4 d = B.desc[blockIdx.x];
+#define AW_APPLY(R) residual_body<R, SrcD, true>(d, smraw, dred, x, zero, W, fluid, B, check_fluid, nullptr, qn, part)
+    AW_SWITCH_RES(d.z, AW_APPLY)
+#undef AW_APPLY
 }
 
 template <int R>
@@ -1710,54 +1727,67 @@ static aw_status build_batches(MGLevel& L, const Geo& geo) {
 }
 static Batch batch(const MGLevel& L, int k) { return Batch{L.desc[k].p, L.meta[k].p, (int)L.h_blocks[k].size()}; }
 
-// Per-level host copy of what the slot metadata needs.
-struct HostLevel {
-    std::vector<int> res;
-    std::vector<uint32_t> off[4];
+// Slot metadata of one batch of level m, laid out in batch order (field-major): block id, offsets,
+// the six face neighbours (cell offset, kind, block) and the block's cells on the adjacent levels.
+// One thread per slot, from the level arrays already on the device (no host copy of the offsets).
+struct MetaSrc {
+    const int* res;
+    const uint32_t* off[4];
 };
-
-// Lay out the slot metadata of level m in batch order (field-major): block id, offsets, the six
-// face neighbours (cell offset, kind, block) and the block's cells on the adjacent levels.
-static aw_status build_meta(MGLevel& L, const Geo& geo, const HostLevel& h, const HostLevel* finer,
-                            const HostLevel* coarser) {
+__global__ void k_build_meta(Geo geo, const int* __restrict__ blocks, int n, MetaSrc h, MetaSrc finer, MetaSrc coarser,
+                             int* __restrict__ mt) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const int b = blocks[j];
+    const int r = h.res[b];
+    auto F = [&](int f, int v) { mt[(size_t)f * n + j] = v; };
+    F(MF_BLOCK, b);
+    for (int q = 0; q < 4; ++q) F(MF_OFF + q, (int)h.off[q][b]);
+    int c[3];
+    bcoord(geo, b, c);
+    for (int a = 0; a < 3; ++a)
+        for (int sd = 0; sd < 2; ++sd) {
+            const int f = MF_NB + 3 * (2 * a + sd);
+            int nc[3] = {c[0], c[1], c[2]};
+            nc[a] += sd ? 1 : -1;
+            int o = 0, kind = NB_NONE, nbk = 0;
+            if (inside(geo, nc)) {
+                const int q = bidx(geo, nc[0], nc[1], nc[2]);
+                const int rn = h.res[q];
+                if (rn) {
+                    o = (int)h.off[0][q];
+                    kind = rn == r ? NB_SAME : (rn < r ? NB_COARSE : NB_FINE);
+                    nbk = q;
+                }
+            }
+            F(f, o);
+            F(f + 1, kind);
+            F(f + 2, nbk);
+        }
+    F(MF_FINE_OFF, finer.res ? (int)finer.off[0][b] : 0);
+    F(MF_FINE_RES, finer.res ? finer.res[b] : 0);
+    F(MF_COARSE_OFF, coarser.res ? (int)coarser.off[0][b] : 0);
+    F(MF_COARSE_RES, coarser.res ? coarser.res[b] : 0);
+}
+static MetaSrc meta_src(const MGLevel* L) {
+    MetaSrc m{};
+    if (!L) return m;
+    m.res = L->res.p;
+    for (int k = 0; k < 4; ++k) m.off[k] = L->off[k].p;
+    return m;
+}
+// The slot metadata of level m's three batches, built on the device.
+static aw_status build_meta(MGLevel& L, const Geo& geo, const MGLevel* finer, const MGLevel* coarser, cudaStream_t s) {
     for (int k = 0; k < 3; ++k) {
         const std::vector<int>& blocks = L.h_blocks[k];
         const size_t n = blocks.size();
         if (!n) continue;
-        std::vector<int> mt(NMETA * n, 0);
-        for (size_t j = 0; j < n; ++j) {
-            const int b = blocks[j];
-            const int r = h.res[b];
-            auto F = [&](int f) -> int& { return mt[(size_t)f * n + j]; };
-            F(MF_BLOCK) = b;
-            for (int q = 0; q < 4; ++q) F(MF_OFF + q) = (int)h.off[q][b];
-            int c[3];
-            bcoord(geo, b, c);
-            for (int a = 0; a < 3; ++a)
-                for (int sd = 0; sd < 2; ++sd) {
-                    const int f = MF_NB + 3 * (2 * a + sd);
-                    int nc[3] = {c[0], c[1], c[2]};
-                    nc[a] += sd ? 1 : -1;
-                    F(f + 1) = NB_NONE;
-                    if (!inside(geo, nc)) continue;
-                    const int nbk = bidx(geo, nc[0], nc[1], nc[2]);
-                    const int rn = h.res[nbk];
-                    if (!rn) continue;
-                    F(f) = (int)h.off[0][nbk];
-                    F(f + 1) = rn == r ? NB_SAME : (rn < r ? NB_COARSE : NB_FINE);
-                    F(f + 2) = nbk;
-                }
-            if (finer) {
-                F(MF_FINE_OFF) = (int)finer->off[0][b];
-                F(MF_FINE_RES) = finer->res[b];
-            }
-            if (coarser) {
-                F(MF_COARSE_OFF) = (int)coarser->off[0][b];
-                F(MF_COARSE_RES) = coarser->res[b];
-            }
-        }
-        AW_TRY(L.meta[k].ensure(mt.size()));
-        AW_CUDA(cudaMemcpy(L.meta[k].p, mt.data(), mt.size() * sizeof(int), cudaMemcpyHostToDevice));
+        AW_TRY(L.blk[k].ensure(n));
+        AW_CUDA(cudaMemcpyAsync(L.blk[k].p, blocks.data(), n * sizeof(int), cudaMemcpyHostToDevice, s));
+        AW_TRY(L.meta[k].ensure(NMETA * n));
+        k_build_meta<<<nblk(n), 256, 0, s>>>(geo, L.blk[k].p, (int)n, meta_src(&L), meta_src(finer), meta_src(coarser),
+                                            L.meta[k].p);
+        AW_LAUNCH();
     }
     return AW_OK;
 }
@@ -2178,22 +2208,11 @@ static aw_status solver_build(aw_solver* S) {
         }
     }
     S->nmsbg = nlev;
-    {
-        std::vector<HostLevel> hl(S->nmsbg);
-        for (int m = 0; m < S->nmsbg; ++m) {
-            MGLevel& L = S->lv[m];
-            hl[m].res = L.h_res;
-            for (int k = 0; k < 4; ++k) {
-                hl[m].off[k].resize(nb);
-                AW_CUDA(cudaMemcpy(hl[m].off[k].data(), L.off[k].p, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost));
-            }
-        }
-        for (int m = 0; m < S->nmsbg; ++m) {
-            MGLevel& L = S->lv[m];
-            AW_TRY(build_meta(L, G.geo, hl[m], m > 0 ? &hl[m - 1] : nullptr, m + 1 < S->nmsbg ? &hl[m + 1] : nullptr));
-            S->smem_max = std::max({S->smem_max, L.smem_smooth, L.smem_prolong, L.smem_meta});
-            S->smem_max64 = std::max(S->smem_max64, L.smem_x64);
-        }
+    for (int m = 0; m < S->nmsbg; ++m) {
+        MGLevel& L = S->lv[m];
+        AW_TRY(build_meta(L, G.geo, m > 0 ? &S->lv[m - 1] : nullptr, m + 1 < S->nmsbg ? &S->lv[m + 1] : nullptr, s));
+        S->smem_max = std::max({S->smem_max, L.smem_smooth, L.smem_prolong, L.smem_meta});
+        S->smem_max64 = std::max(S->smem_max64, L.smem_x64);
     }
     // uniform continuation below one cell per block (FV mode)
     size_t used = (size_t)S->nmsbg;
@@ -2247,6 +2266,7 @@ static aw_status solver_build(aw_solver* S) {
         AW_CUDA(cudaFuncSetAttribute(k_restrict, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max));
     }
     AW_CUDA(cudaFuncSetAttribute(k_residual<SrcD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
+    AW_CUDA(cudaFuncSetAttribute(k_apply_dot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S->smem_max64));
     if (S->d.precision == AW_PRECISION_MIXED) {
         const size_t nc0 = S->lv[0].ncell();
         AW_TRY(S->cg_r.ensure(nc0));
@@ -2485,11 +2505,9 @@ static aw_status cg_body(aw_solver* S, double* p, unsigned ndot, cudaStream_t s,
     AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 0));
     AW_TRY(launch_dep(S, k_cg_direction, nblk(nc), 256, 0, s, S->cg_d.p, L0.x.p, L0.fluid.p, sc, 0,
                       (const int*)(S->cgst.p + 1), nc));
-    AW_TRY(launch_dep(S, k_residual<SrcD>, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p}, S->cg_zero.p,
-                      coef(L0), L0.fluid.p, batch(L0, 2), cf, (float*)nullptr, S->cg_q.p, (double*)nullptr));
-    AW_TRY(launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_d.p, S->cg_q.p, (const float*)nullptr, L0.fluid.p, nc,
-                      S->partials.p));
-    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 2));
+    AW_TRY(launch_dep(S, k_apply_dot, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p}, S->cg_zero.p,
+                      coef(L0), L0.fluid.p, batch(L0, 2), cf, S->cg_q.p, S->partials.p));
+    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, L0.ndesc[2], sc + 2));
     AW_TRY(launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, L0.fluid.p, nc,
                       S->partials.p));
     AW_TRY(launch_dep(S, k_copy_scalar, 1, 1, 0, s, sc, 1, 0));
@@ -2753,14 +2771,11 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
                                  restart ? 1 : 0, (const int*)nullptr, nc)) != AW_OK)
                 break;
             // qn = -A d ; sc[2] = d . qn
-            if ((st = launch_dep(S, k_residual<SrcD>, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p},
-                                 S->cg_zero.p, coef(L0), L0.fluid.p, batch(L0, 2), cf, (float*)nullptr, S->cg_q.p,
-                                 (double*)nullptr)) != AW_OK)
+            if ((st = launch_dep(S, k_apply_dot, (unsigned)L0.ndesc[2], 256, L0.smem_x64, s, SrcD{S->cg_d.p},
+                                 S->cg_zero.p, coef(L0), L0.fluid.p, batch(L0, 2), cf, S->cg_q.p, S->partials.p)) !=
+                AW_OK)
                 break;
-            if ((st = launch_dep(S, k_dot64, ndot, 256, 0, s, S->cg_d.p, S->cg_q.p, (const float*)nullptr, L0.fluid.p, nc,
-                                 S->partials.p)) != AW_OK)
-                break;
-            if ((st = launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, sc + 2)) != AW_OK) break;
+            if ((st = launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, L0.ndesc[2], sc + 2)) != AW_OK) break;
             // p += alpha d ; r -= alpha A d ; FP32 copy of r for the next V-cycle ; rho_old = rho
             if ((st = launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc,
                                  L0.fluid.p, nc, S->partials.p)) != AW_OK)
