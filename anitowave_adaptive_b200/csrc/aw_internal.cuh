@@ -61,7 +61,10 @@ struct DBuf {
         n = count;
         return AW_OK;
     }
-    aw_status ensure(size_t count) { return count <= n ? AW_OK : alloc(count); }
+    // Grow-only storage.  A buffer that has to grow again takes a quarter more than asked for: a level
+    // map that keeps changing (a spreading liquid) then reallocates a few times instead of at every
+    // new layout (each cudaFree synchronises the device).  A first allocation is exact.
+    aw_status ensure(size_t count) { return count <= n ? AW_OK : alloc(n == 0 ? count : count + count / 4); }
     void free() {
         if (p) cudaFree(p);
         p = nullptr;
