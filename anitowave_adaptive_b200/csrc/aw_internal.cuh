@@ -231,6 +231,7 @@ struct MsbgState {
     DBuf<float> tiles_new, tiles_old;
     // per block: holds particles (written by P2G), and its u_new tile was written by this step's G2P
     DBuf<uint8_t> blk_busy, tile_ok;
+    DBuf<int> blk_order;  // blocks by descending particle count (the per-block kernels' CTA order)
     DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for

@@ -507,7 +507,8 @@ template <bool PH>
 __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const float* __restrict__ soa, int64_t n,
                                                  const uint32_t* __restrict__ cs, FaceAcc acc,
                                                  const uint32_t* __restrict__ pid, const float* __restrict__ phase,
-                                                 int smem_floats, uint8_t* __restrict__ occ) {
+                                                 int smem_floats, uint8_t* __restrict__ occ,
+                                                 const int* __restrict__ order) {
     extern __shared__ float sm[];
     __shared__ int nres[27];
     __shared__ uint32_t noff[27][3];
@@ -525,7 +526,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     __shared__ int ncnt_tmp[P2G_NEAR_CELLS];
     __shared__ uint32_t xq_v[(P2G_THREADS / 32) * P2G_XQ];
     __shared__ uint8_t xq_d[(P2G_THREADS / 32) * P2G_XQ];
-    const int b = blockIdx.x;
+    const int b = order ? order[blockIdx.x] : (int)blockIdx.x;
     const int r = L.res[b];
     if (!r) {
         if (threadIdx.x == 0) occ[b] = 0;
@@ -1087,6 +1088,35 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     if (cmask) p2g_flush_tile<PH>(nres, noff, rc, cm, cp, cq, acc);
 }
 
+// The blocks in descending order of particle count, by buckets of equal floor(log2(count)) (empty
+// and inactive blocks last), for the CTA order of the per-block particle kernels: CTAs start in
+// launch order, so the heaviest blocks start first and the last wave holds light ones.  The order
+// within a bucket follows the atomics (it has no effect on the results).
+__global__ void __launch_bounds__(1024) k_block_order(LevelView L, const uint32_t* __restrict__ cs, int nb,
+                                                      int* __restrict__ order) {
+    constexpr int NBK = 33;
+    __shared__ int hist[NBK], base[NBK];
+    auto bucket = [&](int b) {
+        const int r = L.res[b];
+        if (!r) return 0;
+        const uint32_t c0 = L.off[0][b];
+        return 32 - __clz((int)(cs[c0 + (uint32_t)(r * r * r)] - cs[c0]));
+    };
+    if (threadIdx.x < NBK) hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) atomicAdd(&hist[bucket(b)], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int k = NBK - 1; k >= 0; --k) {
+            base[k] = acc;
+            acc += hist[k];
+        }
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < nb; b += blockDim.x) order[atomicAdd(&base[bucket(b)], 1)] = b;
+}
+
 // u = P / m where m > 1e-6, else 0 (normalizeVelocity, P2G.cuh:139-171), over the three axes
 __global__ void k_p2g_normalize(const float* __restrict__ m0, const float* __restrict__ P0, float* u0, uint32_t n0,
                                 const float* __restrict__ m1, const float* __restrict__ P1, float* u1, uint32_t n1,
@@ -1151,6 +1181,11 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             minres = std::min(minres, r);
         }
     AW_TRY(G.blk_busy.ensure(std::max(G.nb, 1)));
+    AW_TRY(G.blk_order.ensure(std::max(G.nb, 1)));
+    if (n > 0) {
+        k_block_order<<<1, 1024, 0, s>>>(G.view0(), cstart, G.nb, G.blk_order.p);
+        AW_LAUNCH();
+    }
     const int NVt = ph ? 9 : 6;
     // the largest tile, or one private tile per warp for blocks of at most two cells per edge
     // 512-thread CTAs: the aw_p2g call takes 0.43 ms on the 3-level dam_drop_128 against 0.48 ms
@@ -1168,11 +1203,11 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             // always opted in: the pair queues' static shared memory counts against the default 48 KB too
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase,
-                                                           (int)smem_f, G.blk_busy.p);
+                                                           (int)smem_f, G.blk_busy.p, G.blk_order.p);
         } else {
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr,
-                                                            (int)smem_f, G.blk_busy.p);
+                                                            (int)smem_f, G.blk_busy.p, G.blk_order.p);
         }
         AW_LAUNCH();
     }
@@ -1578,11 +1613,12 @@ __global__ void __launch_bounds__(G2P_THREADS) k_g2p_fused(LevelView L, float* _
                                                            Field3 uo, const uint32_t* __restrict__ toff,
                                                            float* __restrict__ tn, int* err, int polls, int arm_only,
                                                            DropIn D, const uint8_t* __restrict__ occ,
-                                                           uint8_t* __restrict__ tile_ok, int untiled) {
+                                                           uint8_t* __restrict__ tile_ok, int untiled,
+                                                           const int* __restrict__ order) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar[2];
     __shared__ NbFaces nbr[27];
-    const int b = blockIdx.x;
+    const int b = order ? order[blockIdx.x] : (int)blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
     if (D.perm && !sort_reusable(D.hash, true)) return;
@@ -1775,10 +1811,11 @@ __device__ __forceinline__ void sample_faces3(const LevelView& L, const Field3& 
 __global__ void __launch_bounds__(256) k_advect_tile(LevelView L, float* __restrict__ soa, int64_t n,
                                                      const uint32_t* __restrict__ cs, float dt,
                                                      const uint32_t* __restrict__ toff, const float* __restrict__ tn_g,
-                                                     int* err, DropIn D, const uint8_t* __restrict__ tile_ok, Field3 un) {
+                                                     int* err, DropIn D, const uint8_t* __restrict__ tile_ok, Field3 un,
+                                                     const int* __restrict__ order) {
     extern __shared__ __align__(16) float sm[];
     __shared__ __align__(8) uint64_t bar;
-    const int b = blockIdx.x;
+    const int b = order ? order[blockIdx.x] : (int)blockIdx.x;
     const int r = L.res[b];
     if (!r) return;
     if (D.perm && !sort_reusable(D.hash, false)) return;
@@ -1948,7 +1985,7 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
     G.test_copy_timeout = false;
     k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), soa, n, cs, alpha, fa, fb, G.tile_off.p, G.tiles_new.p,
                                                  G.err.p + 1, polls, arm_only, DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p,
-                                                 G.blk_busy.p ? G.tile_ok.p : nullptr, untiled);
+                                                 G.blk_busy.p ? G.tile_ok.p : nullptr, untiled, G.blk_order.p);
     AW_LAUNCH();
     k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
     AW_LAUNCH();
@@ -2020,7 +2057,7 @@ aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs,
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1,
                                           DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p ? G.tile_ok.p : nullptr,
-                                          Field3{{un[0], un[1], un[2]}});
+                                          Field3{{un[0], un[1], un[2]}}, G.blk_order.p);
     AW_LAUNCH();
     return AW_OK;
 }
@@ -2565,7 +2602,7 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
         Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
         k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,
                                                      nullptr, G.err.p + 1, 1 << 20, 0, DropIn{W.sorted, d_vel, W.hash.p},
-                                                     nullptr, nullptr, 0);
+                                                     nullptr, nullptr, 0, nullptr);
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_vel, W.hash.p, 0, alpha);
         AW_LAUNCH();
@@ -2602,7 +2639,7 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
         const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, dt, G.tile_off.p, G.tiles_new.p,
-                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p}, nullptr, Field3{});
+                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p}, nullptr, Field3{}, nullptr);
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_pos, W.hash.p, 1, 0.f);
         AW_LAUNCH();
