@@ -877,13 +877,15 @@ __global__ void k_cg_direction(double* __restrict__ d, const float* __restrict__
 }
 // qn = -A d (the residual kernel with a zero right-hand side); alpha = rho / (d . A d)
 // p += alpha d; r += alpha qn; and the FP32 copy of r for the next V-cycle
-// ... and the per-CTA partial sums of |r|^2 over fluid cells (grid-stride, part[blockIdx.x])
+// ... and the per-CTA partial sums of |r|^2 over fluid cells (grid-stride, part[blockIdx.x]);
+// rho_old = rho for the next iteration's direction (sc[1] is read by no CTA of this kernel)
 __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, float* __restrict__ rf,
-                            const double* __restrict__ d, const double* __restrict__ qn, const double* __restrict__ sc,
+                            const double* __restrict__ d, const double* __restrict__ qn, double* __restrict__ sc,
                             const uint8_t* __restrict__ fluid, size_t n, double* __restrict__ part) {
     pdl_wait();
     const double dq = -sc[2];
     const double alpha = dq != 0.0 ? sc[0] / dq : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc[1] = sc[0];
     double acc = 0.0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
         p[i] += alpha * d[i];
@@ -902,12 +904,20 @@ __global__ void k_cg_update(double* __restrict__ p, double* __restrict__ r, floa
         if (threadIdx.x == 0) part[blockIdx.x] = t;
     }
 }
-// End of one CG iteration inside the device-side loop: count it, clear the restart flag, and run the
-// loop body again while the residual (||r||^2 in norm2) is finite, at or above the tolerance and the
-// iteration limit is not reached.  st = {iterations, restart, limit}, prm = {||b||, tolerance}.
-__global__ void k_cg_check(cudaGraphConditionalHandle h, const double* __restrict__ norm2,
-                           const double* __restrict__ prm, int* st) {
-    const double rel = sqrt(norm2[0]) / prm[0];
+// End of one CG iteration inside the device-side loop (one CTA of 256 threads): ||r||^2 into norm2
+// from k_cg_update's partial sums (the reduction of k_reduce_sum, so the host loop reads the same
+// value), count the iteration, clear the restart flag, and run the loop body again while the
+// residual is finite, at or above the tolerance and the iteration limit is not reached.
+// st = {iterations, restart, limit}, prm = {||b||, tolerance}.
+__global__ void k_cg_check(cudaGraphConditionalHandle h, const double* __restrict__ part, int nparts,
+                           double* __restrict__ norm2, const double* __restrict__ prm, int* st) {
+    __shared__ double red[32];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) acc += part[i];
+    const double t = block_sum(acc, red);
+    if (threadIdx.x != 0) return;
+    norm2[0] = t;
+    const double rel = sqrt(t) / prm[0];
     const int it = st[0] + 1;
     st[0] = it;
     st[1] = 0;
@@ -2510,9 +2520,7 @@ static aw_status cg_body(aw_solver* S, double* p, unsigned ndot, cudaStream_t s,
     AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, L0.ndesc[2], sc + 2));
     AW_TRY(launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc, L0.fluid.p, nc,
                       S->partials.p));
-    AW_TRY(launch_dep(S, k_copy_scalar, 1, 1, 0, s, sc, 1, 0));
-    AW_TRY(launch_dep(S, k_reduce_sum, 1, 256, 0, s, S->partials.p, (int)ndot, S->norm.p));
-    k_cg_check<<<1, 1, 0, s>>>(h, S->norm.p, S->cgprm.p, S->cgst.p);
+    k_cg_check<<<1, 256, 0, s>>>(h, (const double*)S->partials.p, (int)ndot, S->norm.p, S->cgprm.p, S->cgst.p);
     AW_LAUNCH();
     return AW_OK;
 }
@@ -2780,7 +2788,6 @@ extern "C" aw_status aw_solve(aw_solver* S, const float* d_b, void* d_p, int32_t
             if ((st = launch_dep(S, k_cg_update, ndot, 256, 0, s, p, S->cg_r.p, L0.b.p, S->cg_d.p, S->cg_q.p, sc,
                                  L0.fluid.p, nc, S->partials.p)) != AW_OK)
                 break;
-            if ((st = launch_dep(S, k_copy_scalar, 1, 1, 0, s, sc, 1, 0)) != AW_OK) break;
             ++it;
             restart = false;
             st = read_norm(S, ndot, s, &rn);  // ||r|| from k_cg_update's partial sums
