@@ -232,6 +232,7 @@ struct MsbgState {
     // per block: holds particles (written by P2G), and its u_new tile was written by this step's G2P
     DBuf<uint8_t> blk_busy, tile_ok;
     DBuf<int> blk_order;  // blocks by descending particle count (the per-block kernels' CTA order)
+    bool blk_order_on = false;  // blk_order holds this step's order (small grids only)
     DBuf<float> tiles_bar_new, tiles_bar_old;  // adjoint tiles (VJP kernels)
     DBuf<float> adj_u[3], adj_m[3];             // forward P2G recomputed by aw_vjp_p2g
     DBuf<float> p2g_P[3];                       // P2G momentum accumulator when MOMENTUM_* is not asked for

@@ -1088,6 +1088,7 @@ __global__ void __launch_bounds__(P2G_THREADS, 2) k_p2g_own(LevelView L, const f
     if (cmask) p2g_flush_tile<PH>(nres, noff, rc, cm, cp, cq, acc);
 }
 
+constexpr int kOrderMaxBlocks = 8192;  // grids up to this many blocks take their blocks heaviest first
 // The blocks in descending order of particle count, by buckets of equal floor(log2(count)) (empty
 // and inactive blocks last), for the CTA order of the per-block particle kernels: CTAs start in
 // launch order, so the heaviest blocks start first and the last wave holds light ones.  The order
@@ -1181,11 +1182,17 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             minres = std::min(minres, r);
         }
     AW_TRY(G.blk_busy.ensure(std::max(G.nb, 1)));
-    AW_TRY(G.blk_order.ensure(std::max(G.nb, 1)));
-    if (n > 0) {
+    // Heaviest blocks first, on grids of at most kOrderMaxBlocks blocks: dam_drop_128 (4096 blocks)
+    // G2P 0.084 to 0.077 ms and advection 0.149 to 0.137 ms; on dam_drop2_256 (32768 blocks, many
+    // more waves) the one-CTA ordering pass cost more than it saved (P2G 2.02 to 2.07 ms, G2P 0.441
+    // to 0.457 ms).
+    G.blk_order_on = n > 0 && G.nb <= kOrderMaxBlocks;
+    if (G.blk_order_on) {
+        AW_TRY(G.blk_order.ensure(std::max(G.nb, 1)));
         k_block_order<<<1, 1024, 0, s>>>(G.view0(), cstart, G.nb, G.blk_order.p);
         AW_LAUNCH();
     }
+    const int* order = G.blk_order_on ? G.blk_order.p : nullptr;
     const int NVt = ph ? 9 : 6;
     // the largest tile, or one private tile per warp for blocks of at most two cells per edge
     // 512-thread CTAs: the aw_p2g call takes 0.43 ms on the 3-level dam_drop_128 against 0.48 ms
@@ -1203,11 +1210,11 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
             // always opted in: the pair queues' static shared memory counts against the default 48 KB too
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<true><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, ph->pid, ph->phase,
-                                                           (int)smem_f, G.blk_busy.p, G.blk_order.p);
+                                                           (int)smem_f, G.blk_busy.p, order);
         } else {
             AW_CUDA(cudaFuncSetAttribute(k_p2g_own<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_p2g_own<false><<<G.nb, nthreads, smem, s>>>(G.view0(), soa, n, cstart, acc, nullptr, nullptr,
-                                                            (int)smem_f, G.blk_busy.p, G.blk_order.p);
+                                                            (int)smem_f, G.blk_busy.p, order);
         }
         AW_LAUNCH();
     }
@@ -1985,7 +1992,8 @@ aw_status g2p_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs, fl
     G.test_copy_timeout = false;
     k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), soa, n, cs, alpha, fa, fb, G.tile_off.p, G.tiles_new.p,
                                                  G.err.p + 1, polls, arm_only, DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p,
-                                                 G.blk_busy.p ? G.tile_ok.p : nullptr, untiled, G.blk_order.p);
+                                                 G.blk_busy.p ? G.tile_ok.p : nullptr, untiled,
+                                                 G.blk_order_on ? G.blk_order.p : nullptr);
     AW_LAUNCH();
     k_g2p_inactive<<<16, 256, 0, s>>>(soa, n, cs + G.tot[0], alpha);
     AW_LAUNCH();
@@ -2057,7 +2065,7 @@ aw_status advect_sorted(MsbgState& G, float* soa, int64_t n, const uint32_t* cs,
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), soa, n, cs, dt, G.tile_off.p, G.tiles_new.p, G.err.p + 1,
                                           DropIn{nullptr, nullptr, nullptr}, G.blk_busy.p ? G.tile_ok.p : nullptr,
-                                          Field3{{un[0], un[1], un[2]}}, G.blk_order.p);
+                                          Field3{{un[0], un[1], un[2]}}, G.blk_order_on ? G.blk_order.p : nullptr);
     AW_LAUNCH();
     return AW_OK;
 }
