@@ -1192,6 +1192,8 @@ aw_status p2g_sorted(MsbgState& G, const float* soa, int64_t n, const uint32_t* 
         k_block_order<<<1, 1024, 0, s>>>(G.view0(), cstart, G.nb, G.blk_order.p);
         AW_LAUNCH();
     }
+    // (G2P and the advection use it too; any order left from an earlier call is still a permutation of
+    // the grid's blocks, so a kernel given one covers every block exactly once)
     const int* order = G.blk_order_on ? G.blk_order.p : nullptr;
     const int NVt = ph ? 9 : 6;
     // the largest tile, or one private tile per warp for blocks of at most two cells per edge
@@ -2610,7 +2612,7 @@ extern "C" aw_status aw_g2p(aw_msbg* g, float* d_vel, const float* d_pos, int64_
         Field3 fa{{un[0], un[1], un[2]}}, fb{{uo[0], uo[1], uo[2]}};
         k_g2p_fused<<<G.nb, G2P_THREADS, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, alpha, fa, fb, G.tile_off.p,
                                                      nullptr, G.err.p + 1, 1 << 20, 0, DropIn{W.sorted, d_vel, W.hash.p},
-                                                     nullptr, nullptr, 0, nullptr);
+                                                     nullptr, nullptr, 0, G.blk_order_on ? G.blk_order.p : nullptr);
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_vel, W.hash.p, 0, alpha);
         AW_LAUNCH();
@@ -2647,7 +2649,8 @@ extern "C" aw_status aw_advect(aw_msbg* g, float* d_pos, int64_t n, float dt, aw
         const size_t smem = (size_t)tile_block(maxres) * sizeof(float);
         AW_CUDA(cudaFuncSetAttribute(k_advect_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_advect_tile<<<G.nb, 256, smem, s>>>(G.view0(), W.soa.p, n, W.cell_start.p, dt, G.tile_off.p, G.tiles_new.p,
-                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p}, nullptr, Field3{}, nullptr);
+                                              G.err.p + 1, DropIn{W.sorted, d_pos, W.hash.p}, nullptr, Field3{},
+                                              G.blk_order_on ? G.blk_order.p : nullptr);
         AW_LAUNCH();
         k_inactive_aos<<<16, 256, 0, s>>>(G.geo, W.sorted, W.cell_start.p + G.tot[0], d_pos, W.hash.p, 1, 0.f);
         AW_LAUNCH();
