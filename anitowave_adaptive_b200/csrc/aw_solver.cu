@@ -927,10 +927,6 @@ __global__ void k_fill_zero(float* __restrict__ x, size_t n) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) x[i] = 0.f;
 }
-__global__ void k_copy_scalar(double* __restrict__ sc, int dst, int src) {
-    pdl_wait();
-    sc[dst] = sc[src];
-}
 
 // ---- conjugate gradients with every vector and scalar in FP32 (AW_PRECISION_FP32_PCG) ----------
 // The same V-cycle preconditioner as the mixed form, without its FP64 residual, direction and
